@@ -1,0 +1,333 @@
+"""Benchmark: FDK backprojection GUPS on the 512^3 x 720-view workload.
+
+Workload (the configuration the metric is quoted on): volume 512^3 of
+0.25 mm voxels, 720 views over 360 deg, flat detector 768x768 of 0.4 mm,
+SID/SDD 500/1000 mm, 20 seeded random ellipsoids, Poisson noise at 1e5
+photons, Ram-Lak.  A step is one full FDK pass (cosine preweight + ramp
+filter + weighted backprojection) over the 720 views into the volume.
+
+value   = voxel x view updates per second of the whole job (all ranks), with
+          projections already in HBM (device-timed with CUDA events).
+e2e     = the same metric through the C-ABI with host buffers: each step
+          copies the projections host->device (pinned) and the volume
+          device->host inside the timed region.
+Inputs (1.7 GB projections, 0.54 GB volume) exceed the 126 MB L2, so no
+flush is needed between steps.
+
+--impl reference times the CPU implementation of the path (the FP64
+multithreaded transcription of the reference's loops; the reference has no
+CPU path of its own) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_VOX = 512
+N_VIEWS = 720
+N_DET = 768
+VOX_MM = 0.25
+PIX_MM = 0.4
+SID, SDD = 500.0, 1000.0
+N_ELL = 20
+I0 = 1e5
+UPDATES = N_VOX ** 3 * N_VIEWS
+WORKLOAD = "fdk-512^3-720v-768^2"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-bf16", action="store_true")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """Samples SM clocks and throttle reasons with nvidia-smi during a region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.thread.join(timeout=2)
+
+    def summary(self):
+        import statistics
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[3:7]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return json.load(fh), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
+
+
+def cpu_baseline(n_views_sample=24, z_slab=16):
+    """FP64 oracle FDK on a bounded sample of the same workload: a subset of
+    views (full 768x768 projections: preweight + filter) backprojected into
+    a z-slab of the 512^3 volume.  Returns GUPS on the host cores."""
+    import numpy as np
+    from oracle import oracle as O
+    views_all = O.build_circular_flat(N_VIEWS, N_VIEWS, SID, SDD, N_DET, N_DET, PIX_MM, PIX_MM)
+    step = N_VIEWS // n_views_sample
+    views = np.ascontiguousarray(views_all[::step][:n_views_sample])
+    rng = O.regular_scan_range(N_VIEWS, N_VIEWS)
+    proj = O.uniform((n_views_sample, N_DET, N_DET), 0.0, 1.0, 17)
+    vol = O.volume_struct((z_slab, N_VOX, N_VOX), VOX_MM)
+    filt = O.filter_struct(1)
+    t0 = time.perf_counter()
+    O.fdk(views, N_DET, N_DET, rng, vol, filt, proj)
+    dt = time.perf_counter() - t0
+    updates = n_views_sample * z_slab * N_VOX * N_VOX
+    return {"value": updates / dt / 1e9, "unit": "GUPS", "cores": O.num_threads(), "kind": "port",
+            "sample": f"{n_views_sample} of 720 views (full 768x768 preweight+ramp filter) "
+                      f"backprojected into a 512x512x{z_slab} slab, FP64, {dt:.1f} s"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    for _ in range(args.warmup):
+        cpu_baseline(n_views_sample=4, z_slab=8)
+    vals = []
+    for _ in range(args.steps):
+        vals.append(cpu_baseline(n_views_sample=8, z_slab=8))
+    value = sum(v["value"] for v in vals) / len(vals)
+    ms = UPDATES / (value * 1e9) * 1e3
+    cb = dict(vals[-1])
+    cb["value"] = value
+    print(json.dumps({
+        "metric": "FDK backprojection GUPS (voxel x view updates/s)", "value": value,
+        "unit": "GUPS", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "config": {"workload": WORKLOAD, "volume": [N_VOX] * 3, "views": N_VIEWS,
+                   "detector": [N_DET, N_DET], "sample_per_step": cb["sample"]},
+        "cpu_baseline": cb,
+        "e2e": {"value": value, "unit": "GUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from fdk_cuda_impl_b200 import CircularScan, RampFilter, VolumeGrid
+    from fdk_cuda_impl_b200 import phantom as PH
+    from fdk_cuda_impl_b200.projectors import FdkPlan, JosephPlan
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device(f"cuda:{local}"))
+
+    scan = CircularScan(N_VIEWS, N_VIEWS, SID, SDD, N_DET, N_DET, PIX_MM, PIX_MM)
+    grid = VolumeGrid.cube(N_VOX, VOX_MM)
+    views = scan.views()
+    # independent object per rank (weak scaling, no data-path collective)
+    ell = PH.random_ellipsoids(1000 + rank, N_ELL)
+    phantom = PH.voxelize(grid, ell, device=f"cuda:{local}")
+    jp = JosephPlan(views, N_DET, N_DET, grid, device=local)
+    proj = jp.forward(phantom)
+    jp.close()
+    del jp
+    PH.poisson_noise_(proj, I0, seed=7 + rank)
+    torch.cuda.synchronize()
+
+    plan = FdkPlan(views, N_DET, N_DET, scan.scan_range, grid, RampFilter(), "fp32", device=local)
+    vol = torch.empty(grid.shape, dtype=torch.float32, device=f"cuda:{local}")
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return t.item()
+
+    def timed(fn, k):
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        return max_over_ranks(e0.elapsed_time(e1) / k)
+
+    # full FDK steps, device resident
+    for _ in range(args.warmup):
+        plan.execute(proj, vol)
+    with ClockSampler(local) as clocks:
+        ms = timed(lambda: plan.execute(proj, vol), args.steps)
+    clock_info = clocks.summary()
+    value = world * UPDATES / (ms * 1e-3) / 1e9
+
+    # stage timings for the roofline (same stream, CUDA events)
+    filtered = plan.filter(proj)
+    for _ in range(2):
+        plan.backproject(filtered, vol)
+    ms_bp = timed(lambda: plan.backproject(filtered, vol), args.steps)
+    ms_filter = timed(lambda: plan.filter(proj), args.steps)
+    del filtered
+
+    # end to end through the C-ABI with pinned host buffers
+    h_proj = torch.empty(proj.shape, dtype=torch.float32, pin_memory=True)
+    h_proj.copy_(proj)
+    h_vol = torch.empty(grid.shape, dtype=torch.float32, pin_memory=True)
+    d_in = torch.empty_like(proj)
+    del proj
+
+    def e2e_step():
+        d_in.copy_(h_proj, non_blocking=True)
+        plan.execute(d_in, vol)
+        h_vol.copy_(vol, non_blocking=True)
+
+    for _ in range(max(1, args.warmup - 1)):
+        e2e_step()
+    ms_e2e = timed(e2e_step, args.steps)
+    e2e_value = world * UPDATES / (ms_e2e * 1e-3) / 1e9
+
+    # BF16 tensor-core form on the same inputs
+    bf16 = None
+    if not args.no_bf16:
+        plan_b = FdkPlan(views, N_DET, N_DET, scan.scan_range, grid, RampFilter(), "bf16", device=local)
+        d_in.copy_(h_proj)
+        ref_vol = plan.execute(d_in, vol).clone()
+        vb = torch.empty_like(vol)
+        for _ in range(args.warmup):
+            plan_b.execute(d_in, vb)
+        ms_b = timed(lambda: plan_b.execute(d_in, vb), args.steps)
+        diff = (vb.double() - ref_vol.double()).pow(2).mean().sqrt() / ref_vol.double().pow(2).mean().sqrt()
+        bf16 = {"ms_per_step": ms_b, "gups": world * UPDATES / (ms_b * 1e-3) / 1e9,
+                "speedup_vs_fp32": ms / ms_b, "rel_rmse_vs_fp32_form": float(diff)}
+        plan_b.close()
+        del ref_vol, vb
+
+    peaks, peak_src = measured_peaks()
+    # HBM roofline of the dominant kernel (backprojection): compulsory bytes
+    # per launch = filtered projections read once + volume written once.
+    bp_bytes = 4.0 * N_VIEWS * N_DET * N_DET + 4.0 * N_VOX ** 3
+    achieved = bp_bytes / (ms_bp * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"], "traffic": None, "peak_source": peak_src,
+                "kernel": "fdk_bp_kernel", "kernel_ms": ms_bp,
+                "algorithmic_bytes_per_launch": bp_bytes}
+    # on-chip view of the same kernel: 16 B of bilinear taps per update
+    sm_mhz = clock_info.get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
+    onchip_peak = 148 * 128 * sm_mhz * 1e6 / 1e9  # GB/s of shared/L1 bandwidth
+    onchip = {"tap_bytes_per_update": 16, "achieved_gbs": 16 * UPDATES / (ms_bp * 1e-3) / 1e9,
+              "peak_gbs_nominal": onchip_peak,
+              "frac": 16 * UPDATES / (ms_bp * 1e-3) / 1e9 / onchip_peak,
+              "bp_gups": UPDATES / (ms_bp * 1e-3) / 1e9}
+
+    line = {
+        "metric": "FDK backprojection GUPS (voxel x view updates/s)",
+        "value": value, "unit": "GUPS", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "volume": [N_VOX] * 3, "voxel_mm": VOX_MM,
+                   "views": N_VIEWS, "detector": [N_DET, N_DET], "pixel_mm": PIX_MM,
+                   "sid_sdd_mm": [SID, SDD], "ellipsoids": N_ELL, "noise_i0": I0,
+                   "filter": "ramlak", "precision": "fp32",
+                   "l2": "inputs larger than L2 (1.7 GB projections, 0.54 GB volume)",
+                   "parallelism": f"independent objects x{world}"},
+        "stages_ms": {"filter": ms_filter, "backproject": ms_bp},
+        "roofline": roofline,
+        "onchip": onchip,
+        "e2e": {"value": e2e_value, "unit": "GUPS", "ms_per_step": ms_e2e,
+                "h2d_bytes_per_step": int(h_proj.numel() * 4),
+                "d2h_bytes_per_step": int(h_vol.numel() * 4)},
+        "bf16": bf16,
+        "gpu_launches": 3 * args.steps,
+        "clocks": clock_info,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_baseline()
+        except Exception as exc:  # the baseline is reported, never required
+            line["cpu_baseline"] = {"error": str(exc)}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    plan.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

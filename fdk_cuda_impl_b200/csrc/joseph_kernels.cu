@@ -1,0 +1,299 @@
+// Joseph forward projector and its exact matched backprojector for sm_100a.
+//
+// Discretisation (src/FlatFpBp/FP/kernels/YkFPKernels.cu:10-202): a ray from
+// the source through pixel centre (u,v) is sampled once per voxel centre of
+// the view's main axis; each sample is the bilinear interpolation of that
+// slice on the two minor axes with zero outside the volume; the ray sum is
+// scaled by the chord length per step sqrt(v0^2 + (a1 v1)^2 + (a2 v2)^2).
+// The backprojector applies the transpose of exactly these weights,
+// gathering per voxel over the rays that touch it (no atomics), where the
+// reference scatters with four atomicAdd per sample
+// (src/FlatFpBp/BP/kernels/YkBPJosephKernel.cu:12-113).
+#include "ykb_internal.hpp"
+
+namespace ykb {
+namespace {
+
+// Ray parameters shared bit-for-bit by the forward projector and the ray
+// table of the backprojector: slopes a1,a2 and offsets e1,e2 such that the
+// minor-axis voxel-index coordinates at main-axis slice s are
+//   f1 = fmaf(a1, c0, e1), f2 = fmaf(a2, c0, e2), c0 = s - (n0-1)/2,
+// plus the chord length per step.  Evaluated in FP64, rounded once.
+struct RayParams { float a1, e1, a2, e2, len; bool ok; };
+
+__device__ __forceinline__ double comp(const double* p, int axis, int which)
+{
+    // (main, minor1, minor2) permutation of AxisX/AxisY/AxisZ
+    // (src/common/cuda/operators/YkOperatorKernelTypes.cuh:212-275)
+    const int k = axis == 0 ? which : axis == 1 ? (which == 0 ? 1 : which == 1 ? 0 : 2)
+                                                : (which == 0 ? 2 : which == 1 ? 0 : 1);
+    return p[k];
+}
+
+__device__ __forceinline__ RayParams ray_params(const JosephView& j, int iu, int iv)
+{
+    double det[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) det[c] = j.detS[c] + iu * j.detU[c] + iv * j.detV[c];
+    RayParams r{};
+    const double s0 = comp(j.src, j.axis, 0), s1 = comp(j.src, j.axis, 1), s2 = comp(j.src, j.axis, 2);
+    const double dc0 = s0 - comp(det, j.axis, 0);
+    if (fabs(dc0) < 1e-12) { r.ok = false; return r; }
+    const double a1 = (s1 - comp(det, j.axis, 1)) / dc0;
+    const double a2 = (s2 - comp(det, j.axis, 2)) / dc0;
+    const double b1 = s1 - a1 * s0, b2 = s2 - a2 * s0;
+    const double a1v1 = a1 * j.v1, a2v2 = a2 * j.v2;
+    r.a1 = static_cast<float>(a1);
+    r.a2 = static_cast<float>(a2);
+    r.e1 = static_cast<float>(b1 + 0.5 * (j.n1 - 1));
+    r.e2 = static_cast<float>(b2 + 0.5 * (j.n2 - 1));
+    r.len = static_cast<float>(sqrt(j.v0 * j.v0 + a1v1 * a1v1 + a2v2 * a2v2));
+    r.ok = true;
+    return r;
+}
+
+// Slices s where the sample can touch the volume: -1 < f < n on both minor
+// axes (conservatively widened by one slice each side).
+__device__ __forceinline__ void slice_range(float a, float e, int n, int n0, int& lo, int& hi)
+{
+    const float h = 0.5f * (n0 - 1);
+    if (fabsf(a) < 1e-12f) {
+        if (!(e > -1.f && e < static_cast<float>(n))) { lo = 1; hi = 0; }
+        return;
+    }
+    float t0 = (-1.f - e) / a + h, t1 = (static_cast<float>(n) - e) / a + h;
+    if (t0 > t1) { const float t = t0; t0 = t1; t1 = t; }
+    // clamp before the integer conversion (NaN compares false and stays put)
+    t0 = fminf(fmaxf(t0, -1e7f), 1e7f);
+    t1 = fminf(fmaxf(t1, -1e7f), 1e7f);
+    lo = max(lo, static_cast<int>(floorf(t0)) - 1);
+    hi = min(hi, static_cast<int>(ceilf(t1)) + 1);
+}
+
+// One thread per ray; a block covers 32 channels x 4 rows of one view.
+__global__ void __launch_bounds__(128) joseph_fp_kernel(const float* __restrict__ slab,
+    const JosephView* __restrict__ views, int view0, int nu, int nv, float* __restrict__ proj,
+    int accumulate)
+{
+    const int iu = blockIdx.x * 32 + threadIdx.x;
+    const int iv = blockIdx.y * 4 + threadIdx.y;
+    const int k = view0 + blockIdx.z;
+    if (iu >= nu || iv >= nv) return;
+    const JosephView& j = views[k];
+    const RayParams r = ray_params(j, iu, iv);
+    float acc = 0.f;
+    if (r.ok) {
+        int lo = 0, hi = j.n0 - 1;
+        slice_range(r.a1, r.e1, j.n1, j.n0, lo, hi);
+        slice_range(r.a2, r.e2, j.n2, j.n0, lo, hi);
+        const long plane = static_cast<long>(j.n1) * j.n2;
+        const float half = 0.5f * (j.n0 - 1);
+        for (int s = lo; s <= hi; ++s) {
+            const float c0 = static_cast<float>(s) - half;
+            const float f1 = fmaf(r.a1, c0, r.e1);
+            const float f2 = fmaf(r.a2, c0, r.e2);
+            const float fl1 = floorf(f1), fl2 = floorf(f2);
+            const int i1 = static_cast<int>(fl1), i2 = static_cast<int>(fl2);
+            const float w1 = f1 - fl1, w2 = f2 - fl2;
+            const float* sl = slab + s * plane;
+            const bool c1a = static_cast<unsigned>(i1) < static_cast<unsigned>(j.n1);
+            const bool c1b = static_cast<unsigned>(i1 + 1) < static_cast<unsigned>(j.n1);
+            const bool c2a = static_cast<unsigned>(i2) < static_cast<unsigned>(j.n2);
+            const bool c2b = static_cast<unsigned>(i2 + 1) < static_cast<unsigned>(j.n2);
+            const long ra = static_cast<long>(i2) * j.n1, rb = ra + j.n1;
+            const float p00 = (c1a && c2a) ? __ldg(sl + ra + i1) : 0.f;
+            const float p10 = (c1b && c2a) ? __ldg(sl + ra + i1 + 1) : 0.f;
+            const float p01 = (c1a && c2b) ? __ldg(sl + rb + i1) : 0.f;
+            const float p11 = (c1b && c2b) ? __ldg(sl + rb + i1 + 1) : 0.f;
+            acc += (1.f - w2) * ((1.f - w1) * p00 + w1 * p10) + w2 * ((1.f - w1) * p01 + w1 * p11);
+        }
+        acc *= r.len;
+    }
+    float* dst = proj + (static_cast<long>(k) * nv + iv) * nu + iu;
+    *dst = accumulate ? *dst + acc : acc;
+}
+
+__global__ void __launch_bounds__(128) joseph_ray_table_kernel(const JosephView* __restrict__ views,
+    int nu, int nv, float4* __restrict__ rays, float* __restrict__ lens)
+{
+    const int iu = blockIdx.x * 32 + threadIdx.x;
+    const int iv = blockIdx.y * 4 + threadIdx.y;
+    const int k = blockIdx.z;
+    if (iu >= nu || iv >= nv) return;
+    const RayParams r = ray_params(views[k], iu, iv);
+    const long idx = (static_cast<long>(k) * nv + iv) * nu + iu;
+    rays[idx] = r.ok ? make_float4(r.a1, r.e1, r.a2, r.e2) : make_float4(0.f, -1e30f, 0.f, -1e30f);
+    lens[idx] = r.ok ? r.len : 0.f;
+}
+
+// vol[z][y][x] -> slab[y][z][x] (main axis Y) and slab[x][z][y] (main axis X)
+__global__ void transpose_yzx_kernel(const float* __restrict__ in, int nx, int ny, int nz,
+    float* __restrict__ out)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y, z = blockIdx.z;
+    if (x >= nx) return;
+    out[(static_cast<long>(y) * nz + z) * nx + x] = in[(static_cast<long>(z) * ny + y) * nx + x];
+}
+
+__global__ void transpose_xzy_kernel(const float* __restrict__ in, int nx, int ny, int nz,
+    float* __restrict__ out)
+{
+    __shared__ float tile[32][33];
+    const int z = blockIdx.z;
+    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int y = y0 + r, x = x0 + threadIdx.x;
+        tile[r][threadIdx.x] = (x < nx && y < ny) ? in[(static_cast<long>(z) * ny + y) * nx + x] : 0.f;
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int x = x0 + r, y = y0 + threadIdx.x;
+        if (x < nx && y < ny) out[(static_cast<long>(x) * nz + z) * ny + y] = tile[threadIdx.x][r];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Matched backprojector, voxel-driven.  For voxel (s, j1, j2) in a view's
+// main-axis frame the rays with a non-zero weight are those whose sample on
+// slice s lies within one voxel of (j1, j2) on both minor axes; their pixels
+// lie in the detector image of the square [j1-1,j1+1]x[j2-1,j2+1] on that
+// slice, found from its four projected corners.  Each candidate's sample
+// position is recomputed from the shared ray table with the forward
+// projector's exact arithmetic, so the weights are those of joseph_fp_kernel.
+// ---------------------------------------------------------------------------
+struct ViewProj { float m[12]; };  // (u*w, v*w, w) = M (x', y', z', 1)
+
+__global__ void __launch_bounds__(256) joseph_bp_kernel(const float* __restrict__ proj,
+    const float4* __restrict__ rays, const float* __restrict__ lens,
+    const ViewProj* __restrict__ vp, const JosephView* __restrict__ views, int n_views,
+    int nu, int nv, int nx, int ny, int nz, float* __restrict__ vol, int accumulate)
+{
+    const int x = blockIdx.x * 32 + threadIdx.x;
+    const int y = blockIdx.y * 8 + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x >= nx || y >= ny) return;
+    const long view_elems = static_cast<long>(nu) * nv;
+    float acc = 0.f;
+    for (int k = 0; k < n_views; ++k) {
+        const JosephView& j = views[k];
+        int s, j1, j2;
+        if (j.axis == 0) { s = x; j1 = y; j2 = z; }
+        else if (j.axis == 1) { s = y; j1 = x; j2 = z; }
+        else { s = z; j1 = x; j2 = y; }
+        const float c0 = static_cast<float>(s) - 0.5f * (j.n0 - 1);
+        // detector bounding box of the slice square
+        const ViewProj& m = vp[k];
+        float umin = 1e30f, umax = -1e30f, vmin = 1e30f, vmax = -1e30f;
+#pragma unroll
+        for (int corner = 0; corner < 4; ++corner) {
+            const float d1 = (corner & 1) ? 1.f : -1.f, d2 = (corner & 2) ? 1.f : -1.f;
+            const float q1 = static_cast<float>(j1) + d1 - 0.5f * (j.n1 - 1);
+            const float q2 = static_cast<float>(j2) + d2 - 0.5f * (j.n2 - 1);
+            float px, py, pz;
+            if (j.axis == 0) { px = c0; py = q1; pz = q2; }
+            else if (j.axis == 1) { px = q1; py = c0; pz = q2; }
+            else { px = q1; py = q2; pz = c0; }
+            const float w = fmaf(m.m[8], px, fmaf(m.m[9], py, fmaf(m.m[10], pz, m.m[11])));
+            const float rw = 1.f / w;
+            const float u = fmaf(m.m[0], px, fmaf(m.m[1], py, fmaf(m.m[2], pz, m.m[3]))) * rw;
+            const float v = fmaf(m.m[4], px, fmaf(m.m[5], py, fmaf(m.m[6], pz, m.m[7]))) * rw;
+            umin = fminf(umin, u); umax = fmaxf(umax, u);
+            vmin = fminf(vmin, v); vmax = fmaxf(vmax, v);
+        }
+        constexpr float margin = 0.05f;
+        const int u0 = max(0, static_cast<int>(ceilf(umin - margin)));
+        const int u1 = min(nu - 1, static_cast<int>(floorf(umax + margin)));
+        const int v0 = max(0, static_cast<int>(ceilf(vmin - margin)));
+        const int v1 = min(nv - 1, static_cast<int>(floorf(vmax + margin)));
+        const long base = k * view_elems;
+        for (int iv = v0; iv <= v1; ++iv) {
+            for (int iu = u0; iu <= u1; ++iu) {
+                const long idx = base + static_cast<long>(iv) * nu + iu;
+                const float4 r = __ldg(rays + idx);
+                const float f1 = fmaf(r.x, c0, r.y);
+                const float f2 = fmaf(r.z, c0, r.w);
+                const float fl1 = floorf(f1), fl2 = floorf(f2);
+                const int i1 = static_cast<int>(fl1), i2 = static_cast<int>(fl2);
+                const float w1 = f1 - fl1, w2 = f2 - fl2;
+                const float wa = (i1 == j1) ? 1.f - w1 : ((i1 + 1 == j1) ? w1 : 0.f);
+                const float wb = (i2 == j2) ? 1.f - w2 : ((i2 + 1 == j2) ? w2 : 0.f);
+                const float w = wa * wb;
+                if (w != 0.f) acc = fmaf(__ldg(proj + idx) * __ldg(lens + idx), w, acc);
+            }
+        }
+    }
+    float* dst = vol + (static_cast<long>(z) * ny + y) * nx + x;
+    *dst = accumulate ? *dst + acc : acc;
+}
+
+} // namespace
+
+cudaError_t launch_joseph_transpose(const float* vol, int nx, int ny, int nz, float* vol_yzx,
+    float* vol_xzy, cudaStream_t s)
+{
+    if (vol_yzx) {
+        const dim3 grid((nx + 127) / 128, ny, nz);
+        transpose_yzx_kernel<<<grid, 128, 0, s>>>(vol, nx, ny, nz, vol_yzx);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    if (vol_xzy) {
+        const dim3 grid((nx + 31) / 32, (ny + 31) / 32, nz);
+        transpose_xzy_kernel<<<grid, dim3(32, 8), 0, s>>>(vol, nx, ny, nz, vol_xzy);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_joseph_fp(const float* slabs[3], const JosephView* views,
+    const int* view_axis_host, int n_views, int nu, int nv, float* proj, int accumulate,
+    cudaStream_t s)
+{
+    // consecutive views with the same main axis share one launch (the
+    // forEachAxisRun grouping of YkOperatorKernelTypes.cuh:171-210)
+    int first = 0;
+    while (first < n_views) {
+        const int axis = view_axis_host[first];
+        int end = first + 1;
+        while (end < n_views && view_axis_host[end] == axis) ++end;
+        int done = first;
+        while (done < end) {
+            const int count = min(end - done, 65535);
+            const dim3 grid((nu + 31) / 32, (nv + 3) / 4, count);
+            joseph_fp_kernel<<<grid, dim3(32, 4), 0, s>>>(slabs[axis], views, done, nu, nv, proj,
+                accumulate);
+            const cudaError_t e = cudaGetLastError();
+            if (e != cudaSuccess) return e;
+            done += count;
+        }
+        first = end;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t launch_joseph_ray_table(const JosephView* views, int n_views, int nu, int nv,
+    float4* rays, float* lens, cudaStream_t s)
+{
+    for (int done = 0; done < n_views; done += 65535) {
+        const int count = min(n_views - done, 65535);
+        const dim3 grid((nu + 31) / 32, (nv + 3) / 4, count);
+        joseph_ray_table_kernel<<<grid, dim3(32, 4), 0, s>>>(views + done, nu, nv,
+            rays + static_cast<long>(done) * nu * nv, lens + static_cast<long>(done) * nu * nv);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t launch_joseph_bp(const float* proj, const float4* rays, const float* lens,
+    const float* view_proj, const JosephView* views, int n_views, int nu, int nv,
+    const ykb_volume& vol, float* out, int accumulate, cudaStream_t s)
+{
+    const dim3 grid((vol.nx + 31) / 32, (vol.ny + 7) / 8, vol.nz);
+    joseph_bp_kernel<<<grid, dim3(32, 8), 0, s>>>(proj, rays, lens,
+        reinterpret_cast<const ViewProj*>(view_proj), views, n_views, nu, nv, vol.nx, vol.ny,
+        vol.nz, out, accumulate);
+    return cudaGetLastError();
+}
+
+} // namespace ykb

@@ -1,0 +1,422 @@
+// C-ABI entry points of libykb.so (declared in include/ykb.h).
+#include "ykb_internal.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+
+namespace ykb {
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+void clear_error() { g_last_error.clear(); }
+const char* last_error() { return g_last_error.c_str(); }
+
+ykb_status cuda_status(cudaError_t status, const char* what)
+{
+    if (status == cudaSuccess) return YKB_OK;
+    set_error(std::string("CUDA error in ") + what + ": " + cudaGetErrorName(status) + " (" +
+        cudaGetErrorString(status) + ")");
+    if (status == cudaErrorMemoryAllocation) {
+        cudaGetLastError();  // allocation failure is not sticky; clear it
+        return YKB_ERR_OUT_OF_MEMORY;
+    }
+    return YKB_ERR_CUDA;
+}
+
+namespace {
+
+ykb_status fail(ykb_status code, const std::string& msg)
+{
+    set_error(msg);
+    return code;
+}
+
+bool valid_volume(const ykb_volume* v)
+{
+    return v && v->nx > 0 && v->ny > 0 && v->nz > 0 && v->vox_x > 0.f && v->vox_y > 0.f &&
+        v->vox_z > 0.f && std::isfinite(v->vox_x) && std::isfinite(v->vox_y) &&
+        std::isfinite(v->vox_z) && std::isfinite(v->center_x) && std::isfinite(v->center_y) &&
+        std::isfinite(v->center_z);
+}
+
+// validAnalyticFilter (src/Filter/YkAnalyticFilterSettings.hpp:5-13)
+bool valid_filter(const ykb_filter* p)
+{
+    return p && p->type >= 0 && p->type <= 9 && std::isfinite(p->cutoff) && p->cutoff > 0.f &&
+        p->cutoff <= 0.5f && std::isfinite(p->gain) && p->gain > 0.f &&
+        std::isfinite(p->butterworth_order) && p->butterworth_order > 0.f &&
+        std::isfinite(p->kaiser_beta) && p->kaiser_beta >= 0.f && std::isfinite(p->tukey_alpha) &&
+        p->tukey_alpha >= 0.f && p->tukey_alpha <= 1.f;
+}
+
+ykb_status check_device(int device)
+{
+    int count = 0;
+    const cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess) return cuda_status(e, "cudaGetDeviceCount");
+    if (device < 0 || device >= count)
+        return fail(YKB_ERR_INVALID_CONFIG, "device index out of range");
+    return YKB_OK;
+}
+
+size_t volume_elems(const ykb_volume& v)
+{
+    return static_cast<size_t>(v.nx) * v.ny * v.nz;
+}
+
+// Views per workspace chunk: bounded so the filter workspace stays below
+// about 4 GiB whatever the scan length.
+int chunk_capacity(int n_views, int nu, int nv)
+{
+    const size_t per_view = static_cast<size_t>(nu) * nv * (sizeof(float) * 2);
+    const size_t budget = size_t(4) << 30;
+    const size_t cap = std::max<size_t>(1, budget / std::max<size_t>(per_view, 1));
+    return static_cast<int>(std::min<size_t>(n_views, cap));
+}
+
+} // namespace
+} // namespace ykb
+
+using namespace ykb;
+
+extern "C" {
+
+YKB_API int ykb_version(void) { return 100; }
+
+YKB_API const char* ykb_last_error(void) { return ykb::last_error(); }
+
+// include/YKCBCT/interface/YkSystemReconstruction.hpp:22-28
+YKB_API float ykb_regular_scan_range(int total_views, int views_per_turn)
+{
+    constexpr float kTwoPi = 6.28318530717958647692f;
+    return kTwoPi * static_cast<float>(total_views) / static_cast<float>(views_per_turn);
+}
+
+YKB_API ykb_status ykb_build_circular_flat(const ykb_circular_flat* spec, ykb_cone_view* out,
+    int capacity)
+{
+    clear_error();
+    if (!spec || !out) return fail(YKB_ERR_INVALID_BUFFER, "null spec or output");
+    if (capacity < spec->total_views)
+        return fail(YKB_ERR_INVALID_BUFFER, "output capacity smaller than total_views");
+    std::string why;
+    if (!build_circular_flat(*spec, out, why)) return fail(YKB_ERR_INVALID_GEOMETRY, why);
+    return YKB_OK;
+}
+
+// ------------------------------------------------------------------ FDK ---
+YKB_API ykb_status ykb_fdk_plan_create(const ykb_cone_view* views, int n_views, int nu, int nv,
+    float scan_range_rad, const ykb_volume* volume, const ykb_filter* filter, int precision,
+    int device, ykb_fdk_plan** plan_out)
+{
+    clear_error();
+    if (!plan_out) return fail(YKB_ERR_INVALID_BUFFER, "null plan output");
+    *plan_out = nullptr;
+    if (!views || n_views <= 0 || nu <= 0 || nv <= 0)
+        return fail(YKB_ERR_INVALID_CONFIG, "views, view count and detector size must be positive");
+    if (!valid_volume(volume)) return fail(YKB_ERR_INVALID_CONFIG, "invalid volume grid");
+    if (!valid_filter(filter)) return fail(YKB_ERR_INVALID_CONFIG, "invalid analytic filter parameters");
+    if (precision != YKB_PRECISION_FP32 && precision != YKB_PRECISION_BF16)
+        return fail(YKB_ERR_INVALID_CONFIG, "unknown precision");
+    if (const ykb_status st = check_device(device)) return st;
+    DeviceGuard guard(device);
+
+    ykb_fdk_plan* p = new (std::nothrow) ykb_fdk_plan();
+    if (!p) return fail(YKB_ERR_OUT_OF_MEMORY, "host allocation failed");
+    p->device = device; p->n_views = n_views; p->nu = nu; p->nv = nv;
+    p->scan_range = scan_range_rad; p->volume = *volume; p->filter = *filter;
+    p->precision = precision;
+    std::string why;
+    if (!derive_fdk_geometry(views, n_views, nu, nv, scan_range_rad, p->derived, why)) {
+        delete p;
+        return fail(YKB_ERR_INVALID_GEOMETRY, why);
+    }
+    std::vector<FdkViewCoef> coef;
+    std::vector<FdkPreweightView> pw;
+    build_fdk_coefficients(p->derived, nu, coef, pw, p->axial);
+    // weights are built once with du of the first view (.../FDK/
+    // YkFDKFilterProcessor.hpp:111,216-232)
+    std::vector<double> h;
+    build_ramp_kernel(nu, p->derived[0].du, *filter, h);
+    std::vector<float> hf(h.begin(), h.end());
+
+    p->batch_capacity = chunk_capacity(n_views, nu, nv);
+    const size_t chunk_elems = static_cast<size_t>(p->batch_capacity) * nu * nv;
+    const size_t filt_bytes = chunk_elems * (precision == YKB_PRECISION_BF16 ? 2 : 4);
+    cudaError_t e;
+    if ((e = p->coef.alloc(sizeof(FdkViewCoef) * n_views)) != cudaSuccess ||
+        (e = p->pwv.alloc(sizeof(FdkPreweightView) * n_views)) != cudaSuccess ||
+        (e = p->ramp.alloc(sizeof(float) * hf.size())) != cudaSuccess ||
+        (e = p->work_a.alloc(chunk_elems * sizeof(float))) != cudaSuccess ||
+        (e = p->work_filtered.alloc(filt_bytes)) != cudaSuccess) {
+        delete p;
+        return cuda_status(e, "cudaMalloc (FDK plan workspace)");
+    }
+    if ((e = cudaMemcpy(p->coef.ptr, coef.data(), sizeof(FdkViewCoef) * n_views,
+             cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(p->pwv.ptr, pw.data(), sizeof(FdkPreweightView) * n_views,
+             cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(p->ramp.ptr, hf.data(), sizeof(float) * hf.size(),
+             cudaMemcpyHostToDevice)) != cudaSuccess) {
+        delete p;
+        return cuda_status(e, "cudaMemcpy (FDK plan tables)");
+    }
+    *plan_out = p;
+    return YKB_OK;
+}
+
+YKB_API ykb_status ykb_fdk_plan_destroy(ykb_fdk_plan* plan)
+{
+    clear_error();
+    if (!plan) return YKB_OK;
+    DeviceGuard guard(plan->device);
+    delete plan;
+    return YKB_OK;
+}
+
+YKB_API size_t ykb_fdk_workspace_bytes(const ykb_fdk_plan* p)
+{
+    if (!p) return 0;
+    return p->coef.bytes + p->pwv.bytes + p->ramp.bytes + p->toeplitz_hi.bytes +
+        p->toeplitz_lo.bytes + p->work_a.bytes + p->work_filtered.bytes + p->err_flag.bytes;
+}
+
+namespace {
+
+ykb_status check_range(const ykb_fdk_plan* p, const void* buf, int dtype, int view_offset,
+    int n_views)
+{
+    if (!p) return fail(YKB_ERR_INVALID_CONFIG, "null plan");
+    if (!buf) return fail(YKB_ERR_INVALID_BUFFER, "null projection buffer");
+    if (dtype != YKB_DTYPE_F32 && dtype != YKB_DTYPE_BF16)
+        return fail(YKB_ERR_INVALID_CONFIG, "unknown projection dtype");
+    if (view_offset < 0 || n_views <= 0 || view_offset > p->n_views - n_views)
+        return fail(YKB_ERR_INVALID_CONFIG, "view_offset/n_views outside the prepared views");
+    return YKB_OK;
+}
+
+size_t dtype_bytes(int dtype) { return dtype == YKB_DTYPE_BF16 ? 2 : 4; }
+
+// preweight + ramp for views [first, first+count) of the plan, input rows at
+// proj, output into dst (plan dtype)
+ykb_status filter_chunk(ykb_fdk_plan* p, const void* proj, int proj_dtype, int first, int count,
+    void* dst, cudaStream_t s)
+{
+    const FdkPreweightView* pwv = p->pwv.as<FdkPreweightView>() + first;
+    const int out_dtype = p->precision == YKB_PRECISION_BF16 ? YKB_DTYPE_BF16 : YKB_DTYPE_F32;
+    YKB_TRY_CUDA(launch_fdk_preweight(proj, proj_dtype, pwv, count, p->nu, p->nv,
+        p->work_a.as<float>(), s));
+    YKB_TRY_CUDA(launch_fdk_ramp_fp32(p->work_a.as<float>(), p->ramp.as<float>(), pwv, count,
+        p->nu, p->nv, dst, out_dtype, s));
+    return YKB_OK;
+}
+
+} // namespace
+
+YKB_API ykb_status ykb_fdk_filter(ykb_fdk_plan* p, const void* d_proj, int proj_dtype,
+    int view_offset, int n_views, void* d_filtered, ykb_stream stream)
+{
+    clear_error();
+    if (const ykb_status st = check_range(p, d_proj, proj_dtype, view_offset, n_views)) return st;
+    if (!d_filtered) return fail(YKB_ERR_INVALID_BUFFER, "null filtered output");
+    DeviceGuard guard(p->device);
+    const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const size_t view_elems = static_cast<size_t>(p->nu) * p->nv;
+    const size_t out_b = p->precision == YKB_PRECISION_BF16 ? 2 : 4;
+    for (int c = 0; c < n_views; c += p->batch_capacity) {
+        const int cnt = std::min(p->batch_capacity, n_views - c);
+        const char* in = static_cast<const char*>(d_proj) + c * view_elems * dtype_bytes(proj_dtype);
+        char* out = static_cast<char*>(d_filtered) + c * view_elems * out_b;
+        if (const ykb_status st = filter_chunk(p, in, proj_dtype, view_offset + c, cnt, out, s))
+            return st;
+    }
+    return YKB_OK;
+}
+
+YKB_API ykb_status ykb_fdk_backproject(ykb_fdk_plan* p, const void* d_filtered,
+    int filtered_dtype, int view_offset, int n_views, float* d_volume, int clear_output,
+    ykb_stream stream)
+{
+    clear_error();
+    if (const ykb_status st = check_range(p, d_filtered, filtered_dtype, view_offset, n_views))
+        return st;
+    if (!d_volume) return fail(YKB_ERR_INVALID_BUFFER, "null volume buffer");
+    DeviceGuard guard(p->device);
+    const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    YKB_TRY_CUDA(launch_fdk_backproject(d_filtered, filtered_dtype,
+        p->coef.as<FdkViewCoef>() + view_offset, n_views, p->nu, p->nv, make_grid(p->volume),
+        p->axial, d_volume, clear_output ? 0 : 1, s));
+    return YKB_OK;
+}
+
+YKB_API ykb_status ykb_fdk_execute(ykb_fdk_plan* p, const void* d_proj, int proj_dtype,
+    int view_offset, int n_views, float* d_volume, int clear_output, ykb_stream stream)
+{
+    clear_error();
+    if (const ykb_status st = check_range(p, d_proj, proj_dtype, view_offset, n_views)) return st;
+    if (!d_volume) return fail(YKB_ERR_INVALID_BUFFER, "null volume buffer");
+    DeviceGuard guard(p->device);
+    const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const size_t view_elems = static_cast<size_t>(p->nu) * p->nv;
+    const int filt_dtype = p->precision == YKB_PRECISION_BF16 ? YKB_DTYPE_BF16 : YKB_DTYPE_F32;
+    const VolumeGrid grid = make_grid(p->volume);
+    for (int c = 0; c < n_views; c += p->batch_capacity) {
+        const int cnt = std::min(p->batch_capacity, n_views - c);
+        const char* in = static_cast<const char*>(d_proj) + c * view_elems * dtype_bytes(proj_dtype);
+        if (const ykb_status st = filter_chunk(p, in, proj_dtype, view_offset + c, cnt,
+                p->work_filtered.ptr, s))
+            return st;
+        const int accumulate = (c == 0 && clear_output) ? 0 : 1;
+        YKB_TRY_CUDA(launch_fdk_backproject(p->work_filtered.ptr, filt_dtype,
+            p->coef.as<FdkViewCoef>() + view_offset + c, cnt, p->nu, p->nv, grid, p->axial,
+            d_volume, accumulate, s));
+    }
+    return YKB_OK;
+}
+
+// --------------------------------------------------------------- Joseph ---
+YKB_API ykb_status ykb_joseph_plan_create(const ykb_cone_view* views, int n_views, int nu, int nv,
+    const ykb_volume* volume, int device, ykb_joseph_plan** plan_out)
+{
+    clear_error();
+    if (!plan_out) return fail(YKB_ERR_INVALID_BUFFER, "null plan output");
+    *plan_out = nullptr;
+    if (!views || n_views <= 0 || nu <= 0 || nv <= 0)
+        return fail(YKB_ERR_INVALID_CONFIG, "views, view count and detector size must be positive");
+    if (!valid_volume(volume)) return fail(YKB_ERR_INVALID_CONFIG, "invalid volume grid");
+    if (const ykb_status st = check_device(device)) return st;
+    DeviceGuard guard(device);
+    ykb_joseph_plan* p = new (std::nothrow) ykb_joseph_plan();
+    if (!p) return fail(YKB_ERR_OUT_OF_MEMORY, "host allocation failed");
+    p->device = device; p->n_views = n_views; p->nu = nu; p->nv = nv; p->volume = *volume;
+    std::string why;
+    if (!build_joseph_views(views, n_views, nu, nv, *volume, p->host_views, why)) {
+        delete p;
+        return fail(YKB_ERR_INVALID_GEOMETRY, why);
+    }
+    p->axes.resize(n_views);
+    bool need_x = false, need_y = false;
+    std::vector<float> vp(static_cast<size_t>(n_views) * 12);
+    for (int i = 0; i < n_views; ++i) {
+        const JosephView& j = p->host_views[i];
+        p->axes[i] = j.axis;
+        need_x |= j.axis == 0;
+        need_y |= j.axis == 1;
+        // voxel-space 3x4 projection (u w, v w, w) = M (x', y', z', 1)
+        const double* S = j.src; const double* D0 = j.detS; const double* U = j.detU; const double* V = j.detV;
+        const double n[3] = {U[1] * V[2] - U[2] * V[1], U[2] * V[0] - U[0] * V[2], U[0] * V[1] - U[1] * V[0]};
+        auto dot = [](const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; };
+        const double sd[3] = {S[0] - D0[0], S[1] - D0[1], S[2] - D0[2]};
+        const double plane = -dot(n, sd);
+        const double W[4] = {n[0], n[1], n[2], -dot(n, S)};
+        const double au = dot(sd, U), av = dot(sd, V);
+        double DU[4], DV[4];
+        for (int k = 0; k < 3; ++k) {
+            DU[k] = au * W[k] + plane * U[k];
+            DV[k] = av * W[k] + plane * V[k];
+        }
+        DU[3] = au * W[3] - plane * dot(U, S);
+        DV[3] = av * W[3] - plane * dot(V, S);
+        const double UU = dot(U, U), VV = dot(V, V), UV = dot(U, V);
+        const double gram = UU * VV - UV * UV;
+        if (!(std::fabs(gram) > 1e-30) || !(std::fabs(W[3]) > 1e-12)) {
+            delete p;
+            return fail(YKB_ERR_INVALID_GEOMETRY, "degenerate detector basis or source at the volume centre");
+        }
+        const double inv = 1.0 / gram, norm = 1.0 / W[3];
+        for (int k = 0; k < 4; ++k) {
+            vp[i * 12 + k] = static_cast<float>((DU[k] * VV - DV[k] * UV) * inv * norm);
+            vp[i * 12 + 4 + k] = static_cast<float>((-DU[k] * UV + DV[k] * UU) * inv * norm);
+            vp[i * 12 + 8 + k] = static_cast<float>(W[k] * norm);
+        }
+    }
+    const size_t rays = static_cast<size_t>(n_views) * nu * nv;
+    const size_t vol_bytes = volume_elems(*volume) * sizeof(float);
+    cudaError_t e;
+    if ((e = p->views.alloc(sizeof(JosephView) * n_views)) != cudaSuccess ||
+        (e = p->view_proj.alloc(sizeof(float) * vp.size())) != cudaSuccess ||
+        (e = p->rays.alloc(sizeof(float4) * rays)) != cudaSuccess ||
+        (e = p->lens.alloc(sizeof(float) * rays)) != cudaSuccess ||
+        (need_y && (e = p->slab_y.alloc(vol_bytes)) != cudaSuccess) ||
+        (need_x && (e = p->slab_x.alloc(vol_bytes)) != cudaSuccess)) {
+        delete p;
+        return cuda_status(e, "cudaMalloc (Joseph plan)");
+    }
+    if ((e = cudaMemcpy(p->views.ptr, p->host_views.data(), sizeof(JosephView) * n_views,
+             cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(p->view_proj.ptr, vp.data(), sizeof(float) * vp.size(),
+             cudaMemcpyHostToDevice)) != cudaSuccess) {
+        delete p;
+        return cuda_status(e, "cudaMemcpy (Joseph plan tables)");
+    }
+    // geometry-only ray table, built once on a private stream
+    cudaStream_t s = nullptr;
+    if ((e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)) != cudaSuccess) {
+        delete p;
+        return cuda_status(e, "cudaStreamCreate");
+    }
+    e = launch_joseph_ray_table(p->views.as<JosephView>(), n_views, nu, nv, p->rays.as<float4>(),
+        p->lens.as<float>(), s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+    if (e != cudaSuccess) {
+        delete p;
+        return cuda_status(e, "Joseph ray table");
+    }
+    *plan_out = p;
+    return YKB_OK;
+}
+
+YKB_API ykb_status ykb_joseph_plan_destroy(ykb_joseph_plan* plan)
+{
+    clear_error();
+    if (!plan) return YKB_OK;
+    DeviceGuard guard(plan->device);
+    delete plan;
+    return YKB_OK;
+}
+
+YKB_API size_t ykb_joseph_workspace_bytes(const ykb_joseph_plan* p)
+{
+    if (!p) return 0;
+    return p->views.bytes + p->view_proj.bytes + p->rays.bytes + p->lens.bytes +
+        p->slab_x.bytes + p->slab_y.bytes;
+}
+
+YKB_API ykb_status ykb_joseph_fp(ykb_joseph_plan* p, const float* d_volume, float* d_proj,
+    int accumulate, ykb_stream stream)
+{
+    clear_error();
+    if (!p) return fail(YKB_ERR_INVALID_CONFIG, "null plan");
+    if (!d_volume || !d_proj) return fail(YKB_ERR_INVALID_BUFFER, "null volume or projection buffer");
+    DeviceGuard guard(p->device);
+    const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const ykb_volume& v = p->volume;
+    YKB_TRY_CUDA(launch_joseph_transpose(d_volume, v.nx, v.ny, v.nz, p->slab_y.as<float>(),
+        p->slab_x.as<float>(), s));
+    const float* slabs[3] = {p->slab_x.as<float>(), p->slab_y.as<float>(), d_volume};
+    YKB_TRY_CUDA(launch_joseph_fp(slabs, p->views.as<JosephView>(), p->axes.data(), p->n_views,
+        p->nu, p->nv, d_proj, accumulate ? 1 : 0, s));
+    return YKB_OK;
+}
+
+YKB_API ykb_status ykb_joseph_bp(ykb_joseph_plan* p, const float* d_proj, float* d_volume,
+    int accumulate, ykb_stream stream)
+{
+    clear_error();
+    if (!p) return fail(YKB_ERR_INVALID_CONFIG, "null plan");
+    if (!d_volume || !d_proj) return fail(YKB_ERR_INVALID_BUFFER, "null volume or projection buffer");
+    DeviceGuard guard(p->device);
+    const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    YKB_TRY_CUDA(launch_joseph_bp(d_proj, p->rays.as<float4>(), p->lens.as<float>(),
+        p->view_proj.as<float>(), p->views.as<JosephView>(), p->n_views, p->nu, p->nv, p->volume,
+        d_volume, accumulate ? 1 : 0, s));
+    return YKB_OK;
+}
+
+} // extern "C"

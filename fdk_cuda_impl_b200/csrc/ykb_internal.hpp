@@ -1,0 +1,223 @@
+// Internal declarations shared by the host and CUDA translation units of
+// libykb.so.  Nothing here crosses the C-ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/ykb.h"
+
+namespace ykb {
+
+// --------------------------------------------------------------- errors ---
+void set_error(const std::string& msg);
+void clear_error();
+const char* last_error();
+
+// Returns YKB_ERR_CUDA (and records the message) when status is an error.
+ykb_status cuda_status(cudaError_t status, const char* what);
+
+#define YKB_TRY_CUDA(expr)                                                   \
+    do {                                                                     \
+        const cudaError_t ykb_e_ = (expr);                                   \
+        if (ykb_e_ != cudaSuccess) return ::ykb::cuda_status(ykb_e_, #expr); \
+    } while (0)
+
+// Device buffer owned by a plan (RAII; no exceptions).
+struct DeviceBuffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    DeviceBuffer() = default;
+    DeviceBuffer(const DeviceBuffer&) = delete;
+    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+    ~DeviceBuffer() { reset(); }
+    cudaError_t alloc(size_t n)
+    {
+        reset();
+        if (n == 0) return cudaSuccess;
+        const cudaError_t e = cudaMalloc(&ptr, n);
+        if (e == cudaSuccess) bytes = n; else ptr = nullptr;
+        return e;
+    }
+    void reset()
+    {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+    template <typename T> T* as() const { return static_cast<T*>(ptr); }
+};
+
+// Switches to a device for the lifetime of the object and restores the
+// caller's device afterwards.
+struct DeviceGuard {
+    int previous = -1;
+    explicit DeviceGuard(int device)
+    {
+        if (cudaGetDevice(&previous) != cudaSuccess) previous = -1;
+        if (previous != device) cudaSetDevice(device);
+    }
+    ~DeviceGuard()
+    {
+        int now = -1;
+        if (previous >= 0 && cudaGetDevice(&now) == cudaSuccess && now != previous)
+            cudaSetDevice(previous);
+    }
+};
+
+// ------------------------------------------------------------- geometry ---
+struct dvec3 { double x, y, z; };
+
+// Per-view FDK quantities derived in FP64 from the float geometry
+// (definitions of src/Reconstruction/Analytic/Circular/Flat/FDK/
+// YkFDKVecGeoDerived.hpp:58-304).
+struct FdkDerived {
+    double theta, dtheta, fscale;
+    double sid;     // source_to_axis_mm
+    double dsd;     // source_to_radial_detector_mm
+    double plane;   // source_to_detector_plane_mm
+    double off_u, off_v;
+    double du, dv;
+    dvec3 src, detS, detU, detV, normal, radial;
+    double UU, VV, UV, inv_gram;
+    int start_u;    // placement of the row inside the padded FFT row
+};
+
+bool derive_fdk_geometry(const ykb_cone_view* views, int n, int nu, int nv,
+    float scan_range, std::vector<FdkDerived>& out, std::string& why);
+
+int padded_fft_length(int nu);
+
+// Device-side per-view FDK coefficients (FP64).  Affine rows over world
+// coordinates (X, Y, Z, 1): u = cu.P/cd.P, v = cv.P/cd.P (pixel units,
+// pixel (0,0) at detS), radial depth = cr.P; wbase = SID^2 dtheta 2pi/range.
+struct alignas(16) FdkViewCoef {
+    double cu[4];
+    double cv[4];
+    double cd[4];
+    double cr[4];
+    double wbase;
+    double pad[3];
+};
+
+// Device-side per-view preweight + placement data.
+struct alignas(16) FdkPreweightView {
+    double src[4];
+    double detS[4];
+    double detU[4];
+    double detV[4];
+    double dsd;     // cosine-weight numerator
+    double wgeom;   // DSD / DSO / 2
+    int in_lo, in_hi;   // input samples [in_lo, in_hi) are placed in the padded row
+    int out_lo, out_hi; // outputs [out_lo, out_hi) fall inside the padded row
+};
+
+void build_fdk_coefficients(const std::vector<FdkDerived>& g, int nu,
+    std::vector<FdkViewCoef>& coef, std::vector<FdkPreweightView>& pw,
+    bool& axial);
+
+void build_ramp_kernel(int nu, double du, const ykb_filter& f,
+    std::vector<double>& h);
+
+// Joseph per-view data (FP64), volume-centred voxel units.
+struct alignas(16) JosephView {
+    double src[4];
+    double detS[4];
+    double detU[4];
+    double detV[4];
+    int axis;        // 0: X main axis, 1: Y, 2: Z
+    int n0, n1, n2;  // volume extents along (main, minor1, minor2)
+    double v0, v1, v2;  // voxel sizes (mm) along the same axes
+    double pad;
+};
+
+bool build_joseph_views(const ykb_cone_view* views, int n, int nu, int nv,
+    const ykb_volume& vol, std::vector<JosephView>& out, std::string& why);
+
+bool build_circular_flat(const ykb_circular_flat& spec, ykb_cone_view* out,
+    std::string& why);
+
+// -------------------------------------------------------------- kernels ---
+struct VolumeGrid {
+    int nx, ny, nz;
+    double vx, vy, vz;
+    double ox, oy, oz;  // centre of voxel (0,0,0), FP64
+};
+
+VolumeGrid make_grid(const ykb_volume& v);
+
+// FDK
+cudaError_t launch_fdk_preweight(const void* proj, int proj_dtype,
+    const FdkPreweightView* pw, int n_views, int nu, int nv, float* out,
+    cudaStream_t s);
+cudaError_t launch_fdk_ramp_fp32(const float* pw_rows, const float* h_dev,
+    const FdkPreweightView* pwv, int n_views, int nu, int nv, void* out,
+    int out_dtype, cudaStream_t s);
+cudaError_t launch_fdk_preweight_split_bf16(const void* proj, int proj_dtype,
+    const FdkPreweightView* pw, int n_views, int nu, int nv, int ld,
+    __nv_bfloat16* hi, __nv_bfloat16* lo, cudaStream_t s);
+cudaError_t launch_fdk_ramp_tcgen05(const __nv_bfloat16* a_hi,
+    const __nv_bfloat16* a_lo, const __nv_bfloat16* t_hi,
+    const __nv_bfloat16* t_lo, int rows, int nu, int ld,
+    const FdkPreweightView* pwv, int nv, __nv_bfloat16* out, int* err_flag,
+    cudaStream_t s);
+bool tcgen05_filter_supported(int nu);
+cudaError_t launch_fdk_backproject(const void* filtered, int dtype,
+    const FdkViewCoef* coef, int n_views, int nu, int nv,
+    const VolumeGrid& grid, bool axial, float* vol, int accumulate,
+    cudaStream_t s);
+
+// Joseph
+cudaError_t launch_joseph_transpose(const float* vol, int nx, int ny, int nz,
+    float* vol_yzx, float* vol_xzy, cudaStream_t s);
+cudaError_t launch_joseph_fp(const float* slabs[3], const JosephView* views,
+    const int* view_axis_host, int n_views, int nu, int nv, float* proj,
+    int accumulate, cudaStream_t s);
+cudaError_t launch_joseph_ray_table(const JosephView* views, int n_views,
+    int nu, int nv, float4* rays, float* lens, cudaStream_t s);
+cudaError_t launch_joseph_bp(const float* proj, const float4* rays,
+    const float* lens, const float* view_proj, const JosephView* views,
+    int n_views, int nu, int nv, const ykb_volume& vol, float* out,
+    int accumulate, cudaStream_t s);
+
+} // namespace ykb
+
+// Plan objects (opaque at the C-ABI).
+struct ykb_fdk_plan {
+    int device = 0;
+    int n_views = 0, nu = 0, nv = 0;
+    float scan_range = 0.f;
+    ykb_volume volume{};
+    ykb_filter filter{};
+    int precision = YKB_PRECISION_FP32;
+    bool axial = false;
+    bool tc_filter = false;
+    int batch_capacity = 0;      // views the workspace holds
+    int ld = 0;                  // leading dimension of the bf16 operand rows
+    std::vector<ykb::FdkDerived> derived;
+    ykb::DeviceBuffer coef;      // FdkViewCoef[n_views]
+    ykb::DeviceBuffer pwv;       // FdkPreweightView[n_views]
+    ykb::DeviceBuffer ramp;      // float[2*nu-1]
+    ykb::DeviceBuffer toeplitz_hi, toeplitz_lo;  // bf16 [nu][ld] (BF16 plans)
+    ykb::DeviceBuffer work_a;    // preweighted rows (float) or bf16 hi/lo
+    ykb::DeviceBuffer work_filtered;  // filtered projections (plan dtype)
+    ykb::DeviceBuffer err_flag;  // int, device-side error reporting
+};
+
+struct ykb_joseph_plan {
+    int device = 0;
+    int n_views = 0, nu = 0, nv = 0;
+    ykb_volume volume{};
+    std::vector<ykb::JosephView> host_views;
+    std::vector<int> axes;
+    ykb::DeviceBuffer views;     // JosephView[n]
+    ykb::DeviceBuffer view_proj; // float[n][12]: voxel-space 3x4 projection
+    ykb::DeviceBuffer rays;      // float4[n*nv*nu]: (a1, e1, a2, e2)
+    ykb::DeviceBuffer lens;      // float[n*nv*nu]: chord length per step
+    ykb::DeviceBuffer slab_y, slab_x;  // transposed volume copies
+};

@@ -1,0 +1,206 @@
+/*
+ * ykb.h -- C-ABI of the B200-native flat-panel circular cone-beam FDK and
+ * Joseph forward/back projector library (libykb.so).
+ *
+ * This is the boundary that replaces the reference's internal CUDA entry
+ * points for the path; the C++ Session layer (include/ykb_session.hpp, same
+ * names as YKCBCT's public YkReconstructionApi.hpp) and the torch extension
+ * (fdk_cuda_impl_b200) both call it.  Every entry point:
+ *   - takes plain pointers and sizes (device pointers unless stated),
+ *   - is ordered on the caller's CUDA stream (cudaStream_t passed as
+ *     ykb_stream) and does not synchronise unless stated,
+ *   - never aborts and never throws; it returns a ykb_status whose values
+ *     1..7 are the reference's YK::EApiErrorCode values
+ *     (include/YKCBCT/interface/YkReconstructionApi.hpp:72-81) and
+ *     ykb_last_error() returns the calling thread's last message.
+ * Layouts are the reference's: projections [view][v][u] and volumes
+ * [z][y][x], contiguous float32 (include/YKCBCT/interface/
+ * YkReconstructionTypes.hpp:38-44; doc/geometry-and-data.md).
+ */
+#ifndef YKB_H
+#define YKB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(_WIN32)
+#define YKB_API __declspec(dllexport)
+#else
+#define YKB_API __attribute__((visibility("default")))
+#endif
+
+typedef struct CUstream_st* ykb_stream; /* identical to cudaStream_t */
+
+typedef struct { float x, y, z, w; } ykb_float4;
+
+/* One view of flat cone-beam vector geometry; byte layout of
+ * YK::SConeProjGeomVec (include/YKCBCT/geometry/YkProjectionGeometry.hpp:12-18):
+ * pixel (u,v) centre = detS + u*detU + v*detV, angle.x = view angle (rad). */
+typedef struct {
+    ykb_float4 src;
+    ykb_float4 detS;
+    ykb_float4 detU;
+    ykb_float4 detV;
+    ykb_float4 angle;
+} ykb_cone_view;
+
+/* Volume grid; voxel (i,j,k) centre = center + (index - (n-1)/2) * vox,
+ * as YK::SVolGeom::origin() (include/YKCBCT/geometry/YkVolumeGeometry.hpp:9-55). */
+typedef struct {
+    int nx, ny, nz;
+    float vox_x, vox_y, vox_z;
+    float center_x, center_y, center_z;
+} ykb_volume;
+
+/* Ramp filter selection; members and enum values of YK::SAnalyticFilterParams /
+ * YK::EFdkFilter (include/YKCBCT/algorithms/analytic/YkAnalyticFilterParams.hpp:5-14). */
+typedef struct {
+    int type;      /* 0 None 1 RamLak 2 SheppLogan 3 Cosine 4 Hann 5 Hamming
+                      6 Blackman 7 Butterworth 8 Kaiser 9 Tukey */
+    float cutoff;  /* cycles/sample, (0, 0.5] */
+    float gain;
+    float butterworth_order;
+    float kaiser_beta;
+    float tukey_alpha;
+} ykb_filter;
+
+/* Regular circular orbit with a flat detector: YK::SRegularCircularScanSpec
+ * and YK::SFlatDetectorSpec (include/YKCBCT/geometry/YkGeometryBuilderTypes.hpp). */
+typedef struct {
+    int total_views;
+    int views_per_turn;
+    float start_angle_rad;
+    int rotation_direction; /* +1 / -1 */
+    float sid_mm;
+    float sdd_mm;
+    float z_mm;
+    float source_offset_mm[3];
+    int channels;
+    int rows;
+    float channel_size_mm;
+    float row_size_mm;
+    float offset_unv_mm[3]; /* U, N, V */
+    float tilt_u_rad;
+    float tilt_v_rad;
+    float tilt_n_rad;
+} ykb_circular_flat;
+
+typedef enum {
+    YKB_OK = 0,
+    YKB_ERR_INVALID_CONFIG = 1,    /* EApiErrorCode::InvalidConfig */
+    YKB_ERR_INVALID_GEOMETRY = 2,  /* EApiErrorCode::InvalidGeometry */
+    YKB_ERR_UNSUPPORTED = 3,       /* EApiErrorCode::UnsupportedCombination */
+    YKB_ERR_INVALID_BUFFER = 5,    /* EApiErrorCode::InvalidBuffer */
+    YKB_ERR_STREAMING_STATE = 6,   /* EApiErrorCode::StreamingStateError */
+    YKB_ERR_CUDA = 7,              /* EApiErrorCode::CudaError */
+    YKB_ERR_OUT_OF_MEMORY = 8
+} ykb_status;
+
+typedef enum {
+    YKB_PRECISION_FP32 = 0, /* FP32 ramp filter, FP32 filtered projections */
+    YKB_PRECISION_BF16 = 1  /* BF16 tensor-core Toeplitz filter with split
+                               hi/lo correction, BF16 filtered projections */
+} ykb_precision;
+
+typedef enum { YKB_DTYPE_F32 = 0, YKB_DTYPE_BF16 = 1 } ykb_dtype;
+
+typedef struct ykb_fdk_plan ykb_fdk_plan;
+typedef struct ykb_joseph_plan ykb_joseph_plan;
+
+/* Library version (major*10000 + minor*100 + patch). */
+YKB_API int ykb_version(void);
+
+/* Message of the last failed call on the calling thread ("" if none). */
+YKB_API const char* ykb_last_error(void);
+
+/* Regular scan range 2*pi*total_views/views_per_turn in float, as
+ * regularScanRangeRad (include/YKCBCT/interface/YkSystemReconstruction.hpp:22-28). */
+YKB_API float ykb_regular_scan_range(int total_views, int views_per_turn);
+
+/* Per-view flat geometry of a regular circular orbit; replaces
+ * buildCircularTrajectory + buildProjectionGeometry
+ * (include/YKCBCT/geometry/YkSystemGeometry.hpp:61-73,
+ * include/YKCBCT/geometry/YkModularGeometryBuilder.hpp:9-17).  Host only;
+ * out must hold spec->total_views entries (capacity). */
+YKB_API ykb_status ykb_build_circular_flat(const ykb_circular_flat* spec,
+    ykb_cone_view* out, int capacity);
+
+/* ---------------------------------------------------------------- FDK --- */
+
+/* Prepares an FDK plan for the full view sequence (host geometry, copied):
+ * derived geometry in FP64, projection coefficients, ramp kernel, device
+ * workspace.  Replaces FdkPipeline::prepareWithGeometry
+ * (src/Reconstruction/Analytic/Circular/Flat/FDK/YkFdkPipeline.hpp:344-383).
+ * scan_range_rad is the regular scan range (ykb_regular_scan_range). */
+YKB_API ykb_status ykb_fdk_plan_create(const ykb_cone_view* views, int n_views,
+    int nu, int nv, float scan_range_rad, const ykb_volume* volume,
+    const ykb_filter* filter, int precision, int device, ykb_fdk_plan** plan);
+
+YKB_API ykb_status ykb_fdk_plan_destroy(ykb_fdk_plan* plan);
+
+/* Cosine preweight + ramp filter + weighted backprojection of views
+ * [view_offset, view_offset+n_views) of d_proj ([n_views][nv][nu], dtype
+ * proj_dtype) into d_volume ([nz][ny][nx] float).  clear_output=1 zeroes the
+ * volume first, else the batch accumulates (streaming FDK).  Replaces
+ * FdkPipeline::enqueueBatch (YkFdkPipeline.hpp:388-488). */
+YKB_API ykb_status ykb_fdk_execute(ykb_fdk_plan* plan, const void* d_proj,
+    int proj_dtype, int view_offset, int n_views, float* d_volume,
+    int clear_output, ykb_stream stream);
+
+/* Stage entry: preweight + ramp filter only; d_filtered receives
+ * [n_views][nv][nu] in the plan's filtered dtype (float for FP32 plans,
+ * bf16 for BF16 plans).  Replaces PreweightProcessor::apply +
+ * FilterProcessor::apply (.../FDK/YkFDKPreWeightProcessor.hpp,
+ * .../FDK/YkFDKFilterProcessor.hpp:84-122). */
+YKB_API ykb_status ykb_fdk_filter(ykb_fdk_plan* plan, const void* d_proj,
+    int proj_dtype, int view_offset, int n_views, void* d_filtered,
+    ykb_stream stream);
+
+/* Stage entry: weighted backprojection of already filtered projections
+ * (dtype filtered_dtype).  Replaces BpProcessor::apply / fdk_bp_kernel
+ * (.../FDK/YkBackProjectProcessor.hpp:53-67,
+ * .../FDK/kernels/YkFDKBpKernels.cu:112-209,336-381). */
+YKB_API ykb_status ykb_fdk_backproject(ykb_fdk_plan* plan,
+    const void* d_filtered, int filtered_dtype, int view_offset, int n_views,
+    float* d_volume, int clear_output, ykb_stream stream);
+
+/* Bytes of device workspace the plan holds (introspection). */
+YKB_API size_t ykb_fdk_workspace_bytes(const ykb_fdk_plan* plan);
+
+/* ------------------------------------------------------------- Joseph --- */
+
+/* Prepares the Joseph projector pair for a view sequence.  Replaces
+ * ForwardOperator/BackOperator::prepare for FP_Joseph/BP_Joseph
+ * (src/common/YkProjectionOperators.hpp:120-135,229-240). */
+YKB_API ykb_status ykb_joseph_plan_create(const ykb_cone_view* views,
+    int n_views, int nu, int nv, const ykb_volume* volume, int device,
+    ykb_joseph_plan** plan);
+
+YKB_API ykb_status ykb_joseph_plan_destroy(ykb_joseph_plan* plan);
+
+/* d_proj ([n][nv][nu]) = (accumulate ? d_proj : 0) + A d_volume.  Replaces
+ * ForwardOperator::apply with FP_Joseph (src/common/YkProjectionOperators.hpp:
+ * 138-180) and fp_joseph_launch (src/FlatFpBp/FP/kernels/YkFPKernels.cu:530-565). */
+YKB_API ykb_status ykb_joseph_fp(ykb_joseph_plan* plan, const float* d_volume,
+    float* d_proj, int accumulate, ykb_stream stream);
+
+/* d_volume = (accumulate ? d_volume : 0) + A^T d_proj, the exact transpose of
+ * ykb_joseph_fp, computed voxel-driven without atomics.  Replaces
+ * BackOperator::apply with BP_Joseph (src/common/YkProjectionOperators.hpp:
+ * 293-298) and joseph_bp_launch (src/FlatFpBp/BP/kernels/YkBPJosephKernel.cu:
+ * 226-266). */
+YKB_API ykb_status ykb_joseph_bp(ykb_joseph_plan* plan, const float* d_proj,
+    float* d_volume, int accumulate, ykb_stream stream);
+
+/* Bytes of device workspace the plan holds (introspection). */
+YKB_API size_t ykb_joseph_workspace_bytes(const ykb_joseph_plan* plan);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* YKB_H */

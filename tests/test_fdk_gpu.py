@@ -1,0 +1,149 @@
+"""GPU parity tests of the FDK path (through the C-ABI) against the FP64 oracle.
+
+Tolerances: FP32 plans rel RMSE <= 1e-5 against the FP64 oracle (the FP32
+target); BF16 plans rel RMSE <= 1e-3; stage outputs as stated per test.
+"""
+import numpy as np
+import pytest
+
+from tests import cases as K
+
+pytestmark = pytest.mark.gpu
+
+FP32_TOL = 1e-5
+BF16_TOL = 1e-3
+
+
+def _run_case(oracle, case, precision="fp32", proj_dtype="f32", ph=None):
+    import torch
+    from fdk_cuda_impl_b200.projectors import FdkPlan
+    views = case.scan.views()
+    p = K.projections(oracle, case, views, ph)
+    if proj_dtype == "bf16":
+        pt = torch.from_numpy(p).to(torch.bfloat16)
+        p = pt.float().numpy()
+        dev_p = pt.cuda()
+    else:
+        dev_p = torch.from_numpy(p).cuda()
+    plan = FdkPlan(views, case.scan.channels, case.scan.rows, case.scan.scan_range, case.grid,
+                   case.filt, precision=precision)
+    out = plan.execute(dev_p).cpu().numpy()
+    ref = oracle.fdk(views, case.scan.channels, case.scan.rows, case.scan.scan_range,
+                     K.oracle_volume(oracle, case.grid), K.oracle_filter(oracle, case.filt), p)
+    return out, ref, plan, views, p
+
+
+def test_fdk_small_fp32(oracle, cuda_device):
+    out, ref, *_ = _run_case(oracle, K.c1_small())
+    assert np.isfinite(out).all()
+    assert K.rel_rmse(out, ref) <= FP32_TOL
+
+
+def test_fdk_c1_full_fp32(oracle, cuda_device):
+    # 128^3 @ 0.5 mm, 180 views, 192x128 @ 0.8 mm, 500/1000 mm, Ram-Lak
+    out, ref, *_ = _run_case(oracle, K.c1())
+    assert K.rel_rmse(out, ref) <= FP32_TOL
+
+
+def test_fdk_tilted_odd_sizes(oracle, cuda_device):
+    # detector tilt + offsets + source offset + off-centre anisotropic grid:
+    # exercises the general (non-axial) backprojection path
+    out, ref, *_ = _run_case(oracle, K.odd_case())
+    assert K.rel_rmse(out, ref) <= FP32_TOL
+
+
+@pytest.mark.parametrize("kind", ["none", "shepplogan", "cosine", "hamming", "blackman",
+                                  "butterworth", "kaiser", "tukey"])
+def test_fdk_windows(oracle, cuda_device, kind):
+    case = K.c1_small()
+    case.filt = K.RampFilter.named(kind, cutoff=0.45)
+    out, ref, *_ = _run_case(oracle, case)
+    assert K.rel_rmse(out, ref) <= FP32_TOL
+
+
+def test_fdk_filter_stage(oracle, cuda_device):
+    import torch
+    from fdk_cuda_impl_b200.projectors import FdkPlan
+    case = K.c1_small()
+    views = case.scan.views()
+    p = K.projections(oracle, case, views)
+    plan = FdkPlan(views, 96, 64, case.scan.scan_range, case.grid, case.filt)
+    got = plan.filter(torch.from_numpy(p).cuda()).cpu().numpy()
+    ref = oracle.fdk_filter(views, 96, 64, case.scan.scan_range,
+                            K.oracle_filter(oracle, case.filt), p)
+    assert K.rel_rmse(got, ref) <= 1e-6
+
+
+def test_fdk_backproject_stage(oracle, cuda_device):
+    import torch
+    from fdk_cuda_impl_b200.projectors import FdkPlan
+    case = K.c1_small()
+    views = case.scan.views()
+    f = oracle.normal((60, 64, 96), 21)
+    plan = FdkPlan(views, 96, 64, case.scan.scan_range, case.grid, case.filt)
+    got = plan.backproject(torch.from_numpy(f).cuda()).cpu().numpy()
+    ref = oracle.fdk_backproject(views, 96, 64, case.scan.scan_range,
+                                 K.oracle_volume(oracle, case.grid), f.astype(np.float64))
+    assert K.rel_rmse(got, ref) <= FP32_TOL
+
+
+def test_fdk_streaming_batches(oracle, cuda_device):
+    # fdk/batch-consistency (Yktest/test_pipeline_smoke.cpp:2077-2122): a run
+    # split into contiguous batches equals the full run (pin: max diff < 1e-4)
+    import torch
+    from fdk_cuda_impl_b200.projectors import FdkPlan
+    case = K.c1_small()
+    views = case.scan.views()
+    p = torch.from_numpy(K.projections(oracle, case, views)).cuda()
+    plan = FdkPlan(views, 96, 64, case.scan.scan_range, case.grid, case.filt)
+    full = plan.execute(p).clone()
+    vol = torch.full(case.grid.shape, 123.0, device="cuda")
+    plan.execute(p[0:5], vol, view_offset=0, clear=True)
+    plan.execute(p[5:23], vol, view_offset=5, clear=False)
+    plan.execute(p[23:], vol, view_offset=23, clear=False)
+    diff = (vol - full).abs().max().item()
+    assert diff < 1e-4
+    assert K.rel_rmse(vol.cpu().numpy(), full.cpu().numpy()) < 1e-6
+
+
+def test_fdk_bf16_form(oracle, cuda_device):
+    out, ref, *_ = _run_case(oracle, K.c1_small(), precision="bf16")
+    assert K.rel_rmse(out, ref) <= BF16_TOL
+
+
+def test_fdk_bf16_projection_input(oracle, cuda_device):
+    out, ref, *_ = _run_case(oracle, K.c1_small(), proj_dtype="bf16")
+    assert K.rel_rmse(out, ref) <= FP32_TOL
+
+
+def test_fdk_extreme_detector_offset(oracle, cuda_device):
+    # principal point far outside the detector: the padded FFT row drops
+    # samples; the Toeplitz form must drop exactly the same ones
+    case = K.c1_small()
+    case.scan.offset_unv_mm = (70.0, 0.0, 5.0)
+    out, ref, *_ = _run_case(oracle, case)
+    d = oracle.fdk_derived(case.scan.views(), 96, 64, case.scan.scan_range)
+    N = 256
+    assert ((d[:, 10] < 0) | (d[:, 10] + 96 > N)).any()  # masks are active
+    assert K.rel_rmse(out, ref) <= FP32_TOL
+
+
+def test_fdk_noisy_short_views(oracle, cuda_device):
+    case = K.c1_small()
+    case.noise_i0 = 5e4
+    out, ref, *_ = _run_case(oracle, case)
+    assert K.rel_rmse(out, ref) <= FP32_TOL
+
+
+def test_fdk_errors_are_status_codes(cuda_device, oracle):
+    import torch
+    from fdk_cuda_impl_b200 import _lib as L
+    from fdk_cuda_impl_b200.projectors import FdkPlan
+    case = K.c1_small()
+    plan = FdkPlan(case.scan.views(), 96, 64, case.scan.scan_range, case.grid, case.filt)
+    p = torch.zeros((10, 64, 96), device="cuda")
+    with pytest.raises(L.YkbError) as e:
+        plan.execute(p, view_offset=55)
+    assert e.value.code == L.ERR_INVALID_CONFIG
+    # the context stays usable
+    assert torch.isfinite(plan.execute(p, view_offset=50)).all()
