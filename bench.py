@@ -121,7 +121,7 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
 
 
-def cpu_baseline(n_views_sample=24, z_slab=16):
+def cpu_baseline(n_views_sample=96, z_slab=64):
     """FP64 oracle FDK on a bounded sample of the same workload: a subset of
     views (full 768x768 projections: preweight + filter) backprojected into
     a z-slab of the 512^3 volume.  Returns GUPS on the host cores."""
@@ -149,10 +149,10 @@ def run_reference(args):
         return
     from oracle import oracle as O
     for _ in range(args.warmup):
-        cpu_baseline(n_views_sample=4, z_slab=8)
+        cpu_baseline(n_views_sample=8, z_slab=8)
     vals = []
     for _ in range(args.steps):
-        vals.append(cpu_baseline(n_views_sample=8, z_slab=8))
+        vals.append(cpu_baseline(n_views_sample=36, z_slab=32))
     value = sum(v["value"] for v in vals) / len(vals)
     ms = UPDATES / (value * 1e9) * 1e3
     cb = dict(vals[-1])

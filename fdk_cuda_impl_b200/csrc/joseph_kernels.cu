@@ -81,7 +81,8 @@ __global__ void __launch_bounds__(128) joseph_fp_kernel(const float* __restrict_
     if (iu >= nu || iv >= nv) return;
     const JosephView& j = views[k];
     const RayParams r = ray_params(j, iu, iv);
-    float acc = 0.f;
+    // FP64 ray sum: keeps the adjoint identity at the 1e-7 level
+    double acc = 0.0;
     if (r.ok) {
         int lo = 0, hi = j.n0 - 1;
         slice_range(r.a1, r.e1, j.n1, j.n0, lo, hi);
@@ -105,12 +106,13 @@ __global__ void __launch_bounds__(128) joseph_fp_kernel(const float* __restrict_
             const float p10 = (c1b && c2a) ? __ldg(sl + ra + i1 + 1) : 0.f;
             const float p01 = (c1a && c2b) ? __ldg(sl + rb + i1) : 0.f;
             const float p11 = (c1b && c2b) ? __ldg(sl + rb + i1 + 1) : 0.f;
-            acc += (1.f - w2) * ((1.f - w1) * p00 + w1 * p10) + w2 * ((1.f - w1) * p01 + w1 * p11);
+            acc += static_cast<double>((1.f - w2) * ((1.f - w1) * p00 + w1 * p10) +
+                w2 * ((1.f - w1) * p01 + w1 * p11));
         }
         acc *= r.len;
     }
     float* dst = proj + (static_cast<long>(k) * nv + iv) * nu + iu;
-    *dst = accumulate ? *dst + acc : acc;
+    *dst = accumulate ? static_cast<float>(*dst + acc) : static_cast<float>(acc);
 }
 
 __global__ void __launch_bounds__(128) joseph_ray_table_kernel(const JosephView* __restrict__ views,
@@ -174,7 +176,7 @@ __global__ void __launch_bounds__(256) joseph_bp_kernel(const float* __restrict_
     const int z = blockIdx.z;
     if (x >= nx || y >= ny) return;
     const long view_elems = static_cast<long>(nu) * nv;
-    float acc = 0.f;
+    double acc = 0.0;  // FP64 voxel sum (see joseph_fp_kernel)
     for (int k = 0; k < n_views; ++k) {
         const JosephView& j = views[k];
         int s, j1, j2;
@@ -219,12 +221,12 @@ __global__ void __launch_bounds__(256) joseph_bp_kernel(const float* __restrict_
                 const float wa = (i1 == j1) ? 1.f - w1 : ((i1 + 1 == j1) ? w1 : 0.f);
                 const float wb = (i2 == j2) ? 1.f - w2 : ((i2 + 1 == j2) ? w2 : 0.f);
                 const float w = wa * wb;
-                if (w != 0.f) acc = fmaf(__ldg(proj + idx) * __ldg(lens + idx), w, acc);
+                if (w != 0.f) acc += static_cast<double>(__ldg(proj + idx) * __ldg(lens + idx) * w);
             }
         }
     }
     float* dst = vol + (static_cast<long>(z) * ny + y) * nx + x;
-    *dst = accumulate ? *dst + acc : acc;
+    *dst = accumulate ? static_cast<float>(*dst + acc) : static_cast<float>(acc);
 }
 
 } // namespace
