@@ -31,6 +31,12 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+# the workload the metric is quoted on, and a small case of the same kernels
+# (inputs still larger than L2) used for profiler captures
+CONFIGS = {
+    "c2": dict(N_VOX=512, N_VIEWS=720, N_DET=768, VOX_MM=0.25, PIX_MM=0.4),
+    "small": dict(N_VOX=256, N_VIEWS=360, N_DET=384, VOX_MM=0.5, PIX_MM=0.8),
+}
 N_VOX = 512
 N_VIEWS = 720
 N_DET = 768
@@ -43,6 +49,15 @@ UPDATES = N_VOX ** 3 * N_VIEWS
 WORKLOAD = "fdk-512^3-720v-768^2"
 
 
+def select_config(name: str) -> None:
+    global N_VOX, N_VIEWS, N_DET, VOX_MM, PIX_MM, UPDATES, WORKLOAD
+    c = CONFIGS[name]
+    N_VOX, N_VIEWS, N_DET, VOX_MM, PIX_MM = (c["N_VOX"], c["N_VIEWS"], c["N_DET"], c["VOX_MM"],
+                                             c["PIX_MM"])
+    UPDATES = N_VOX ** 3 * N_VIEWS
+    WORKLOAD = f"fdk-{N_VOX}^3-{N_VIEWS}v-{N_DET}^2"
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -51,6 +66,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-bf16", action="store_true")
+    ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
     return ap.parse_args()
 
 
@@ -171,6 +187,7 @@ def run_reference(args):
 
 def main():
     args = parse()
+    select_config(args.config)
     if args.impl == "reference":
         run_reference(args)
         return
