@@ -171,6 +171,23 @@ YKB_API ykb_status ykb_fdk_backproject(ykb_fdk_plan* plan,
 /* Bytes of device workspace the plan holds (introspection). */
 YKB_API size_t ykb_fdk_workspace_bytes(const ykb_fdk_plan* plan);
 
+/* The preweight + ramp filter stage of ykb_fdk_filter for callers that
+ * cannot call cudaMalloc (an application whose memory pool owns the GPU,
+ * a real-time loop that forbids allocation after start-up): no plan and no
+ * device allocation.  This entry point has no counterpart in the reference.
+ * Geometry and filter come from the host arguments (as ykb_fdk_plan_create
+ * takes them); d_proj holds [n_views][nv][nu] (proj_dtype), d_filtered
+ * receives [n_views][nv][nu] float.  Scratch is one fixed 32 MiB device
+ * array inside the library, present on every GPU that loads it until exit;
+ * limits: nu <= 8192, n_views <= 16384, nu*nv*4 bytes <= 31.8 MiB per view,
+ * else YKB_ERR_INVALID_CONFIG.  The first call on a device looks up that
+ * device's scratch address (make it before any stream capture).  All calls
+ * share the one array: calls that overlap on the GPU (different streams,
+ * without ordering between them) race and corrupt each other. */
+YKB_API ykb_status ykb_fdk_filter_static(const ykb_cone_view* views,
+    int n_views, int nu, int nv, float scan_range_rad, const ykb_filter* filter,
+    const void* d_proj, int proj_dtype, float* d_filtered, ykb_stream stream);
+
 /* ------------------------------------------------------------- Joseph --- */
 
 /* Prepares the Joseph projector pair for a view sequence.  Replaces
