@@ -78,6 +78,7 @@ SIGNATURES = {
     "ykb_fdk_filter": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_int, _P, _P]),
     "ykb_fdk_backproject": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_int, _P, C.c_int, _P]),
     "ykb_fdk_workspace_bytes": (C.c_size_t, [_P]),
+    "ykb_fdk_check": (C.c_int, [_P, _P]),
     "ykb_fdk_filter_static": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_float, C.POINTER(Filter),
                                         _P, C.c_int, _P, _P]),
     "ykb_joseph_plan_create": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.POINTER(Volume),

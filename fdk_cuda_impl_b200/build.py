@@ -80,7 +80,7 @@ def build(verbose: bool = False) -> str:
     newest = max(os.path.getmtime(o) for o in objs)
     if not os.path.exists(LIB) or os.path.getmtime(LIB) < newest:
         tmp = LIB + ".tmp"
-        cmd = [nvcc, *ARCH, "-shared", "-o", tmp, *objs, "-lcuda"]
+        cmd = [nvcc, *ARCH, "-shared", "-o", tmp, *objs]
         res = subprocess.run(cmd, capture_output=True, text=True)
         if res.returncode != 0:
             raise RuntimeError(f"link failed:\n{res.stdout}\n{res.stderr}")

@@ -1,0 +1,600 @@
+// FDK weighted backprojection with TMA-staged projection tiles (sm_100a).
+//
+// Same arithmetic as fdk_bp_kernel in fdk_kernels.cu (the math of
+// .../FDK/kernels/YkFDKBpKernels.cu:112-209 with exact software bilinear
+// weights), organised for Blackwell:
+//   * a CTA owns a 16x16x32 voxel tile; each of its 256 consumer threads walks
+//     a 32-voxel z-column and keeps the 32 sums in registers over all views;
+//   * one producer warp computes, per view, the detector box covering the
+//     tile's footprint (+1 bilinear tap, +1 pixel margin) and loads it with
+//     cp.async.bulk.tensor (3D tile mode, this GPU's memory only, no
+//     multicast) into a ring of shared-memory stages guarded by full/empty
+//     mbarriers.  Out-of-detector box elements are zero-filled by TMA, which
+//     is the reference's Border addressing;
+//   * consumers read the four taps from shared memory without bounds checks:
+//     the box is sized by a pre-pass over all (tile, view) pairs with the same
+//     footprint function, and each (column, view) checks its end points.
+// Every mbarrier wait is bounded (~2 s of %globaltimer); a timeout sets the
+// plan's error word, stops the CTA and drains the copies in flight.
+#include "ykb_internal.hpp"
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <mutex>
+
+namespace ykb {
+namespace {
+
+constexpr int TX = 16, TY = 16, ZT = 32;
+constexpr int NCONS = TX * TY;          // consumer threads
+constexpr int NCWARPS = NCONS / 32;
+constexpr int NTHREADS = NCONS + 32;    // + producer warp
+constexpr unsigned long long kWaitNs = 2000000000ull;
+
+// error word bits
+constexpr int kErrTimeout = 1;
+constexpr int kErrFootprint = 2;
+constexpr int kErrAlign = 4;
+
+// a TMA tile copy writes shared memory at 128-byte aligned addresses: each
+// stage starts on a 128-byte boundary
+__host__ __device__ constexpr int stage_stride_floats(int bw, int bh)
+{
+    return (bw * bh + 31) / 32 * 32;
+}
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+                 "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok) : "r"(smem_addr(bar)), "r"(parity) : "memory");
+    return ok != 0;
+}
+
+// bounded wait: false after ~2 s
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
+{
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    while (!mbar_try_wait(bar, parity))
+        if (global_ns() - t0 > kWaitNs) return false;
+    return true;
+}
+
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar,
+    int x, int y, int z)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4}], [%5];"
+        ::"r"(smem_addr(dst)), "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_addr(bar)) : "memory");
+}
+
+__device__ __forceinline__ double rcp64(double x)
+{
+    double r = static_cast<double>(__frcp_rn(static_cast<float>(x)));
+    return r * (2.0 - x * r);
+}
+
+// Packed FP32 pairs (sm_100 f32x2 arithmetic): two z-voxels per instruction.
+typedef unsigned long long f2;
+__device__ __forceinline__ f2 f2pack(float lo, float hi)
+{
+    f2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void f2unpack(f2 v, float& lo, float& hi)
+{
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f2 f2fma(f2 a, f2 b, f2 c)
+{
+    f2 d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ f2 f2add(f2 a, f2 b)
+{
+    f2 d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f2 f2sub(f2 a, f2 b)
+{
+    f2 d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+template <int OFF>
+__device__ __forceinline__ float lds(uint32_t addr)
+{
+    float v;
+    asm("ld.shared.f32 %0, [%1+%2];" : "=f"(v) : "r"(addr), "n"(OFF));
+    return v;
+}
+
+// floor by rounding: t = (v - 1/2) + 1.5*2^23 holds round(v - 1/2) in its
+// low mantissa bits for |v| < 2^22, and round(v - 1/2) = floor(v) except at
+// integer v, where it may give v - 1 with fraction 1 -- the same bilinear
+// value.  The map v -> t is monotonic.
+constexpr float kRoundMagic = 12582912.0f;
+constexpr uint32_t kRoundMagicBits = 0x4B400000u;
+
+// Per (column, view) terms of the axial path, independent of the staged box:
+// computed one view ahead so their FP64 latency overlaps the previous view.
+struct ColTerms {
+    float u, vbq, vs, w;
+};
+
+__device__ __forceinline__ ColTerms axial_terms(const FdkViewCoef& c, double X, double Y,
+    double Z0, double vz)
+{
+    const double den = fma(c.cd[1], Y, fma(c.cd[0], X, c.cd[3]));
+    const double rd = rcp64(den);
+    const double un = fma(c.cu[1], Y, fma(c.cu[0], X, c.cu[3]));
+    const double vn = fma(c.cv[2], Z0, fma(c.cv[1], Y, fma(c.cv[0], X, c.cv[3])));
+    const double dep = fma(c.cr[1], Y, fma(c.cr[0], X, c.cr[3]));
+    const double rdep = rcp64(dep);
+    ColTerms t;
+    t.u = static_cast<float>(un * rd);
+    t.vbq = static_cast<float>(vn * rd - 0.5);
+    t.vs = static_cast<float>(c.cv[2] * vz * rd);
+    t.w = static_cast<float>(c.wbase * rdep * rdep);
+    return t;
+}
+
+// Detector box of a voxel tile for one view: columns [c0, c1], rows [r0, r1]
+// covering every bilinear tap of the tile's voxel centres with two pixels of
+// margin each side, c0 rounded down to the TMA alignment (16 bytes).  The
+// pre-pass and the producer evaluate the same corners with the same code.
+struct Box { int c0, c1, r0, r1; };
+
+__device__ __forceinline__ void corner_uv(const FdkViewCoef& c, double X, double Y, double Z,
+    double& u, double& v)
+{
+    const double den = fma(c.cd[2], Z, fma(c.cd[1], Y, fma(c.cd[0], X, c.cd[3])));
+    const double r = rcp64(den);
+    u = fma(c.cu[2], Z, fma(c.cu[1], Y, fma(c.cu[0], X, c.cu[3]))) * r;
+    v = fma(c.cv[2], Z, fma(c.cv[1], Y, fma(c.cv[0], X, c.cv[3]))) * r;
+}
+
+__device__ __forceinline__ Box box_from_range(double umin, double umax, double vmin, double vmax)
+{
+    umin = fmax(umin, -1e8); umax = fmin(umax, 1e8);
+    vmin = fmax(vmin, -1e8); vmax = fmin(vmax, 1e8);
+    Box b;
+    b.c0 = (static_cast<int>(floor(umin)) - 2) & ~3;
+    b.c1 = static_cast<int>(floor(umax)) + 3;
+    b.r0 = static_cast<int>(floor(vmin)) - 2;
+    b.r1 = static_cast<int>(floor(vmax)) + 3;
+    return b;
+}
+
+struct TileGeom {
+    double x0, x1, y0, y1, z0, z1;
+};
+
+__device__ __forceinline__ TileGeom tile_geom(const VolumeGrid& g, int bx, int by, int bz)
+{
+    TileGeom t;
+    const int xa = bx * TX, ya = by * TY, za = bz * ZT;
+    t.x0 = g.ox + xa * g.vx;
+    t.x1 = g.ox + min(xa + TX - 1, g.nx - 1) * g.vx;
+    t.y0 = g.oy + ya * g.vy;
+    t.y1 = g.oy + min(ya + TY - 1, g.ny - 1) * g.vy;
+    t.z0 = g.oz + za * g.vz;
+    t.z1 = g.oz + (za + ZT - 1) * g.vz;  // all ZT slices are evaluated
+    return t;
+}
+
+// Pre-pass: largest box over all (tile, view) pairs.
+__global__ void box_extent_kernel(const FdkViewCoef* __restrict__ coef, int n_views, VolumeGrid g,
+    int tiles_x, int tiles_y, int tiles_z, int* __restrict__ out)
+{
+    const long n = static_cast<long>(tiles_x) * tiles_y * tiles_z * n_views;
+    int w = 0, h = 0;
+    for (long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long>(gridDim.x) * blockDim.x) {
+        const int k = static_cast<int>(i % n_views);
+        const long t = i / n_views;
+        const int bx = static_cast<int>(t % tiles_x);
+        const int by = static_cast<int>((t / tiles_x) % tiles_y);
+        const int bz = static_cast<int>(t / (static_cast<long>(tiles_x) * tiles_y));
+        const TileGeom tg = tile_geom(g, bx, by, bz);
+        double umin = 1e300, umax = -1e300, vmin = 1e300, vmax = -1e300;
+        for (int q = 0; q < 8; ++q) {
+            double u, v;
+            corner_uv(coef[k], (q & 1) ? tg.x1 : tg.x0, (q & 2) ? tg.y1 : tg.y0,
+                (q & 4) ? tg.z1 : tg.z0, u, v);
+            umin = fmin(umin, u); umax = fmax(umax, u);
+            vmin = fmin(vmin, v); vmax = fmax(vmax, v);
+        }
+        const Box b = box_from_range(umin, umax, vmin, vmax);
+        w = max(w, b.c1 - b.c0 + 1);
+        h = max(h, b.r1 - b.r0 + 1);
+    }
+    atomicMax(out, w);
+    atomicMax(out + 1, h);
+}
+
+template <int BW, bool AXIAL>
+__global__ void __launch_bounds__(NTHREADS, 3) fdk_bp_tma_kernel(const __grid_constant__ CUtensorMap map,
+    const FdkViewCoef* __restrict__ coef, int n_views, VolumeGrid g, int BH, int stages,
+    float* __restrict__ vol, int accumulate, int* __restrict__ err)
+{
+    extern __shared__ unsigned char smem_raw[];
+    // 128-byte aligned base (the launch requests 128 bytes of slack)
+    unsigned char* smem = reinterpret_cast<unsigned char*>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~static_cast<uintptr_t>(127));
+    const int stage_floats = stage_stride_floats(BW, BH);
+    const uint32_t box_bytes = static_cast<uint32_t>(BW * BH * sizeof(float));
+    const size_t ring_bytes = static_cast<size_t>(stage_floats) * sizeof(float) * stages;
+    float* ring = reinterpret_cast<float*>(smem);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + ring_bytes);
+    uint64_t* empty = full + stages;
+    int4* boxes = reinterpret_cast<int4*>(empty + stages);
+    int* abort_ptr = reinterpret_cast<int*>(boxes + stages);
+    int& abort_flag = *abort_ptr;
+
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    if (tid == 0) {
+        abort_flag = 0;
+        if ((smem_addr(full) & 7u) != 0 || (smem_addr(ring) & 127u) != 0) {
+            atomicOr(err, kErrAlign);
+            abort_flag = 1;
+        }
+        for (int s = 0; s < stages; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], NCWARPS);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (abort_flag) return;
+    const TileGeom tg = tile_geom(g, blockIdx.x, blockIdx.y, blockIdx.z);
+
+    if (warp == NCWARPS) {
+        // ------------------------------------------------------ producer ---
+        // lanes 0..7 project one tile corner each; lane 0 owns the barriers
+        int issued = 0;
+        bool ok = true;
+        for (int k = 0; k < n_views; ++k) {
+            const int s = k % stages;
+            const int use = k / stages;
+            int go = 1;
+            if (lane == 0) {
+                if (use > 0 && !mbar_wait(&empty[s], (use - 1) & 1)) go = 0;
+                if (*(volatile int*)&abort_flag) go = 0;
+            }
+            go = __shfl_sync(0xffffffffu, go, 0);
+            if (!go) { ok = false; break; }
+            double umin = 1e300, umax = -1e300, vmin = 1e300, vmax = -1e300;
+            if (lane < 8) {
+                corner_uv(coef[k], (lane & 1) ? tg.x1 : tg.x0, (lane & 2) ? tg.y1 : tg.y0,
+                    (lane & 4) ? tg.z1 : tg.z0, umin, vmin);
+                umax = umin; vmax = vmin;
+            }
+#pragma unroll
+            for (int o = 4; o > 0; o >>= 1) {
+                umin = fmin(umin, __shfl_xor_sync(0xffffffffu, umin, o));
+                umax = fmax(umax, __shfl_xor_sync(0xffffffffu, umax, o));
+                vmin = fmin(vmin, __shfl_xor_sync(0xffffffffu, vmin, o));
+                vmax = fmax(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+            }
+            int aligned = 1;
+            if (lane == 0) {
+                const Box b = box_from_range(umin, umax, vmin, vmax);
+                float* dst = ring + static_cast<size_t>(s) * stage_floats;
+                if ((smem_addr(dst) & 127u) != 0 || (b.c0 & 3) != 0) {
+                    aligned = 0;  // never issue a copy the hardware would reject
+                } else {
+                    boxes[s] = make_int4(b.c0, b.r0, b.c1, b.r1);
+                    mbar_arrive_expect_tx(&full[s], box_bytes);
+                    tma_load_3d(dst, &map, &full[s], b.c0, b.r0, k);
+                }
+            }
+            aligned = __shfl_sync(0xffffffffu, aligned, 0);
+            if (!aligned) {
+                if (lane == 0) atomicOr(err, kErrAlign);
+                ok = false;
+                break;
+            }
+            issued = k + 1;
+        }
+        if (!ok && lane == 0) {
+            atomicOr(err, kErrTimeout);
+            *(volatile int*)&abort_flag = 1;
+            // drain: every issued copy must land before the CTA exits
+            const int first = max(0, issued - stages);
+            for (int k = first; k < issued; ++k) mbar_wait(&full[k % stages], (k / stages) & 1);
+        }
+        return;
+    }
+
+    // --------------------------------------------------------- consumers ---
+    const int lx = tid % TX, ly = tid / TX;
+    const int x = blockIdx.x * TX + lx, y = blockIdx.y * TY + ly;
+    const int z0 = blockIdx.z * ZT;
+    const bool active = x < g.nx && y < g.ny;
+    const double X = g.ox + x * g.vx, Y = g.oy + y * g.vy, Z0 = g.oz + z0 * g.vz;
+    float acc[ZT];
+#pragma unroll
+    for (int i = 0; i < ZT; ++i) acc[i] = 0.f;
+    f2 acc2[ZT / 2];
+#pragma unroll
+    for (int j = 0; j < ZT / 2; ++j) acc2[j] = 0ull;
+    bool bad = false;
+    ColTerms cur{};
+    if (AXIAL) cur = axial_terms(coef[0], X, Y, Z0, g.vz);
+
+    for (int k = 0; k < n_views; ++k) {
+        const int s = k % stages;
+        if (!mbar_wait(&full[s], (k / stages) & 1)) {
+            atomicOr(err, kErrTimeout);
+            *(volatile int*)&abort_flag = 1;
+            return;
+        }
+        const int4 b = boxes[s];
+        const float* S = ring + static_cast<size_t>(s) * stage_floats;
+        const FdkViewCoef& c = coef[k];
+        if (AXIAL) {
+            // next view's terms first: independent of this view's stage
+            const ColTerms nxt = (k + 1 < n_views) ? axial_terms(coef[k + 1], X, Y, Z0, g.vz) : cur;
+            const float u = cur.u;
+            const float fu = floorf(u);
+            const int iu = static_cast<int>(fu);
+            float au = u - fu;
+            float vbq = cur.vbq, vs = cur.vs, w = cur.w;
+            // rows of the column's end points (the rounding map is monotonic)
+            const int na = static_cast<int>(__float_as_uint(vbq + kRoundMagic) - kRoundMagicBits);
+            const int nb = static_cast<int>(__float_as_uint(fmaf(static_cast<float>(ZT - 1), vs, vbq) +
+                kRoundMagic) - kRoundMagicBits);
+            const int lo = min(na, nb), hi = max(na, nb) + 1;
+            // |v| < 2^21 along the column keeps the rounding word exact
+            const bool finite = fabsf(u) < 1e6f && fabsf(vbq) < 1e6f && fabsf(vs) < 3e4f &&
+                fabsf(w) < 1e30f;
+            int col = iu - b.x;
+            if (!active || !finite || iu < b.x || iu + 1 > b.z || lo < b.y || hi > b.w) {
+                if (active) bad = true;
+                // no contribution; every read stays at the stage origin
+                w = 0.f; au = 0.f; vs = 0.f;
+                vbq = static_cast<float>(b.y);
+                col = 0;
+            }
+            // smem byte address of tap (row n, col) = n*4BW + base, n taken
+            // from the rounding word (wrapping 32-bit arithmetic)
+            const uint32_t base = smem_addr(S) + 4u * static_cast<uint32_t>(col) -
+                4u * BW * (static_cast<uint32_t>(b.y) + kRoundMagicBits);
+            const f2 vs2 = f2pack(vs, vs), vb2 = f2pack(vbq, vbq);
+            const f2 au2 = f2pack(au, au), w2 = f2pack(w, w);
+            const f2 M2 = f2pack(kRoundMagic, kRoundMagic), H2 = f2pack(0.5f, 0.5f);
+#pragma unroll
+            for (int j = 0; j < ZT / 2; ++j) {
+                const f2 vq = f2fma(f2pack(2.f * j, 2.f * j + 1.f), vs2, vb2);
+                const f2 t = f2add(vq, M2);
+                const f2 fr = f2add(f2sub(vq, f2sub(t, M2)), H2);
+                float t0, t1;
+                f2unpack(t, t0, t1);
+                const uint32_t a0 = __float_as_uint(t0) * (4u * BW) + base;
+                const uint32_t a1 = __float_as_uint(t1) * (4u * BW) + base;
+                const f2 p00 = f2pack(lds<0>(a0), lds<0>(a1));
+                const f2 p10 = f2pack(lds<4>(a0), lds<4>(a1));
+                const f2 p01 = f2pack(lds<4 * BW>(a0), lds<4 * BW>(a1));
+                const f2 p11 = f2pack(lds<4 * BW + 4>(a0), lds<4 * BW + 4>(a1));
+                const f2 r0 = f2fma(au2, f2sub(p10, p00), p00);
+                const f2 r1 = f2fma(au2, f2sub(p11, p01), p01);
+                acc2[j] = f2fma(w2, f2fma(fr, f2sub(r1, r0), r0), acc2[j]);
+            }
+            cur = nxt;
+        } else {
+            const double den0 = fma(c.cd[2], Z0, fma(c.cd[1], Y, fma(c.cd[0], X, c.cd[3])));
+            const double un0 = fma(c.cu[2], Z0, fma(c.cu[1], Y, fma(c.cu[0], X, c.cu[3])));
+            const double vn0 = fma(c.cv[2], Z0, fma(c.cv[1], Y, fma(c.cv[0], X, c.cv[3])));
+            const double dp0 = fma(c.cr[2], Z0, fma(c.cr[1], Y, fma(c.cr[0], X, c.cr[3])));
+            const float s0 = static_cast<float>(c.wbase);
+            const float dn = static_cast<float>(den0), ddn = static_cast<float>(c.cd[2] * g.vz);
+            const float uu = static_cast<float>(un0), dun = static_cast<float>(c.cu[2] * g.vz);
+            const float vv = static_cast<float>(vn0), dvn = static_cast<float>(c.cv[2] * g.vz);
+            const float dp = static_cast<float>(dp0), ddp = static_cast<float>(c.cr[2] * g.vz);
+            // end points: u(z) and v(z) are monotonic along the column
+            const float ra = 1.f / dn, rb = 1.f / fmaf(ZT - 1.f, ddn, dn);
+            const float ua = uu * ra, ub = fmaf(ZT - 1.f, dun, uu) * rb;
+            const float va = vv * ra, vb2 = fmaf(ZT - 1.f, dvn, vv) * rb;
+            // u(z), v(z) are monotonic; one row/column of slack covers the
+            // rounding of the interior samples
+            const int ulo = static_cast<int>(floorf(fminf(ua, ub))) - 1;
+            const int uhi = static_cast<int>(floorf(fmaxf(ua, ub))) + 2;
+            const int vlo = static_cast<int>(floorf(fminf(va, vb2))) - 1;
+            const int vhi = static_cast<int>(floorf(fmaxf(va, vb2))) + 2;
+            float scale = s0;
+            float gdn = dn, gddn = ddn, guu = uu, gdun = dun, gvv = vv, gdvn = dvn, gdp = dp, gddp = ddp;
+            const bool finite = fabsf(ua) < 1e7f && fabsf(ub) < 1e7f && fabsf(va) < 1e7f &&
+                fabsf(vb2) < 1e7f && dn > 0.f && fmaf(ZT - 1.f, ddn, dn) > 0.f &&
+                dp > 0.f && fmaf(ZT - 1.f, ddp, dp) > 0.f;
+            if (!active || !finite || ulo < b.x || uhi > b.z || vlo < b.y || vhi > b.w) {
+                if (active) bad = true;
+                scale = 0.f;  // no contribution; reads stay at the stage origin
+                gdn = 1.f; gddn = 0.f; guu = static_cast<float>(b.x); gdun = 0.f;
+                gvv = static_cast<float>(b.y); gdvn = 0.f; gdp = 1.f; gddp = 0.f;
+            }
+            const int cb = -b.x - b.y * BW;
+#pragma unroll
+            for (int i = 0; i < ZT; ++i) {
+                const float fi = static_cast<float>(i);
+                const float rden = 1.f / fmaf(fi, gddn, gdn);
+                const float u = fmaf(fi, gdun, guu) * rden;
+                const float v = fmaf(fi, gdvn, gvv) * rden;
+                const float rdep = 1.f / fmaf(fi, gddp, gdp);
+                const float w = scale * rdep * rdep;
+                const float fu = floorf(u), fv = floorf(v);
+                const int a = static_cast<int>(fv) * BW + static_cast<int>(fu) + cb;
+                const float au = u - fu, av = v - fv;
+                const float p00 = S[a], p10 = S[a + 1], p01 = S[a + BW], p11 = S[a + BW + 1];
+                const float r0 = fmaf(au, p10 - p00, p00);
+                const float r1 = fmaf(au, p11 - p01, p01);
+                acc[i] = fmaf(w, fmaf(av, r1 - r0, r0), acc[i]);
+            }
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[s]);
+    }
+    if (bad) atomicOr(err, kErrFootprint);
+    if (!active) return;
+    if (AXIAL) {
+#pragma unroll
+        for (int j = 0; j < ZT / 2; ++j) f2unpack(acc2[j], acc[2 * j], acc[2 * j + 1]);
+    }
+    const long plane = static_cast<long>(g.nx) * g.ny;
+    float* dst = vol + static_cast<long>(y) * g.nx + x;
+#pragma unroll
+    for (int i = 0; i < ZT; ++i) {
+        const int z = z0 + i;
+        if (z < g.nz) {
+            float* p = dst + z * plane;
+            *p = accumulate ? *p + acc[i] : acc[i];
+        }
+    }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
+{
+    static std::once_flag once;
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess && q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+constexpr int kWidths[] = {36, 52, 68, 100, 132, 196, 256};
+
+template <int BW>
+cudaError_t launch_bw(const CUtensorMap& map, const FdkViewCoef* coef, int n_views,
+    const VolumeGrid& g, int BH, int stages, size_t smem, bool axial, float* vol, int accumulate,
+    int* err, cudaStream_t s)
+{
+    const dim3 grid((g.nx + TX - 1) / TX, (g.ny + TY - 1) / TY, (g.nz + ZT - 1) / ZT);
+    if (axial) {
+        auto k = fdk_bp_tma_kernel<BW, true>;
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            static_cast<int>(smem));
+        if (e != cudaSuccess) return e;
+        k<<<grid, NTHREADS, smem, s>>>(map, coef, n_views, g, BH, stages, vol, accumulate, err);
+    } else {
+        auto k = fdk_bp_tma_kernel<BW, false>;
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            static_cast<int>(smem));
+        if (e != cudaSuccess) return e;
+        k<<<grid, NTHREADS, smem, s>>>(map, coef, n_views, g, BH, stages, vol, accumulate, err);
+    }
+    return cudaGetLastError();
+}
+
+} // namespace
+
+// Largest tile box over all views and tiles; returns the chosen width (one of
+// kWidths, 0 if none fits) and height.
+cudaError_t fdk_tma_box(const FdkViewCoef* coef, int n_views, const VolumeGrid& g, int* scratch2,
+    int* bw, int* bh, cudaStream_t s)
+{
+    *bw = 0; *bh = 0;
+    cudaError_t e = cudaMemsetAsync(scratch2, 0, 2 * sizeof(int), s);
+    if (e != cudaSuccess) return e;
+    const int tx = (g.nx + TX - 1) / TX, ty = (g.ny + TY - 1) / TY, tz = (g.nz + ZT - 1) / ZT;
+    box_extent_kernel<<<1184, 256, 0, s>>>(coef, n_views, g, tx, ty, tz, scratch2);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    int host[2] = {0, 0};
+    if ((e = cudaMemcpyAsync(host, scratch2, sizeof host, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+        return e;
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
+    for (int w : kWidths)
+        if (w >= host[0]) { *bw = w; break; }
+    *bh = host[1];
+    if (*bh > 256) *bw = 0;
+    return cudaSuccess;
+}
+
+// Stages that fit the shared-memory budget for a box (0 when none).
+int fdk_tma_stages(int bw, int bh)
+{
+    const size_t stage = static_cast<size_t>(stage_stride_floats(bw, bh)) * sizeof(float);
+    const size_t budget = 72 * 1024;  // three CTAs per SM
+    int s = static_cast<int>(budget / std::max<size_t>(stage, 1));
+    s = std::min(s, 8);
+    return s >= 2 ? s : 0;
+}
+
+bool fdk_tma_available() { return encode_fn() != nullptr; }
+
+cudaError_t launch_fdk_backproject_tma(const float* filtered, int ld, int rows_total_views,
+    const FdkViewCoef* coef, int n_views, int nu, int nv, const VolumeGrid& g, bool axial,
+    int bw, int bh, float* vol, int accumulate, int* err, cudaStream_t s)
+{
+    auto enc = encode_fn();
+    if (!enc) return cudaErrorNotSupported;
+    CUtensorMap map;
+    const cuuint64_t dims[3] = {static_cast<cuuint64_t>(nu), static_cast<cuuint64_t>(nv),
+                                static_cast<cuuint64_t>(rows_total_views)};
+    const cuuint64_t strides[2] = {static_cast<cuuint64_t>(ld) * sizeof(float),
+                                   static_cast<cuuint64_t>(ld) * nv * sizeof(float)};
+    const cuuint32_t box[3] = {static_cast<cuuint32_t>(bw), static_cast<cuuint32_t>(bh), 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(filtered),
+        dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+        CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
+    const int stages = fdk_tma_stages(bw, bh);
+    if (stages == 0) return cudaErrorInvalidConfiguration;
+    const size_t ring = static_cast<size_t>(stage_stride_floats(bw, bh)) * sizeof(float) * stages;
+    const size_t smem = 128 + ring + 2 * stages * sizeof(uint64_t) + stages * sizeof(int4) + 16;
+    switch (bw) {
+    case 36: return launch_bw<36>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, s);
+    case 52: return launch_bw<52>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, s);
+    case 68: return launch_bw<68>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, s);
+    case 100: return launch_bw<100>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, s);
+    case 132: return launch_bw<132>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, s);
+    case 196: return launch_bw<196>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, s);
+    case 256: return launch_bw<256>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, s);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+} // namespace ykb

@@ -55,7 +55,7 @@ constexpr int RBM = 64, RBN = 128, RBK = 32;
 template <typename TOut>
 __global__ void __launch_bounds__(256) ramp_fp32_kernel(const float* __restrict__ A,
     const float* __restrict__ h, const FdkPreweightView* __restrict__ pwv, long rows,
-    int nu, int nv, TOut* __restrict__ C)
+    int nu, int nv, TOut* __restrict__ C, int ldc)
 {
     __shared__ __align__(16) float As[RBK][RBM + 4];
     __shared__ float hs[RBN + RBK];
@@ -114,8 +114,8 @@ __global__ void __launch_bounds__(256) ramp_fp32_kernel(const float* __restrict_
             const int j = j0 + tx * 8 + q;
             if (j >= nu) continue;
             const float v = (j >= p.out_lo && j < p.out_hi) ? acc[i][q] : 0.f;
-            if constexpr (sizeof(TOut) == 4) C[m * nu + j] = v;
-            else C[m * nu + j] = __float2bfloat16_rn(v);
+            if constexpr (sizeof(TOut) == 4) C[m * ldc + j] = v;
+            else C[m * ldc + j] = __float2bfloat16_rn(v);
         }
     }
 }
@@ -134,11 +134,11 @@ __global__ void __launch_bounds__(256) ramp_fp32_kernel(const float* __restrict_
 // and only v advances along the column.
 // ---------------------------------------------------------------------------
 template <typename T>
-__device__ __forceinline__ float tap(const T* img, int nu, int nv, int iu, int iv)
+__device__ __forceinline__ float tap(const T* img, int nu, int nv, int ld, int iu, int iv)
 {
     return (static_cast<unsigned>(iu) < static_cast<unsigned>(nu) &&
             static_cast<unsigned>(iv) < static_cast<unsigned>(nv))
-        ? load_as_float(img + static_cast<long>(iv) * nu + iu) : 0.f;
+        ? load_as_float(img + static_cast<long>(iv) * ld + iu) : 0.f;
 }
 
 __device__ __forceinline__ double rcp_fp64(double x)
@@ -151,7 +151,7 @@ __device__ __forceinline__ double rcp_fp64(double x)
 
 template <int ZT, bool AXIAL, typename T>
 __global__ void __launch_bounds__(256) fdk_bp_kernel(const T* __restrict__ proj,
-    const FdkViewCoef* __restrict__ coef, int n_views, int nu, int nv, VolumeGrid g,
+    const FdkViewCoef* __restrict__ coef, int n_views, int nu, int nv, int ld, VolumeGrid g,
     float* __restrict__ vol, int accumulate)
 {
     const int x = blockIdx.x * 32 + threadIdx.x;
@@ -164,7 +164,7 @@ __global__ void __launch_bounds__(256) fdk_bp_kernel(const T* __restrict__ proj,
     float acc[ZT];
 #pragma unroll
     for (int i = 0; i < ZT; ++i) acc[i] = 0.f;
-    const long view_elems = static_cast<long>(nu) * nv;
+    const long view_elems = static_cast<long>(ld) * nv;
 
     for (int k = 0; k < n_views; ++k) {
         const FdkViewCoef& c = coef[k];
@@ -188,8 +188,8 @@ __global__ void __launch_bounds__(256) fdk_bp_kernel(const T* __restrict__ proj,
                 const float fv = floorf(v);
                 const int iv = static_cast<int>(fv);
                 const float av = v - fv;
-                const float p00 = tap(img, nu, nv, iu, iv), p10 = tap(img, nu, nv, iu + 1, iv);
-                const float p01 = tap(img, nu, nv, iu, iv + 1), p11 = tap(img, nu, nv, iu + 1, iv + 1);
+                const float p00 = tap(img, nu, nv, ld, iu, iv), p10 = tap(img, nu, nv, ld, iu + 1, iv);
+                const float p01 = tap(img, nu, nv, ld, iu, iv + 1), p11 = tap(img, nu, nv, ld, iu + 1, iv + 1);
                 const float r0 = fmaf(au, p10 - p00, p00);
                 const float r1 = fmaf(au, p11 - p01, p01);
                 acc[i] = fmaf(w, fmaf(av, r1 - r0, r0), acc[i]);
@@ -216,8 +216,8 @@ __global__ void __launch_bounds__(256) fdk_bp_kernel(const T* __restrict__ proj,
                 const float fu = floorf(u), fv = floorf(v);
                 const int iu = static_cast<int>(fu), iv = static_cast<int>(fv);
                 const float au = u - fu, av = v - fv;
-                const float p00 = tap(img, nu, nv, iu, iv), p10 = tap(img, nu, nv, iu + 1, iv);
-                const float p01 = tap(img, nu, nv, iu, iv + 1), p11 = tap(img, nu, nv, iu + 1, iv + 1);
+                const float p00 = tap(img, nu, nv, ld, iu, iv), p10 = tap(img, nu, nv, ld, iu + 1, iv);
+                const float p01 = tap(img, nu, nv, ld, iu, iv + 1), p11 = tap(img, nu, nv, ld, iu + 1, iv + 1);
                 const float r0 = fmaf(au, p10 - p00, p00);
                 const float r1 = fmaf(au, p11 - p01, p01);
                 acc[i] = fmaf(w, fmaf(av, r1 - r0, r0), acc[i]);
@@ -252,35 +252,35 @@ cudaError_t launch_fdk_preweight(const void* proj, int proj_dtype,
 
 cudaError_t launch_fdk_ramp_fp32(const float* pw_rows, const float* h_dev,
     const FdkPreweightView* pwv, int n_views, int nu, int nv, void* out, int out_dtype,
-    cudaStream_t s)
+    int ldc, cudaStream_t s)
 {
     const long rows = static_cast<long>(n_views) * nv;
     if (rows <= 0) return cudaSuccess;
     const dim3 grid((nu + RBN - 1) / RBN, static_cast<unsigned>((rows + RBM - 1) / RBM));
     if (out_dtype == YKB_DTYPE_BF16)
         ramp_fp32_kernel<__nv_bfloat16><<<grid, 256, 0, s>>>(pw_rows, h_dev, pwv, rows, nu, nv,
-            static_cast<__nv_bfloat16*>(out));
+            static_cast<__nv_bfloat16*>(out), ldc);
     else
         ramp_fp32_kernel<float><<<grid, 256, 0, s>>>(pw_rows, h_dev, pwv, rows, nu, nv,
-            static_cast<float*>(out));
+            static_cast<float*>(out), ldc);
     return cudaGetLastError();
 }
 
 cudaError_t launch_fdk_backproject(const void* filtered, int dtype, const FdkViewCoef* coef,
-    int n_views, int nu, int nv, const VolumeGrid& g, bool axial, float* vol, int accumulate,
-    cudaStream_t s)
+    int n_views, int nu, int nv, int ld, const VolumeGrid& g, bool axial, float* vol,
+    int accumulate, cudaStream_t s)
 {
     constexpr int ZT = 16;
     const dim3 block(32, 8);
     const dim3 grid((g.nx + 31) / 32, (g.ny + 7) / 8, (g.nz + ZT - 1) / ZT);
     if (dtype == YKB_DTYPE_BF16) {
         auto p = static_cast<const __nv_bfloat16*>(filtered);
-        if (axial) fdk_bp_kernel<ZT, true><<<grid, block, 0, s>>>(p, coef, n_views, nu, nv, g, vol, accumulate);
-        else fdk_bp_kernel<ZT, false><<<grid, block, 0, s>>>(p, coef, n_views, nu, nv, g, vol, accumulate);
+        if (axial) fdk_bp_kernel<ZT, true><<<grid, block, 0, s>>>(p, coef, n_views, nu, nv, ld, g, vol, accumulate);
+        else fdk_bp_kernel<ZT, false><<<grid, block, 0, s>>>(p, coef, n_views, nu, nv, ld, g, vol, accumulate);
     } else {
         auto p = static_cast<const float*>(filtered);
-        if (axial) fdk_bp_kernel<ZT, true><<<grid, block, 0, s>>>(p, coef, n_views, nu, nv, g, vol, accumulate);
-        else fdk_bp_kernel<ZT, false><<<grid, block, 0, s>>>(p, coef, n_views, nu, nv, g, vol, accumulate);
+        if (axial) fdk_bp_kernel<ZT, true><<<grid, block, 0, s>>>(p, coef, n_views, nu, nv, ld, g, vol, accumulate);
+        else fdk_bp_kernel<ZT, false><<<grid, block, 0, s>>>(p, coef, n_views, nu, nv, ld, g, vol, accumulate);
     }
     return cudaGetLastError();
 }

@@ -146,12 +146,16 @@ YKB_API ykb_status ykb_fdk_plan_create(const ykb_cone_view* views, int n_views, 
     std::vector<float> hf(h.begin(), h.end());
 
     p->batch_capacity = chunk_capacity(n_views, nu, nv);
+    // filtered rows padded to 16 bytes: the pitch a TMA tensor map needs
+    p->ld = (nu + 7) / 8 * 8;
     const size_t chunk_elems = static_cast<size_t>(p->batch_capacity) * nu * nv;
-    const size_t filt_bytes = chunk_elems * (precision == YKB_PRECISION_BF16 ? 2 : 4);
+    const size_t filt_bytes = static_cast<size_t>(p->batch_capacity) * p->ld * nv *
+        (precision == YKB_PRECISION_BF16 ? 2 : 4);
     cudaError_t e;
     if ((e = p->coef.alloc(sizeof(FdkViewCoef) * n_views)) != cudaSuccess ||
         (e = p->pwv.alloc(sizeof(FdkPreweightView) * n_views)) != cudaSuccess ||
         (e = p->ramp.alloc(sizeof(float) * hf.size())) != cudaSuccess ||
+        (e = p->err_flag.alloc(4 * sizeof(int))) != cudaSuccess ||
         (e = p->work_a.alloc(chunk_elems * sizeof(float))) != cudaSuccess ||
         (e = p->work_filtered.alloc(filt_bytes)) != cudaSuccess) {
         delete p;
@@ -162,9 +166,27 @@ YKB_API ykb_status ykb_fdk_plan_create(const ykb_cone_view* views, int n_views, 
         (e = cudaMemcpy(p->pwv.ptr, pw.data(), sizeof(FdkPreweightView) * n_views,
              cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemcpy(p->ramp.ptr, hf.data(), sizeof(float) * hf.size(),
-             cudaMemcpyHostToDevice)) != cudaSuccess) {
+             cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemset(p->err_flag.ptr, 0, 4 * sizeof(int))) != cudaSuccess) {
         delete p;
         return cuda_status(e, "cudaMemcpy (FDK plan tables)");
+    }
+    // size the shared-memory projection box of the TMA backprojection from
+    // the footprints of every (tile, view) pair
+    if (fdk_tma_available()) {
+        cudaStream_t s = nullptr;
+        if ((e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)) != cudaSuccess) {
+            delete p;
+            return cuda_status(e, "cudaStreamCreate");
+        }
+        e = fdk_tma_box(p->coef.as<FdkViewCoef>(), n_views, make_grid(p->volume),
+            p->err_flag.as<int>() + 2, &p->tma_bw, &p->tma_bh, s);
+        cudaStreamDestroy(s);
+        if (e != cudaSuccess) {
+            delete p;
+            return cuda_status(e, "backprojection box pre-pass");
+        }
+        p->use_tma = p->tma_bw > 0 && fdk_tma_stages(p->tma_bw, p->tma_bh) > 0;
     }
     *plan_out = p;
     return YKB_OK;
@@ -205,14 +227,33 @@ size_t dtype_bytes(int dtype) { return dtype == YKB_DTYPE_BF16 ? 2 : 4; }
 // preweight + ramp for views [first, first+count) of the plan, input rows at
 // proj, output into dst (plan dtype)
 ykb_status filter_chunk(ykb_fdk_plan* p, const void* proj, int proj_dtype, int first, int count,
-    void* dst, cudaStream_t s)
+    void* dst, int ldc, cudaStream_t s)
 {
     const FdkPreweightView* pwv = p->pwv.as<FdkPreweightView>() + first;
     const int out_dtype = p->precision == YKB_PRECISION_BF16 ? YKB_DTYPE_BF16 : YKB_DTYPE_F32;
     YKB_TRY_CUDA(launch_fdk_preweight(proj, proj_dtype, pwv, count, p->nu, p->nv,
         p->work_a.as<float>(), s));
     YKB_TRY_CUDA(launch_fdk_ramp_fp32(p->work_a.as<float>(), p->ramp.as<float>(), pwv, count,
-        p->nu, p->nv, dst, out_dtype, s));
+        p->nu, p->nv, dst, out_dtype, ldc, s));
+    return YKB_OK;
+}
+
+// weighted backprojection of `count` filtered views (row pitch ld) starting
+// at plan view `first`
+ykb_status backproject_chunk(ykb_fdk_plan* p, const void* filtered, int dtype, int ld, int first,
+    int count, float* vol, int accumulate, cudaStream_t s)
+{
+    const VolumeGrid grid = make_grid(p->volume);
+    const FdkViewCoef* coef = p->coef.as<FdkViewCoef>() + first;
+    const bool tma_ok = p->use_tma && dtype == YKB_DTYPE_F32 && ld % 4 == 0 &&
+        (reinterpret_cast<uintptr_t>(filtered) & 15) == 0;
+    if (tma_ok)
+        YKB_TRY_CUDA(launch_fdk_backproject_tma(static_cast<const float*>(filtered), ld, count, coef,
+            count, p->nu, p->nv, grid, p->axial, p->tma_bw, p->tma_bh, vol, accumulate,
+            p->err_flag.as<int>(), s));
+    else
+        YKB_TRY_CUDA(launch_fdk_backproject(filtered, dtype, coef, count, p->nu, p->nv, ld, grid,
+            p->axial, vol, accumulate, s));
     return YKB_OK;
 }
 
@@ -232,7 +273,7 @@ YKB_API ykb_status ykb_fdk_filter(ykb_fdk_plan* p, const void* d_proj, int proj_
         const int cnt = std::min(p->batch_capacity, n_views - c);
         const char* in = static_cast<const char*>(d_proj) + c * view_elems * dtype_bytes(proj_dtype);
         char* out = static_cast<char*>(d_filtered) + c * view_elems * out_b;
-        if (const ykb_status st = filter_chunk(p, in, proj_dtype, view_offset + c, cnt, out, s))
+        if (const ykb_status st = filter_chunk(p, in, proj_dtype, view_offset + c, cnt, out, p->nu, s))
             return st;
     }
     return YKB_OK;
@@ -248,10 +289,8 @@ YKB_API ykb_status ykb_fdk_backproject(ykb_fdk_plan* p, const void* d_filtered,
     if (!d_volume) return fail(YKB_ERR_INVALID_BUFFER, "null volume buffer");
     DeviceGuard guard(p->device);
     const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    YKB_TRY_CUDA(launch_fdk_backproject(d_filtered, filtered_dtype,
-        p->coef.as<FdkViewCoef>() + view_offset, n_views, p->nu, p->nv, make_grid(p->volume),
-        p->axial, d_volume, clear_output ? 0 : 1, s));
-    return YKB_OK;
+    return backproject_chunk(p, d_filtered, filtered_dtype, p->nu, view_offset, n_views, d_volume,
+        clear_output ? 0 : 1, s);
 }
 
 YKB_API ykb_status ykb_fdk_execute(ykb_fdk_plan* p, const void* d_proj, int proj_dtype,
@@ -264,19 +303,37 @@ YKB_API ykb_status ykb_fdk_execute(ykb_fdk_plan* p, const void* d_proj, int proj
     const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const size_t view_elems = static_cast<size_t>(p->nu) * p->nv;
     const int filt_dtype = p->precision == YKB_PRECISION_BF16 ? YKB_DTYPE_BF16 : YKB_DTYPE_F32;
-    const VolumeGrid grid = make_grid(p->volume);
     for (int c = 0; c < n_views; c += p->batch_capacity) {
         const int cnt = std::min(p->batch_capacity, n_views - c);
         const char* in = static_cast<const char*>(d_proj) + c * view_elems * dtype_bytes(proj_dtype);
         if (const ykb_status st = filter_chunk(p, in, proj_dtype, view_offset + c, cnt,
-                p->work_filtered.ptr, s))
+                p->work_filtered.ptr, p->ld, s))
             return st;
         const int accumulate = (c == 0 && clear_output) ? 0 : 1;
-        YKB_TRY_CUDA(launch_fdk_backproject(p->work_filtered.ptr, filt_dtype,
-            p->coef.as<FdkViewCoef>() + view_offset + c, cnt, p->nu, p->nv, grid, p->axial,
-            d_volume, accumulate, s));
+        if (const ykb_status st = backproject_chunk(p, p->work_filtered.ptr, filt_dtype, p->ld,
+                view_offset + c, cnt, d_volume, accumulate, s))
+            return st;
     }
     return YKB_OK;
+}
+
+YKB_API ykb_status ykb_fdk_check(ykb_fdk_plan* p, ykb_stream stream)
+{
+    clear_error();
+    if (!p) return fail(YKB_ERR_INVALID_CONFIG, "null plan");
+    DeviceGuard guard(p->device);
+    const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    int word = 0;
+    YKB_TRY_CUDA(cudaMemcpyAsync(&word, p->err_flag.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));
+    YKB_TRY_CUDA(cudaStreamSynchronize(s));
+    if (word == 0) return YKB_OK;
+    YKB_TRY_CUDA(cudaMemsetAsync(p->err_flag.ptr, 0, sizeof(int), s));
+    YKB_TRY_CUDA(cudaStreamSynchronize(s));
+    std::string msg = "device-side failure in the backprojection:";
+    if (word & 1) msg += " a pipeline wait timed out;";
+    if (word & 2) msg += " a voxel column left its projection box;";
+    if (word & 4) msg += " a staged copy was not 128-byte aligned (skipped);";
+    return fail(YKB_ERR_CUDA, msg);
 }
 
 // --------------------------------------------------------------- Joseph ---

@@ -10,7 +10,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/ykb.h"
+#include "ykb.h"
 
 namespace ykb {
 
@@ -157,7 +157,7 @@ cudaError_t launch_fdk_preweight(const void* proj, int proj_dtype,
     cudaStream_t s);
 cudaError_t launch_fdk_ramp_fp32(const float* pw_rows, const float* h_dev,
     const FdkPreweightView* pwv, int n_views, int nu, int nv, void* out,
-    int out_dtype, cudaStream_t s);
+    int out_dtype, int ldc, cudaStream_t s);
 cudaError_t launch_fdk_preweight_split_bf16(const void* proj, int proj_dtype,
     const FdkPreweightView* pw, int n_views, int nu, int nv, int ld,
     __nv_bfloat16* hi, __nv_bfloat16* lo, cudaStream_t s);
@@ -168,9 +168,17 @@ cudaError_t launch_fdk_ramp_tcgen05(const __nv_bfloat16* a_hi,
     cudaStream_t s);
 bool tcgen05_filter_supported(int nu);
 cudaError_t launch_fdk_backproject(const void* filtered, int dtype,
-    const FdkViewCoef* coef, int n_views, int nu, int nv,
+    const FdkViewCoef* coef, int n_views, int nu, int nv, int ld,
     const VolumeGrid& grid, bool axial, float* vol, int accumulate,
     cudaStream_t s);
+// TMA-staged backprojection (fdk_bp_tma.cu)
+bool fdk_tma_available();
+int fdk_tma_stages(int bw, int bh);
+cudaError_t fdk_tma_box(const FdkViewCoef* coef, int n_views, const VolumeGrid& g,
+    int* scratch2, int* bw, int* bh, cudaStream_t s);
+cudaError_t launch_fdk_backproject_tma(const float* filtered, int ld, int views_in_buffer,
+    const FdkViewCoef* coef, int n_views, int nu, int nv, const VolumeGrid& g, bool axial,
+    int bw, int bh, float* vol, int accumulate, int* err, cudaStream_t s);
 
 // Joseph
 cudaError_t launch_joseph_transpose(const float* vol, int nx, int ny, int nz,
@@ -198,7 +206,9 @@ struct ykb_fdk_plan {
     bool axial = false;
     bool tc_filter = false;
     int batch_capacity = 0;      // views the workspace holds
-    int ld = 0;                  // leading dimension of the bf16 operand rows
+    int ld = 0;                  // row pitch (elements) of the filtered workspace
+    bool use_tma = false;        // TMA-staged backprojection
+    int tma_bw = 0, tma_bh = 0;  // its projection box
     std::vector<ykb::FdkDerived> derived;
     ykb::DeviceBuffer coef;      // FdkViewCoef[n_views]
     ykb::DeviceBuffer pwv;       // FdkPreweightView[n_views]
@@ -206,7 +216,7 @@ struct ykb_fdk_plan {
     ykb::DeviceBuffer toeplitz_hi, toeplitz_lo;  // bf16 [nu][ld] (BF16 plans)
     ykb::DeviceBuffer work_a;    // preweighted rows (float) or bf16 hi/lo
     ykb::DeviceBuffer work_filtered;  // filtered projections (plan dtype)
-    ykb::DeviceBuffer err_flag;  // int, device-side error reporting
+    ykb::DeviceBuffer err_flag;  // int[4]: device error word, box pre-pass scratch
 };
 
 struct ykb_joseph_plan {

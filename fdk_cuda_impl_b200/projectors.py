@@ -69,6 +69,10 @@ class FdkPlan:
     def workspace_bytes(self) -> int:
         return int(self.lib.ykb_fdk_workspace_bytes(self._h))
 
+    def check(self) -> None:
+        """Synchronises the current stream and raises on a device-side error."""
+        L.check(self.lib.ykb_fdk_check(self._h, _stream_handle(self.device)))
+
     def _vol_out(self, volume):
         if volume is None:
             return torch.empty(self.grid.shape, dtype=torch.float32, device=f"cuda:{self.device}")

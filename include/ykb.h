@@ -171,6 +171,13 @@ YKB_API ykb_status ykb_fdk_backproject(ykb_fdk_plan* plan,
 /* Bytes of device workspace the plan holds (introspection). */
 YKB_API size_t ykb_fdk_workspace_bytes(const ykb_fdk_plan* plan);
 
+/* Synchronises `stream` and reports (then clears) the plan's device-side
+ * error word: YKB_ERR_CUDA when a bounded pipeline wait timed out or a voxel
+ * column fell outside its staged projection box (the kernels never hang or
+ * fault on these; they stop and record them).  The reference has no
+ * equivalent: it aborts the process on CUDA errors (src/global/YkMacro.hpp:35-41). */
+YKB_API ykb_status ykb_fdk_check(ykb_fdk_plan* plan, ykb_stream stream);
+
 /* The preweight + ramp filter stage of ykb_fdk_filter for callers that
  * cannot call cudaMalloc (an application whose memory pool owns the GPU,
  * a real-time loop that forbids allocation after start-up): no plan and no

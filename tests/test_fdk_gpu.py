@@ -28,6 +28,7 @@ def _run_case(oracle, case, precision="fp32", proj_dtype="f32", ph=None):
     plan = FdkPlan(views, case.scan.channels, case.scan.rows, case.scan.scan_range, case.grid,
                    case.filt, precision=precision)
     out = plan.execute(dev_p).cpu().numpy()
+    plan.check()  # no device-side timeout or footprint error
     ref = oracle.fdk(views, case.scan.channels, case.scan.rows, case.scan.scan_range,
                      K.oracle_volume(oracle, case.grid), K.oracle_filter(oracle, case.filt), p)
     return out, ref, plan, views, p
@@ -84,6 +85,7 @@ def test_fdk_backproject_stage(oracle, cuda_device):
     f = oracle.normal((60, 64, 96), 21)
     plan = FdkPlan(views, 96, 64, case.scan.scan_range, case.grid, case.filt)
     got = plan.backproject(torch.from_numpy(f).cuda()).cpu().numpy()
+    plan.check()
     ref = oracle.fdk_backproject(views, 96, 64, case.scan.scan_range,
                                  K.oracle_volume(oracle, case.grid), f.astype(np.float64))
     assert K.rel_rmse(got, ref) <= FP32_TOL
@@ -103,6 +105,7 @@ def test_fdk_streaming_batches(oracle, cuda_device):
     plan.execute(p[0:5], vol, view_offset=0, clear=True)
     plan.execute(p[5:23], vol, view_offset=5, clear=False)
     plan.execute(p[23:], vol, view_offset=23, clear=False)
+    plan.check()
     diff = (vol - full).abs().max().item()
     assert diff < 1e-4
     assert K.rel_rmse(vol.cpu().numpy(), full.cpu().numpy()) < 1e-6
@@ -149,3 +152,41 @@ def test_fdk_errors_are_status_codes(cuda_device, oracle):
     assert e.value.code == L.ERR_INVALID_CONFIG
     # the context stays usable
     assert torch.isfinite(plan.execute(p, view_offset=50)).all()
+
+
+def test_fdk_backproject_stage_unaligned_pitch(oracle, cuda_device):
+    # nu not a multiple of 4: the stage entry cannot use a TMA tensor map on
+    # the caller's buffer and takes the global-load kernel
+    import torch
+    from fdk_cuda_impl_b200.projectors import FdkPlan
+    case = K.odd_case()
+    views = case.scan.views()
+    nu, nv = case.scan.channels, case.scan.rows
+    f = oracle.normal((len(views), nv, nu), 31)
+    plan = FdkPlan(views, nu, nv, case.scan.scan_range, case.grid, case.filt)
+    got = plan.backproject(torch.from_numpy(f).cuda()).cpu().numpy()
+    plan.check()
+    ref = oracle.fdk_backproject(views, nu, nv, case.scan.scan_range,
+                                 K.oracle_volume(oracle, case.grid), f.astype(np.float64))
+    assert K.rel_rmse(got, ref) <= FP32_TOL
+
+
+def test_fdk_tma_matches_global_path(oracle, cuda_device):
+    # the staged (TMA) and the global-load backprojections give the same
+    # volume: the same weights applied in the same order
+    import torch
+    from fdk_cuda_impl_b200.projectors import FdkPlan
+    case = K.c1_small()
+    views = case.scan.views()
+    p = torch.from_numpy(K.projections(oracle, case, views)).cuda()
+    fp32 = FdkPlan(views, 96, 64, case.scan.scan_range, case.grid, case.filt)
+    filtered = fp32.filter(p)
+    staged = fp32.backproject(filtered)  # 16-byte aligned buffer -> TMA path
+    # the same values 4 bytes off a 16-byte boundary: no tensor map possible
+    flat = torch.empty(filtered.numel() + 1, device="cuda")
+    shifted = flat[1:].view(filtered.shape)
+    shifted.copy_(filtered)
+    assert shifted.data_ptr() % 16 != 0
+    direct = fp32.backproject(shifted)
+    fp32.check()
+    assert K.rel_rmse(staged.cpu().numpy(), direct.cpu().numpy()) < 1e-6
