@@ -1,0 +1,363 @@
+// Ramp filter on the 5th-generation tensor cores (tcgen05, sm_100a).
+//
+// The reference filters each detector row by zero-padded FFT convolution
+// (.../FDK/kernels/YkFDKFilterKernels.cu:32-140).  With N >= 2 Nu that is the
+// linear product C = A T, A = preweighted rows [rows][Nu], T[k][j] = h(j-k)
+// (Toeplitz and, h being even, symmetric).  Here it runs as one BF16 GEMM with
+// FP32 accumulation in TMEM and a split hi/lo correction:
+//     A T ~= A_hi T_hi + A_hi T_lo + A_lo T_hi,
+// folded into a single GEMM over K' = 3 Nu ([A_hi | A_hi | A_lo] x
+// [T_hi; T_lo; T_hi]) so one accumulator carries all three products.
+//
+// CTA = 128 output rows x TN output columns, 4 warps:
+//   warp 0 lane 0 : TMA producer (A and T tiles, 128-byte swizzle, this
+//                   GPU's memory only, no multicast) into a 4-stage ring;
+//   warp 1 lane 0 : MMA issuer (tcgen05.mma kind::f16, M=128, N=TN, K=16),
+//                   releases stages with tcgen05.commit;
+//   all 4 warps   : epilogue, tcgen05.ld of their 32 TMEM lanes, placement
+//                   mask, FP32 store.
+// Every mbarrier wait is bounded; on a timeout the CTA records an error,
+// drains what it issued and frees its TMEM.
+#include "ykb_internal.hpp"
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
+namespace ykb {
+namespace {
+
+constexpr int TM = 128, TK = 64, STAGES = 4;
+constexpr uint32_t kAStageBytes = TM * TK * 2;  // 16 KiB
+constexpr unsigned long long kWaitNs = 2000000000ull;
+constexpr int kErrTimeout = 8;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ unsigned long long now_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ void bar_init(uint64_t* b, uint32_t n)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(n) : "memory");
+}
+__device__ __forceinline__ void bar_expect_tx(uint64_t* b, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)),
+                 "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool bar_try(uint64_t* b, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                 " selp.u32 %0, 1, 0, p;\n}\n"
+                 : "=r"(ok) : "r"(smem_u32(b)), "r"(parity) : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool bar_wait(uint64_t* b, uint32_t parity)
+{
+    if (bar_try(b, parity)) return true;
+    const unsigned long long t0 = now_ns();
+    while (!bar_try(b, parity))
+        if (now_ns() - t0 > kWaitNs) return false;
+    return true;
+}
+__device__ __forceinline__ void tma_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y)
+{
+    asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+                 " [%0], [%1, {%2, %3}], [%4];"
+                 ::"r"(smem_u32(dst)), "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar)) : "memory");
+}
+
+// UMMA shared-memory descriptor of a K-major tile in the 128-byte swizzle
+// layout written by TMA: rows of 128 B, 8-row atoms 1024 B apart (SBO),
+// descriptor version 1, layout SWIZZLE_128B (2).  The tile base is 1024-byte
+// aligned; the k-th 16-element slice starts 32*k bytes further.
+__device__ __forceinline__ uint64_t kmajor_sw128_desc(uint32_t saddr)
+{
+    return static_cast<uint64_t>((saddr >> 4) & 0x3FFFu) | (static_cast<uint64_t>(1) << 16) |
+        (static_cast<uint64_t>(1024 >> 4) << 32) | (static_cast<uint64_t>(1) << 46) |
+        (static_cast<uint64_t>(2) << 61);
+}
+
+// instruction descriptor: D F32, A/B BF16, both K-major, N = TN, M = 128
+template <int TN>
+__device__ __forceinline__ uint32_t instr_desc()
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(TN >> 3) << 17) |
+        (static_cast<uint32_t>(TM >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc,
+    uint32_t accumulate)
+{
+    asm volatile("{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                 " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+                 ::"r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(accumulate) : "memory");
+}
+__device__ __forceinline__ void mma_commit(uint64_t* bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                 ::"r"(smem_u32(bar)) : "memory");
+}
+
+template <int TN>
+__global__ void __launch_bounds__(128, 1) ramp_tc_kernel(
+    const __grid_constant__ CUtensorMap map_a_hi, const __grid_constant__ CUtensorMap map_a_lo,
+    const __grid_constant__ CUtensorMap map_t_hi, const __grid_constant__ CUtensorMap map_t_lo,
+    long rows, int nu, int nv, int kchunks, const FdkPreweightView* __restrict__ pwv,
+    float* __restrict__ C, int ldc, int* __restrict__ err)
+{
+    constexpr uint32_t kBStageBytes = TN * TK * 2;
+    constexpr uint32_t kTmemCols = TN <= 32 ? 32 : TN <= 64 ? 64 : TN <= 128 ? 128 : 256;
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char* smem = reinterpret_cast<unsigned char*>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+    unsigned char* a_ring = smem;
+    unsigned char* b_ring = smem + STAGES * kAStageBytes;
+    uint64_t* full = reinterpret_cast<uint64_t*>(b_ring + STAGES * kBStageBytes);
+    uint64_t* empty = full + STAGES;
+    uint64_t* done = empty + STAGES;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+    int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long m0 = static_cast<long>(blockIdx.y) * TM;
+    const int n0 = blockIdx.x * TN;
+    const int total = 3 * kchunks;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(smem_u32(tmem_slot)), "r"(kTmemCols) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (threadIdx.x == 32) {
+        for (int s = 0; s < STAGES; ++s) { bar_init(&full[s], 1); bar_init(&empty[s], 1); }
+        bar_init(done, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        // ------------------------------------------------------- producer ---
+        int issued = 0;
+        for (int i = 0; i < total; ++i) {
+            const int s = i % STAGES;
+            if (i >= STAGES && !bar_wait(&empty[s], ((i / STAGES) - 1) & 1)) {
+                atomicOr(err, kErrTimeout);
+                *(volatile int*)abort_flag = 1;
+                break;
+            }
+            if (*(volatile int*)abort_flag) break;
+            const int seg = i / kchunks, kc = i % kchunks;
+            const CUtensorMap* ma = seg == 2 ? &map_a_lo : &map_a_hi;
+            const CUtensorMap* mt = seg == 1 ? &map_t_lo : &map_t_hi;
+            bar_expect_tx(&full[s], kAStageBytes + kBStageBytes);
+            tma_2d(a_ring + s * kAStageBytes, ma, &full[s], kc * TK, static_cast<int>(m0));
+            tma_2d(b_ring + s * kBStageBytes, mt, &full[s], kc * TK, n0);
+            issued = i + 1;
+        }
+        // every issued copy must land before the CTA can exit
+        for (int i = (issued > STAGES ? issued - STAGES : 0); i < issued; ++i)
+            bar_wait(&full[i % STAGES], (i / STAGES) & 1);
+    } else if (warp == 1 && lane == 0) {
+        // ----------------------------------------------------- MMA issuer ---
+        const uint32_t idesc = instr_desc<TN>();
+        int issued = 0;
+        for (int i = 0; i < total; ++i) {
+            const int s = i % STAGES;
+            if (!bar_wait(&full[s], (i / STAGES) & 1)) {
+                atomicOr(err, kErrTimeout);
+                *(volatile int*)abort_flag = 1;
+                break;
+            }
+            if (*(volatile int*)abort_flag) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint64_t da = kmajor_sw128_desc(smem_u32(a_ring + s * kAStageBytes));
+            const uint64_t db = kmajor_sw128_desc(smem_u32(b_ring + s * kBStageBytes));
+#pragma unroll
+            for (int kk = 0; kk < TK / 16; ++kk)
+                mma_bf16(tmem, da + 2 * kk, db + 2 * kk, idesc, (i > 0 || kk > 0) ? 1u : 0u);
+            mma_commit(&empty[s]);
+            issued = i + 1;
+        }
+        // `done` completes when every issued MMA has retired
+        mma_commit(done);
+        (void)issued;
+    }
+    __syncwarp();
+
+    // --------------------------------------------------------- epilogue ---
+    const bool ok = bar_wait(done, 0);
+    if (!ok) atomicOr(err, kErrTimeout);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const long m = m0 + warp * 32 + lane;
+    const bool row_ok = ok && !*(volatile int*)abort_flag && m < rows;
+    int out_lo = 0, out_hi = 0;
+    if (row_ok) {
+        const FdkPreweightView& p = pwv[m / nv];
+        out_lo = p.out_lo;
+        out_hi = p.out_hi;
+    }
+#pragma unroll 1
+    for (int c = 0; c < TN; c += 16) {
+        uint32_t r[16];
+        const uint32_t taddr = tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c);
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                     : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+                       "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
+                       "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                     : "r"(taddr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (row_ok) {
+            float* dst = C + m * ldc;
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                const int j = n0 + c + i;
+                if (j < nu) dst[j] = (j >= out_lo && j < out_hi) ? __uint_as_float(r[i]) : 0.f;
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
+                     ::"r"(tmem), "r"(kTmemCols) : "memory");
+}
+
+// preweighted rows split into bf16 hi and lo parts, rows padded to lda
+__global__ void __launch_bounds__(128) preweight_split_kernel(const void* __restrict__ in, int in_bf16,
+    const FdkPreweightView* __restrict__ pw, int nu, int nv, int lda, __nv_bfloat16* __restrict__ hi,
+    __nv_bfloat16* __restrict__ lo)
+{
+    const long row = blockIdx.x;
+    const int view = static_cast<int>(row / nv);
+    const int iv = static_cast<int>(row - static_cast<long>(view) * nv);
+    const FdkPreweightView& p = pw[view];
+    const double qx0 = p.detS[0] + iv * p.detV[0] - p.src[0];
+    const double qy0 = p.detS[1] + iv * p.detV[1] - p.src[1];
+    const double qz0 = p.detS[2] + iv * p.detV[2] - p.src[2];
+    const double scale = p.dsd * p.wgeom;
+    for (int iu = threadIdx.x; iu < lda; iu += blockDim.x) {
+        float x = 0.f;
+        if (iu < nu && iu >= p.in_lo && iu < p.in_hi) {
+            const double qx = fma(static_cast<double>(iu), p.detU[0], qx0);
+            const double qy = fma(static_cast<double>(iu), p.detU[1], qy0);
+            const double qz = fma(static_cast<double>(iu), p.detU[2], qz0);
+            const double r2 = fmax(qx * qx + qy * qy + qz * qz, 1e-20);
+            double r = rsqrtf(static_cast<float>(r2));
+            r = r * (1.5 - 0.5 * r2 * r * r);
+            const float v = in_bf16
+                ? __bfloat162float(static_cast<const __nv_bfloat16*>(in)[row * nu + iu])
+                : static_cast<const float*>(in)[row * nu + iu];
+            x = v * static_cast<float>(scale * r);
+        }
+        const __nv_bfloat16 h = __float2bfloat16_rn(x);
+        hi[row * lda + iu] = h;
+        lo[row * lda + iu] = __float2bfloat16_rn(x - __bfloat162float(h));
+    }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 tma_encode()
+{
+    static std::once_flag once;
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess && q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+bool make_map(CUtensorMap* map, const void* base, long inner, long outer, long ld_elems, int box_inner,
+    int box_outer)
+{
+    auto enc = tma_encode();
+    if (!enc) return false;
+    const cuuint64_t dims[2] = {static_cast<cuuint64_t>(inner), static_cast<cuuint64_t>(outer)};
+    const cuuint64_t strides[1] = {static_cast<cuuint64_t>(ld_elems) * 2};
+    const cuuint32_t box[2] = {static_cast<cuuint32_t>(box_inner), static_cast<cuuint32_t>(box_outer)};
+    const cuuint32_t estr[2] = {1, 1};
+    return enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box,
+               estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <int TN>
+cudaError_t launch_tn(const CUtensorMap& ah, const CUtensorMap& al, const CUtensorMap& th,
+    const CUtensorMap& tl, long rows, int nu, int nv, int kchunks, const FdkPreweightView* pwv,
+    float* C, int ldc, int* err, cudaStream_t s)
+{
+    const size_t smem = 1024 + STAGES * (kAStageBytes + TN * TK * 2) + (2 * STAGES + 1) * 8 + 16;
+    auto k = ramp_tc_kernel<TN>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    const dim3 grid((nu + TN - 1) / TN, static_cast<unsigned>((rows + TM - 1) / TM));
+    k<<<grid, 128, smem, s>>>(ah, al, th, tl, rows, nu, nv, kchunks, pwv, C, ldc, err);
+    return cudaGetLastError();
+}
+
+} // namespace
+
+int tc_filter_tile_n(int nu)
+{
+    // fewest padded columns, then the widest tile
+    int best = 0;
+    long best_cols = 0;
+    for (int tn : {256, 192, 128, 64}) {
+        const long cols = static_cast<long>((nu + tn - 1) / tn) * tn;
+        if (best == 0 || cols < best_cols) { best = tn; best_cols = cols; }
+    }
+    return best;
+}
+
+bool tcgen05_filter_supported(int nu) { return tma_encode() != nullptr && nu >= 16; }
+
+int tc_filter_lda(int nu) { return (nu + TK - 1) / TK * TK; }
+
+cudaError_t launch_fdk_preweight_split_bf16(const void* proj, int proj_dtype,
+    const FdkPreweightView* pw, int n_views, int nu, int nv, int ld, __nv_bfloat16* hi,
+    __nv_bfloat16* lo, cudaStream_t s)
+{
+    const long rows = static_cast<long>(n_views) * nv;
+    if (rows <= 0) return cudaSuccess;
+    preweight_split_kernel<<<static_cast<unsigned>(rows), 128, 0, s>>>(proj,
+        proj_dtype == YKB_DTYPE_BF16 ? 1 : 0, pw, nu, nv, ld, hi, lo);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fdk_ramp_tcgen05(const __nv_bfloat16* a_hi, const __nv_bfloat16* a_lo,
+    const __nv_bfloat16* t_hi, const __nv_bfloat16* t_lo, int rows, int nu, int ld,
+    const FdkPreweightView* pwv, int nv, float* out, int ldc, int* err, cudaStream_t s)
+{
+    if (rows <= 0) return cudaSuccess;
+    const int tn = tc_filter_tile_n(nu);
+    CUtensorMap ah, al, th, tl;
+    // A: [rows][ld] K-major, box 64 x 128; T: [nu][ld] K-major, box 64 x TN
+    if (!make_map(&ah, a_hi, nu, rows, ld, TK, TM) || !make_map(&al, a_lo, nu, rows, ld, TK, TM) ||
+        !make_map(&th, t_hi, nu, nu, ld, TK, tn) || !make_map(&tl, t_lo, nu, nu, ld, TK, tn))
+        return cudaErrorInvalidValue;
+    const int kchunks = (nu + TK - 1) / TK;
+    switch (tn) {
+    case 256: return launch_tn<256>(ah, al, th, tl, rows, nu, nv, kchunks, pwv, out, ldc, err, s);
+    case 192: return launch_tn<192>(ah, al, th, tl, rows, nu, nv, kchunks, pwv, out, ldc, err, s);
+    case 128: return launch_tn<128>(ah, al, th, tl, rows, nu, nv, kchunks, pwv, out, ldc, err, s);
+    default: return launch_tn<64>(ah, al, th, tl, rows, nu, nv, kchunks, pwv, out, ldc, err, s);
+    }
+}
+
+} // namespace ykb

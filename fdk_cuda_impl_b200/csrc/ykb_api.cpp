@@ -148,9 +148,11 @@ YKB_API ykb_status ykb_fdk_plan_create(const ykb_cone_view* views, int n_views, 
     p->batch_capacity = chunk_capacity(n_views, nu, nv);
     // filtered rows padded to 16 bytes: the pitch a TMA tensor map needs
     p->ld = (nu + 7) / 8 * 8;
-    const size_t chunk_elems = static_cast<size_t>(p->batch_capacity) * nu * nv;
-    const size_t filt_bytes = static_cast<size_t>(p->batch_capacity) * p->ld * nv *
-        (precision == YKB_PRECISION_BF16 ? 2 : 4);
+    p->tc_filter = precision == YKB_PRECISION_BF16 && tcgen05_filter_supported(nu);
+    p->lda = p->tc_filter ? tc_filter_lda(nu) : nu;
+    // work_a holds the preweighted rows: float, or bf16 hi + bf16 lo
+    const size_t chunk_elems = static_cast<size_t>(p->batch_capacity) * p->lda * nv;
+    const size_t filt_bytes = static_cast<size_t>(p->batch_capacity) * p->ld * nv * sizeof(float);
     cudaError_t e;
     if ((e = p->coef.alloc(sizeof(FdkViewCoef) * n_views)) != cudaSuccess ||
         (e = p->pwv.alloc(sizeof(FdkPreweightView) * n_views)) != cudaSuccess ||
@@ -170,6 +172,26 @@ YKB_API ykb_status ykb_fdk_plan_create(const ykb_cone_view* views, int n_views, 
         (e = cudaMemset(p->err_flag.ptr, 0, 4 * sizeof(int))) != cudaSuccess) {
         delete p;
         return cuda_status(e, "cudaMemcpy (FDK plan tables)");
+    }
+    if (p->tc_filter) {
+        // Toeplitz operand T[j][k] = h(j-k) split into bf16 hi and lo parts
+        const size_t tn = static_cast<size_t>(nu) * p->lda;
+        std::vector<__nv_bfloat16> thi(tn, __float2bfloat16_rn(0.f)), tlo(tn, __float2bfloat16_rn(0.f));
+        for (int j = 0; j < nu; ++j)
+            for (int k = 0; k < nu; ++k) {
+                const double v = h[static_cast<size_t>(j - k + nu - 1)];
+                const __nv_bfloat16 hb = __float2bfloat16_rn(static_cast<float>(v));
+                thi[static_cast<size_t>(j) * p->lda + k] = hb;
+                tlo[static_cast<size_t>(j) * p->lda + k] =
+                    __float2bfloat16_rn(static_cast<float>(v - static_cast<double>(__bfloat162float(hb))));
+            }
+        if ((e = p->toeplitz_hi.alloc(tn * 2)) != cudaSuccess ||
+            (e = p->toeplitz_lo.alloc(tn * 2)) != cudaSuccess ||
+            (e = cudaMemcpy(p->toeplitz_hi.ptr, thi.data(), tn * 2, cudaMemcpyHostToDevice)) != cudaSuccess ||
+            (e = cudaMemcpy(p->toeplitz_lo.ptr, tlo.data(), tn * 2, cudaMemcpyHostToDevice)) != cudaSuccess) {
+            delete p;
+            return cuda_status(e, "Toeplitz operand");
+        }
     }
     // size the shared-memory projection box of the TMA backprojection from
     // the footprints of every (tile, view) pair
@@ -230,11 +252,21 @@ ykb_status filter_chunk(ykb_fdk_plan* p, const void* proj, int proj_dtype, int f
     void* dst, int ldc, cudaStream_t s)
 {
     const FdkPreweightView* pwv = p->pwv.as<FdkPreweightView>() + first;
-    const int out_dtype = p->precision == YKB_PRECISION_BF16 ? YKB_DTYPE_BF16 : YKB_DTYPE_F32;
+    if (p->tc_filter) {
+        const size_t half = static_cast<size_t>(p->batch_capacity) * p->nv * p->lda;
+        __nv_bfloat16* a_hi = p->work_a.as<__nv_bfloat16>();
+        __nv_bfloat16* a_lo = a_hi + half;
+        YKB_TRY_CUDA(launch_fdk_preweight_split_bf16(proj, proj_dtype, pwv, count, p->nu, p->nv,
+            p->lda, a_hi, a_lo, s));
+        YKB_TRY_CUDA(launch_fdk_ramp_tcgen05(a_hi, a_lo, p->toeplitz_hi.as<__nv_bfloat16>(),
+            p->toeplitz_lo.as<__nv_bfloat16>(), count * p->nv, p->nu, p->lda, pwv, p->nv,
+            static_cast<float*>(dst), ldc, p->err_flag.as<int>(), s));
+        return YKB_OK;
+    }
     YKB_TRY_CUDA(launch_fdk_preweight(proj, proj_dtype, pwv, count, p->nu, p->nv,
         p->work_a.as<float>(), s));
     YKB_TRY_CUDA(launch_fdk_ramp_fp32(p->work_a.as<float>(), p->ramp.as<float>(), pwv, count,
-        p->nu, p->nv, dst, out_dtype, ldc, s));
+        p->nu, p->nv, dst, YKB_DTYPE_F32, ldc, s));
     return YKB_OK;
 }
 
@@ -268,7 +300,7 @@ YKB_API ykb_status ykb_fdk_filter(ykb_fdk_plan* p, const void* d_proj, int proj_
     DeviceGuard guard(p->device);
     const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const size_t view_elems = static_cast<size_t>(p->nu) * p->nv;
-    const size_t out_b = p->precision == YKB_PRECISION_BF16 ? 2 : 4;
+    const size_t out_b = sizeof(float);
     for (int c = 0; c < n_views; c += p->batch_capacity) {
         const int cnt = std::min(p->batch_capacity, n_views - c);
         const char* in = static_cast<const char*>(d_proj) + c * view_elems * dtype_bytes(proj_dtype);
@@ -302,7 +334,7 @@ YKB_API ykb_status ykb_fdk_execute(ykb_fdk_plan* p, const void* d_proj, int proj
     DeviceGuard guard(p->device);
     const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const size_t view_elems = static_cast<size_t>(p->nu) * p->nv;
-    const int filt_dtype = p->precision == YKB_PRECISION_BF16 ? YKB_DTYPE_BF16 : YKB_DTYPE_F32;
+    const int filt_dtype = YKB_DTYPE_F32;
     for (int c = 0; c < n_views; c += p->batch_capacity) {
         const int cnt = std::min(p->batch_capacity, n_views - c);
         const char* in = static_cast<const char*>(d_proj) + c * view_elems * dtype_bytes(proj_dtype);
@@ -333,6 +365,7 @@ YKB_API ykb_status ykb_fdk_check(ykb_fdk_plan* p, ykb_stream stream)
     if (word & 1) msg += " a pipeline wait timed out;";
     if (word & 2) msg += " a voxel column left its projection box;";
     if (word & 4) msg += " a staged copy was not 128-byte aligned (skipped);";
+    if (word & 8) msg += " a tensor-core filter pipeline wait timed out;";
     return fail(YKB_ERR_CUDA, msg);
 }
 

@@ -164,9 +164,10 @@ cudaError_t launch_fdk_preweight_split_bf16(const void* proj, int proj_dtype,
 cudaError_t launch_fdk_ramp_tcgen05(const __nv_bfloat16* a_hi,
     const __nv_bfloat16* a_lo, const __nv_bfloat16* t_hi,
     const __nv_bfloat16* t_lo, int rows, int nu, int ld,
-    const FdkPreweightView* pwv, int nv, __nv_bfloat16* out, int* err_flag,
+    const FdkPreweightView* pwv, int nv, float* out, int ldc, int* err_flag,
     cudaStream_t s);
 bool tcgen05_filter_supported(int nu);
+int tc_filter_lda(int nu);
 cudaError_t launch_fdk_backproject(const void* filtered, int dtype,
     const FdkViewCoef* coef, int n_views, int nu, int nv, int ld,
     const VolumeGrid& grid, bool axial, float* vol, int accumulate,
@@ -207,6 +208,7 @@ struct ykb_fdk_plan {
     bool tc_filter = false;
     int batch_capacity = 0;      // views the workspace holds
     int ld = 0;                  // row pitch (elements) of the filtered workspace
+    int lda = 0;                 // row pitch of the bf16 GEMM operands (tensor-core filter)
     bool use_tma = false;        // TMA-staged backprojection
     int tma_bw = 0, tma_bh = 0;  // its projection box
     std::vector<ykb::FdkDerived> derived;
@@ -214,7 +216,7 @@ struct ykb_fdk_plan {
     ykb::DeviceBuffer pwv;       // FdkPreweightView[n_views]
     ykb::DeviceBuffer ramp;      // float[2*nu-1]
     ykb::DeviceBuffer toeplitz_hi, toeplitz_lo;  // bf16 [nu][ld] (BF16 plans)
-    ykb::DeviceBuffer work_a;    // preweighted rows (float) or bf16 hi/lo
+    ykb::DeviceBuffer work_a;    // preweighted rows: float, or bf16 hi then lo
     ykb::DeviceBuffer work_filtered;  // filtered projections (plan dtype)
     ykb::DeviceBuffer err_flag;  // int[4]: device error word, box pre-pass scratch
 };

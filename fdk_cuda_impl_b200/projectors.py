@@ -64,7 +64,7 @@ class FdkPlan:
 
     @property
     def filtered_dtype(self):
-        return torch.bfloat16 if self.precision == L.PRECISION_BF16 else torch.float32
+        return torch.float32
 
     def workspace_bytes(self) -> int:
         return int(self.lib.ykb_fdk_workspace_bytes(self._h))

@@ -101,9 +101,10 @@ typedef enum {
 } ykb_status;
 
 typedef enum {
-    YKB_PRECISION_FP32 = 0, /* FP32 ramp filter, FP32 filtered projections */
-    YKB_PRECISION_BF16 = 1  /* BF16 tensor-core Toeplitz filter with split
-                               hi/lo correction, BF16 filtered projections */
+    YKB_PRECISION_FP32 = 0, /* FP32 ramp filter */
+    YKB_PRECISION_BF16 = 1  /* BF16 tensor-core (tcgen05) Toeplitz filter with
+                               split hi/lo correction and FP32 accumulation;
+                               pairs with BF16 projection input */
 } ykb_precision;
 
 typedef enum { YKB_DTYPE_F32 = 0, YKB_DTYPE_BF16 = 1 } ykb_dtype;
@@ -152,8 +153,7 @@ YKB_API ykb_status ykb_fdk_execute(ykb_fdk_plan* plan, const void* d_proj,
     int clear_output, ykb_stream stream);
 
 /* Stage entry: preweight + ramp filter only; d_filtered receives
- * [n_views][nv][nu] in the plan's filtered dtype (float for FP32 plans,
- * bf16 for BF16 plans).  Replaces PreweightProcessor::apply +
+ * [n_views][nv][nu] float.  Replaces PreweightProcessor::apply +
  * FilterProcessor::apply (.../FDK/YkFDKPreWeightProcessor.hpp,
  * .../FDK/YkFDKFilterProcessor.hpp:84-122). */
 YKB_API ykb_status ykb_fdk_filter(ykb_fdk_plan* plan, const void* d_proj,

@@ -190,3 +190,28 @@ def test_fdk_tma_matches_global_path(oracle, cuda_device):
     direct = fp32.backproject(shifted)
     fp32.check()
     assert K.rel_rmse(staged.cpu().numpy(), direct.cpu().numpy()) < 1e-6
+
+
+@pytest.mark.parametrize("nu,nv,views", [(96, 64, 12), (53, 41, 7), (192, 24, 5), (384, 8, 3)])
+def test_tc_filter_stage(oracle, cuda_device, nu, nv, views):
+    # tcgen05 BF16 Toeplitz filter with hi/lo split against the FP64 filter:
+    # the three-product split keeps about 16 mantissa bits
+    import torch
+    from fdk_cuda_impl_b200.geometry import CircularScan
+    from fdk_cuda_impl_b200.projectors import FdkPlan
+    scan = CircularScan(views, views, 500.0, 1000.0, nu, nv, 1.0, 1.0)
+    v = scan.views()
+    case = K.c1_small()
+    p = oracle.uniform((views, nv, nu), 0.0, 2.0, 40 + nu)
+    plan = FdkPlan(v, nu, nv, scan.scan_range, case.grid, case.filt, precision="bf16")
+    got = plan.filter(torch.from_numpy(p).cuda()).cpu().numpy()
+    plan.check()
+    ref = oracle.fdk_filter(v, nu, nv, scan.scan_range, K.oracle_filter(oracle, case.filt), p)
+    assert got.dtype == np.float32
+    assert K.rel_rmse(got, ref) <= 1e-4
+
+
+def test_bf16_form_c1(oracle, cuda_device):
+    # BF16 projections in, tensor-core filter: end-to-end bound 1e-3
+    out, ref, *_ = _run_case(oracle, K.c1(), precision="bf16", proj_dtype="bf16")
+    assert K.rel_rmse(out, ref) <= BF16_TOL
