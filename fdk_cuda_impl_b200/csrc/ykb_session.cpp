@@ -1,0 +1,393 @@
+// C++ Session layer over the C-ABI (include/ykb_session.hpp).  Validation
+// order, error codes and streaming rules follow ReconstructionSession
+// (src/interface/YkReconstructionApi.cpp:137-397) and Session::executeFdk_ /
+// executeFp_ (src/interface/YkSession.cpp:693-728, 881-939).
+#include "ykb_session.hpp"
+#include "ykb_internal.hpp"
+
+#include <cmath>
+#include <cstddef>
+#include <new>
+#include <string>
+#include <vector>
+
+namespace YK {
+namespace {
+
+bool has_bytes(uint32_t actual, size_t required) { return actual >= required; }
+
+bool valid_location(EMemoryLocation l) { return l == EMemoryLocation::Host || l == EMemoryLocation::Device; }
+
+// resolveParkerEnabled (include/YKCBCT/interface/YkSystemReconstruction.hpp:29-39)
+bool parker_enabled(const SSystemConfig& g, const SReconstructionSpec& r)
+{
+    if (r.fdk.parker.mode == EParkerMode::Enabled) return true;
+    if (r.fdk.parker.mode == EParkerMode::Disabled) return false;
+    constexpr float kTwoPi = 6.28318530717958647692f;
+    const float range = kTwoPi * static_cast<float>(g.circular.total_views) /
+        static_cast<float>(g.circular.views_per_turn);
+    return range < kTwoPi - 1e-5f;
+}
+
+// SRigidTransform::aroundEulerPoint(centre, rx, ry, rz).inverse() applied to
+// a view (include/YKCBCT/geometry/YkRigidTransform.hpp,
+// transformProjectionGeometry in YkProjectionGeometry.hpp:229-247)
+void pose_views(std::vector<ykb_cone_view>& views, const SForwardProjectionPose& pose,
+    const float3& centre)
+{
+    const double cx = std::cos(pose.rotation_x_rad), sx = std::sin(pose.rotation_x_rad);
+    const double cy = std::cos(pose.rotation_y_rad), sy = std::sin(pose.rotation_y_rad);
+    const double cz = std::cos(pose.rotation_z_rad), sz = std::sin(pose.rotation_z_rad);
+    // R = Rz Ry Rx; the inverse rotation is R^T about the same centre
+    const double R[3][3] = {
+        {cz * cy, cz * sy * sx - sz * cx, cz * sy * cx + sz * sx},
+        {sz * cy, sz * sy * sx + cz * cx, sz * sy * cx - cz * sx},
+        {-sy, cy * sx, cy * cx}};
+    auto inv_vec = [&](const ykb_float4& v) {
+        ykb_float4 r = v;
+        r.x = static_cast<float>(R[0][0] * v.x + R[1][0] * v.y + R[2][0] * v.z);
+        r.y = static_cast<float>(R[0][1] * v.x + R[1][1] * v.y + R[2][1] * v.z);
+        r.z = static_cast<float>(R[0][2] * v.x + R[1][2] * v.y + R[2][2] * v.z);
+        return r;
+    };
+    auto inv_pt = [&](const ykb_float4& p) {
+        ykb_float4 d = p;
+        d.x = p.x - centre.x; d.y = p.y - centre.y; d.z = p.z - centre.z;
+        ykb_float4 r = inv_vec(d);
+        r.x += centre.x; r.y += centre.y; r.z += centre.z;
+        return r;
+    };
+    for (auto& v : views) {
+        v.src = inv_pt(v.src);
+        v.detS = inv_pt(v.detS);
+        v.detU = inv_vec(v.detU);
+        v.detV = inv_vec(v.detV);
+    }
+}
+
+struct DeviceScratch {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    bool ensure(size_t n)
+    {
+        if (bytes >= n) return true;
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+        if (cudaMalloc(&ptr, n) != cudaSuccess) { cudaGetLastError(); return false; }
+        bytes = n;
+        return true;
+    }
+    void reset()
+    {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+};
+
+class Session final : public IReconstructionSession {
+public:
+    ~Session() override { release(); }
+
+    bool initialize(const SSystemSpec& system) override
+    {
+        release();
+        clear_();
+        if (!has_bytes(system.struct_size, offsetof(SSystemSpec, device) + sizeof(system.device)))
+            return fail_(EApiErrorCode::InvalidConfig, "SSystemSpec struct_size is too small (truncated)");
+        if (system.api_version != 2)
+            return fail_(EApiErrorCode::InvalidConfig, "unsupported SSystemSpec api_version");
+        const auto& g = system.geometry;
+        const auto& r = system.reconstruction;
+        if (static_cast<int>(g.detector) < 0 || static_cast<int>(g.detector) > 1 ||
+            static_cast<int>(g.trajectory) < 0 || static_cast<int>(g.trajectory) > 3 ||
+            static_cast<int>(r.pipeline) < 0 || static_cast<int>(r.pipeline) > 11)
+            return fail_(EApiErrorCode::InvalidConfig, "invalid pipeline, detector or trajectory enum");
+        if (g.detector != EDetectorKind::Flat || g.trajectory != ETrajectoryKind::Circular)
+            return fail_(EApiErrorCode::UnsupportedCombination,
+                "this library implements the flat-panel circular trajectory only");
+        if (r.pipeline != EPipeline::FDK && r.pipeline != EPipeline::ForwardProjection)
+            return fail_(EApiErrorCode::UnsupportedCombination,
+                "this library implements the FDK and ForwardProjection pipelines only");
+        if (static_cast<int>(r.forward_projector) < 0 || static_cast<int>(r.forward_projector) > 3 ||
+            static_cast<int>(r.back_projector) < 0 || static_cast<int>(r.back_projector) > 5)
+            return fail_(EApiErrorCode::InvalidConfig, "invalid forward/back projector selection");
+        const auto& pose = g.forward_projection_pose;
+        if (!std::isfinite(pose.rotation_x_rad) || !std::isfinite(pose.rotation_y_rad) ||
+            !std::isfinite(pose.rotation_z_rad))
+            return fail_(EApiErrorCode::InvalidGeometry,
+                "Forward-projection volume rotation must contain finite radians");
+        if (r.pipeline == EPipeline::ForwardProjection &&
+            r.forward_projector != EForwardProjector::Joseph)
+            // resolveForwardProjector maps Automatic to Siddon for flat
+            // detectors (src/interface/YkProjectorSelection.hpp:11-24)
+            return fail_(EApiErrorCode::UnsupportedCombination,
+                "forward projection here is Joseph: request EForwardProjector::Joseph");
+        if (g.volume.nx <= 0 || g.volume.ny <= 0 || g.volume.nz <= 0 ||
+            !(g.volume.voxel_x_mm > 0.f) || !(g.volume.voxel_y_mm > 0.f) ||
+            !(g.volume.voxel_z_mm > 0.f) || !std::isfinite(g.volume.center_mm.x) ||
+            !std::isfinite(g.volume.center_mm.y) || !std::isfinite(g.volume.center_mm.z))
+            return fail_(EApiErrorCode::InvalidGeometry, "invalid volume grid");
+
+        ykb_circular_flat spec{};
+        spec.total_views = g.circular.total_views;
+        spec.views_per_turn = g.circular.views_per_turn;
+        spec.start_angle_rad = g.circular.start_angle_rad;
+        spec.rotation_direction = g.circular.rotation_direction;
+        spec.sid_mm = g.circular.sid_mm;
+        spec.sdd_mm = g.circular.sdd_mm;
+        spec.z_mm = g.circular.z_mm;
+        spec.source_offset_mm[0] = g.circular.source_offset_mm.x;
+        spec.source_offset_mm[1] = g.circular.source_offset_mm.y;
+        spec.source_offset_mm[2] = g.circular.source_offset_mm.z;
+        spec.channels = g.flat_detector.channels;
+        spec.rows = g.flat_detector.rows;
+        spec.channel_size_mm = g.flat_detector.channel_size_mm;
+        spec.row_size_mm = g.flat_detector.row_size_mm;
+        spec.offset_unv_mm[0] = g.flat_detector.pose.offset_unv_mm.x;
+        spec.offset_unv_mm[1] = g.flat_detector.pose.offset_unv_mm.y;
+        spec.offset_unv_mm[2] = g.flat_detector.pose.offset_unv_mm.z;
+        spec.tilt_u_rad = g.flat_detector.pose.tilt_u_rad;
+        spec.tilt_v_rad = g.flat_detector.pose.tilt_v_rad;
+        spec.tilt_n_rad = g.flat_detector.pose.tilt_n_rad;
+        if (spec.total_views <= 0)
+            return fail_(EApiErrorCode::InvalidGeometry, "total_views must be positive");
+        views_.assign(static_cast<size_t>(spec.total_views), ykb_cone_view{});
+        if (ykb_build_circular_flat(&spec, views_.data(), spec.total_views) != YKB_OK)
+            return fail_(EApiErrorCode::InvalidGeometry, ykb_last_error());
+
+        volume_ = ykb_volume{g.volume.nx, g.volume.ny, g.volume.nz, g.volume.voxel_x_mm,
+            g.volume.voxel_y_mm, g.volume.voxel_z_mm, g.volume.center_mm.x, g.volume.center_mm.y,
+            g.volume.center_mm.z};
+        nu_ = spec.channels;
+        nv_ = spec.rows;
+        device_ = system.device;
+        pipeline_ = r.pipeline;
+        int count = 0;
+        if (device_ < 0 || cudaGetDeviceCount(&count) != cudaSuccess || device_ >= count) {
+            cudaGetLastError();
+            return fail_(EApiErrorCode::InvalidGeometry, "invalid GPU selection");
+        }
+        ykb::DeviceGuard guard(device_);
+        if (pipeline_ == EPipeline::FDK) {
+            const auto& f = r.fdk.filter;
+            if (static_cast<int>(f.type) < 0 || static_cast<int>(f.type) > 9 ||
+                !std::isfinite(f.cutoff) || !(f.cutoff > 0.f) || f.cutoff > .5f ||
+                !std::isfinite(f.gain) || !(f.gain > 0.f) || !std::isfinite(f.butterworth_order) ||
+                !(f.butterworth_order > 0.f) || !std::isfinite(f.kaiser_beta) || f.kaiser_beta < 0.f ||
+                !std::isfinite(f.tukey_alpha) || f.tukey_alpha < 0.f || f.tukey_alpha > 1.f) {
+                views_.clear();
+                return fail_(EApiErrorCode::InvalidGeometry, "invalid analytic filter parameters");
+            }
+            if (parker_enabled(g, r)) {
+                views_.clear();
+                return fail_(EApiErrorCode::UnsupportedCombination,
+                    "short-scan (Parker) FDK is not provided by this library");
+            }
+            const ykb_filter filt{static_cast<int>(f.type), f.cutoff, f.gain, f.butterworth_order,
+                f.kaiser_beta, f.tukey_alpha};
+            const float range = ykb_regular_scan_range(spec.total_views, spec.views_per_turn);
+            if (ykb_fdk_plan_create(views_.data(), spec.total_views, nu_, nv_, range, &volume_, &filt,
+                    YKB_PRECISION_FP32, device_, &fdk_) != YKB_OK) {
+                const std::string msg = ykb_last_error();
+                release();
+                return fail_(EApiErrorCode::InvalidGeometry, msg.c_str());
+            }
+        } else {
+            if (pose.enabled) pose_views(views_, pose, g.volume.center_mm);
+            if (ykb_joseph_plan_create(views_.data(), spec.total_views, nu_, nv_, &volume_, device_,
+                    &joseph_) != YKB_OK) {
+                const std::string msg = ykb_last_error();
+                release();
+                return fail_(EApiErrorCode::InvalidGeometry, msg.c_str());
+            }
+        }
+        if (cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking) != cudaSuccess) {
+            cudaGetLastError();
+            release();
+            return fail_(EApiErrorCode::CudaError, "cudaStreamCreate failed");
+        }
+        view_count_ = spec.total_views;
+        received_ = 0;
+        initialized_ = true;
+        return true;
+    }
+
+    bool execute(const SExecutionRequest& request) override
+    {
+        clear_();
+        if (!initialized_)
+            return fail_(EApiErrorCode::StreamingStateError, "the session is not initialized");
+        if (!has_bytes(request.struct_size,
+                offsetof(SExecutionRequest, iteration_count) + sizeof(request.iteration_count)))
+            return fail_(EApiErrorCode::InvalidConfig, "SExecutionRequest struct_size is too small (truncated)");
+        if (request.struct_size > offsetof(SExecutionRequest, progress_callback) &&
+            request.struct_size < offsetof(SExecutionRequest, progress_user_data) +
+                sizeof(request.progress_user_data))
+            return fail_(EApiErrorCode::InvalidConfig, "SExecutionRequest progress tail is truncated");
+        if (request.api_version != 2)
+            return fail_(EApiErrorCode::InvalidConfig, "unsupported SExecutionRequest api_version");
+        if (!request.projection.data || !request.volume.data ||
+            !valid_location(request.projection.location) || !valid_location(request.volume.location))
+            return fail_(EApiErrorCode::InvalidBuffer, "null projection/volume buffer or invalid location");
+        const int offset = request.view_offset;
+        const int count = request.view_count > 0 ? request.view_count : view_count_;
+        if (offset < 0 || count <= 0 || offset > view_count_ - count)
+            return fail_(EApiErrorCode::InvalidConfig, "view_offset/view_count outside the prepared views");
+        const bool fdk = pipeline_ == EPipeline::FDK;
+        if (fdk) {
+            if (offset != received_)
+                return fail_(EApiErrorCode::StreamingStateError,
+                    "FDK batches must be submitted with contiguous view_offset (no gaps or repeats)");
+            if (received_ > 0 && request.clear_output)
+                return fail_(EApiErrorCode::StreamingStateError,
+                    "only the first FDK batch may set clear_output");
+        } else if (offset != 0 || count != view_count_) {
+            return fail_(EApiErrorCode::StreamingStateError,
+                "this pipeline takes the complete view sequence from view_offset 0");
+        }
+        const size_t view_elems = static_cast<size_t>(nu_) * nv_;
+        const size_t vol_elems = static_cast<size_t>(volume_.nx) * volume_.ny * volume_.nz;
+        if (request.projection.element_count < view_elems * count ||
+            request.volume.element_count < vol_elems)
+            return fail_(EApiErrorCode::InvalidBuffer,
+                "projection/volume element_count smaller than this execution needs");
+        ykb::DeviceGuard guard(device_);
+        const bool ok = fdk ? run_fdk_(request, offset, count) : run_fp_(request, count);
+        if (!ok) return false;
+        if (fdk) received_ += count;
+        return true;
+    }
+
+    bool isInitialized() const override { return initialized_; }
+    EApiErrorCode lastError() const override { return code_; }
+    const char* lastErrorMessage() const override { return message_.c_str(); }
+
+    void reset() override { received_ = 0; }
+
+    void release() override
+    {
+        if (stream_) cudaStreamSynchronize(stream_);
+        if (fdk_) ykb_fdk_plan_destroy(fdk_);
+        if (joseph_) ykb_joseph_plan_destroy(joseph_);
+        fdk_ = nullptr;
+        joseph_ = nullptr;
+        proj_scratch_.reset();
+        vol_scratch_.reset();
+        if (stream_) cudaStreamDestroy(stream_);
+        stream_ = nullptr;
+        views_.clear();
+        view_count_ = received_ = 0;
+        initialized_ = false;
+    }
+
+private:
+    bool cuda_fail_(cudaError_t e, const char* what)
+    {
+        cudaGetLastError();
+        return fail_(EApiErrorCode::CudaError,
+            (std::string(what) + ": " + cudaGetErrorString(e)).c_str());
+    }
+
+    bool run_fdk_(const SExecutionRequest& r, int offset, int count)
+    {
+        const size_t proj_bytes = static_cast<size_t>(nu_) * nv_ * count * sizeof(float);
+        const size_t vol_bytes = static_cast<size_t>(volume_.nx) * volume_.ny * volume_.nz * sizeof(float);
+        const float* d_proj = r.projection.data;
+        if (r.projection.location == EMemoryLocation::Host) {
+            if (!proj_scratch_.ensure(proj_bytes))
+                return fail_(EApiErrorCode::CudaError, "device projection staging allocation failed");
+            cudaError_t e = cudaMemcpyAsync(proj_scratch_.ptr, r.projection.data, proj_bytes,
+                cudaMemcpyHostToDevice, stream_);
+            if (e != cudaSuccess) return cuda_fail_(e, "projection upload");
+            d_proj = static_cast<const float*>(proj_scratch_.ptr);
+        }
+        float* d_vol = r.volume.data;
+        if (r.volume.location == EMemoryLocation::Host) {
+            // a host volume accumulates in device scratch across batches and is
+            // copied back once the last batch has arrived
+            if (!vol_scratch_.ensure(vol_bytes))
+                return fail_(EApiErrorCode::CudaError, "device volume scratch allocation failed");
+            d_vol = static_cast<float*>(vol_scratch_.ptr);
+        }
+        if (ykb_fdk_execute(fdk_, d_proj, YKB_DTYPE_F32, offset, count, d_vol,
+                r.clear_output ? 1 : 0, stream_) != YKB_OK)
+            return fail_(EApiErrorCode::CudaError, ykb_last_error());
+        if (r.volume.location == EMemoryLocation::Host && received_ + count == view_count_) {
+            const cudaError_t e = cudaMemcpyAsync(r.volume.data, d_vol, vol_bytes,
+                cudaMemcpyDeviceToHost, stream_);
+            if (e != cudaSuccess) return cuda_fail_(e, "volume download");
+        }
+        if (ykb_fdk_check(fdk_, stream_) != YKB_OK)
+            return fail_(EApiErrorCode::CudaError, ykb_last_error());
+        return true;
+    }
+
+    bool run_fp_(const SExecutionRequest& r, int count)
+    {
+        const size_t proj_bytes = static_cast<size_t>(nu_) * nv_ * count * sizeof(float);
+        const size_t vol_bytes = static_cast<size_t>(volume_.nx) * volume_.ny * volume_.nz * sizeof(float);
+        const float* d_vol = r.volume.data;
+        if (r.volume.location == EMemoryLocation::Host) {
+            if (!vol_scratch_.ensure(vol_bytes))
+                return fail_(EApiErrorCode::CudaError, "device volume scratch allocation failed");
+            const cudaError_t e = cudaMemcpyAsync(vol_scratch_.ptr, r.volume.data, vol_bytes,
+                cudaMemcpyHostToDevice, stream_);
+            if (e != cudaSuccess) return cuda_fail_(e, "volume upload");
+            d_vol = static_cast<const float*>(vol_scratch_.ptr);
+        }
+        float* d_proj = r.projection.data;
+        if (r.projection.location == EMemoryLocation::Host) {
+            if (!proj_scratch_.ensure(proj_bytes))
+                return fail_(EApiErrorCode::CudaError, "device projection scratch allocation failed");
+            d_proj = static_cast<float*>(proj_scratch_.ptr);
+        }
+        if (ykb_joseph_fp(joseph_, d_vol, d_proj, 0, stream_) != YKB_OK)
+            return fail_(EApiErrorCode::CudaError, ykb_last_error());
+        if (r.projection.location == EMemoryLocation::Host) {
+            const cudaError_t e = cudaMemcpyAsync(r.projection.data, d_proj, proj_bytes,
+                cudaMemcpyDeviceToHost, stream_);
+            if (e != cudaSuccess) return cuda_fail_(e, "projection download");
+        }
+        const cudaError_t e = cudaStreamSynchronize(stream_);
+        if (e != cudaSuccess) return cuda_fail_(e, "forward projection");
+        return true;
+    }
+
+    bool fail_(EApiErrorCode code, const char* message)
+    {
+        code_ = code;
+        message_ = message ? message : "";
+        return false;
+    }
+    void clear_()
+    {
+        code_ = EApiErrorCode::None;
+        message_.clear();
+    }
+
+    std::vector<ykb_cone_view> views_;
+    ykb_volume volume_{};
+    int nu_ = 0, nv_ = 0, device_ = 0;
+    EPipeline pipeline_ = EPipeline::FDK;
+    int view_count_ = 0, received_ = 0;
+    bool initialized_ = false;
+    ykb_fdk_plan* fdk_ = nullptr;
+    ykb_joseph_plan* joseph_ = nullptr;
+    cudaStream_t stream_ = nullptr;
+    DeviceScratch proj_scratch_, vol_scratch_;
+    EApiErrorCode code_ = EApiErrorCode::None;
+    std::string message_;
+};
+
+} // namespace
+
+IReconstructionSession* ReconstructionSessionFactory::create()
+{
+    return new (std::nothrow) Session();
+}
+
+void ReconstructionSessionFactory::destroy(IReconstructionSession* session) { delete session; }
+
+} // namespace YK
