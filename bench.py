@@ -14,9 +14,10 @@ e2e     = the same metric through the C-ABI with host buffers: each step
 Inputs (1.7 GB projections, 0.54 GB volume) exceed the 126 MB L2, so no
 flush is needed between steps.
 
---impl reference times the CPU implementation of the path (the FP64
-multithreaded transcription of the reference's loops; the reference has no
-CPU path of its own) on a bounded sample of the same workload.
+--impl reference times the reference's own implementation on the same
+workload: its CUDA build (the reference has no CPU path), compiled for sm_100a
+from its sources into oracle/_ref, through its stock FDK pipeline; the FP64
+CPU oracle on a bounded sample when that build is absent.
 """
 from __future__ import annotations
 
@@ -159,30 +160,86 @@ def cpu_baseline(n_views_sample=96, z_slab=64):
                       f"backprojected into a 512x512x{z_slab} slab, FP64, {dt:.1f} s"}
 
 
+def make_workload(rank: int, local: int):
+    """The benchmark's seeded inputs on cuda:local: ellipsoid phantom (one
+    independent object per rank), Joseph forward projection, Poisson noise."""
+    import torch
+    from fdk_cuda_impl_b200 import CircularScan, VolumeGrid
+    from fdk_cuda_impl_b200 import phantom as PH
+    from fdk_cuda_impl_b200.projectors import JosephPlan
+    scan = CircularScan(N_VIEWS, N_VIEWS, SID, SDD, N_DET, N_DET, PIX_MM, PIX_MM)
+    grid = VolumeGrid.cube(N_VOX, VOX_MM)
+    views = scan.views()
+    ell = PH.random_ellipsoids(1000 + rank, N_ELL)
+    phantom = PH.voxelize(grid, ell, device=f"cuda:{local}")
+    jp = JosephPlan(views, N_DET, N_DET, grid, device=local)
+    proj = jp.forward(phantom)
+    jp.close()
+    del jp, phantom
+    PH.poisson_noise_(proj, I0, seed=7 + rank)
+    torch.cuda.synchronize()
+    return scan, grid, views, proj
+
+
 def run_reference(args):
+    """The reference's own implementation of the path on the same workload.
+
+    The reference has no CPU path (its FDK and Joseph operators are CUDA
+    only), so its own implementation is its CUDA build: oracle/_ref/libykref.so,
+    compiled for sm_100a from the reference sources by oracle/ref_build.py,
+    driven through its stock FdkPipeline (the path its Session runs).  value =
+    projections already on the device (chunked device-to-device uploads inside
+    the pipeline), e2e = host projections and the volume read back, as its
+    Session requires.  Without that build, the FP64 CPU oracle port is timed on
+    a bounded sample instead.  Under torchrun only rank 0 runs."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    from oracle import oracle as O
-    for _ in range(args.warmup):
-        cpu_baseline(n_views_sample=8, z_slab=8)
-    vals = []
-    for _ in range(args.steps):
-        vals.append(cpu_baseline(n_views_sample=36, z_slab=32))
-    value = sum(v["value"] for v in vals) / len(vals)
-    ms = UPDATES / (value * 1e9) * 1e3
-    cb = dict(vals[-1])
-    cb["value"] = value
-    print(json.dumps({
-        "metric": "FDK backprojection GUPS (voxel x view updates/s)", "value": value,
-        "unit": "GUPS", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic", "impl": "reference",
-        "config": {"workload": WORKLOAD, "volume": [N_VOX] * 3, "views": N_VIEWS,
-                   "detector": [N_DET, N_DET], "sample_per_step": cb["sample"]},
-        "cpu_baseline": cb,
-        "e2e": {"value": value, "unit": "GUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }), flush=True)
+    from oracle import ref as R
+    cfg = {"workload": WORKLOAD, "volume": [N_VOX] * 3, "voxel_mm": VOX_MM, "views": N_VIEWS,
+           "detector": [N_DET, N_DET], "pixel_mm": PIX_MM, "sid_sdd_mm": [SID, SDD],
+           "ellipsoids": N_ELL, "noise_i0": I0, "filter": "ramlak"}
+    line = {"metric": "FDK backprojection GUPS (voxel x view updates/s)", "unit": "GUPS",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "data": "synthetic", "impl": "reference"}
+    import torch
+    if R.available() and torch.cuda.is_available():
+        from fdk_cuda_impl_b200 import RampFilter
+        scan, grid, _, proj = make_workload(0, 0)
+        h_proj = proj.cpu().numpy()
+        del proj
+        torch.cuda.empty_cache()
+        ms_dev, ms_host = R.fdk_time(scan, grid, RampFilter(), h_proj, warmup=args.warmup,
+                                     reps=args.steps, timeout=1800)
+        value = UPDATES / (ms_dev * 1e-3) / 1e9
+        cb = cpu_baseline(n_views_sample=24, z_slab=32)
+        line.update({
+            "value": value, "ms_per_step": ms_dev, "dtype": "f32",
+            "config": dict(cfg, implementation="reference CUDA build (YKCBCT FdkPipeline, "
+                           "sm_100a, -O3 -use_fast_math), oracle/_ref/libykref.so",
+                           l2="inputs larger than L2"),
+            "e2e": {"value": UPDATES / (ms_host * 1e-3) / 1e9, "unit": "GUPS",
+                    "ms_per_step": ms_host, "h2d_bytes_per_step": int(h_proj.nbytes),
+                    "d2h_bytes_per_step": int(4 * N_VOX ** 3)},
+            "cpu_baseline": cb,
+            "gpu_launches": None,
+        })
+    else:
+        from oracle import oracle as O  # noqa: F401  (the CPU port)
+        for _ in range(args.warmup):
+            cpu_baseline(n_views_sample=8, z_slab=8)
+        vals = [cpu_baseline(n_views_sample=36, z_slab=32) for _ in range(args.steps)]
+        value = sum(v["value"] for v in vals) / len(vals)
+        cb = dict(vals[-1], value=value)
+        line.update({
+            "value": value, "ms_per_step": UPDATES / (value * 1e9) * 1e3, "dtype": "f64",
+            "config": dict(cfg, implementation="FP64 CPU oracle port (no reference build present)",
+                           sample_per_step=cb["sample"]),
+            "cpu_baseline": cb,
+            "e2e": {"value": value, "unit": "GUPS", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+        })
+    print(json.dumps(line), flush=True)
 
 
 def main():
@@ -207,18 +264,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device(f"cuda:{local}"))
 
-    scan = CircularScan(N_VIEWS, N_VIEWS, SID, SDD, N_DET, N_DET, PIX_MM, PIX_MM)
-    grid = VolumeGrid.cube(N_VOX, VOX_MM)
-    views = scan.views()
-    # independent object per rank (weak scaling, no data-path collective)
-    ell = PH.random_ellipsoids(1000 + rank, N_ELL)
-    phantom = PH.voxelize(grid, ell, device=f"cuda:{local}")
-    jp = JosephPlan(views, N_DET, N_DET, grid, device=local)
-    proj = jp.forward(phantom)
-    jp.close()
-    del jp
-    PH.poisson_noise_(proj, I0, seed=7 + rank)
-    torch.cuda.synchronize()
+    scan, grid, views, proj = make_workload(rank, local)
 
     plan = FdkPlan(views, N_DET, N_DET, scan.scan_range, grid, RampFilter(), "fp32", device=local)
     vol = torch.empty(grid.shape, dtype=torch.float32, device=f"cuda:{local}")

@@ -204,10 +204,14 @@ inline void project_point(const Derived& g, const d3& P, double& u, double& v,
     v = (-DU * g.UV + DV * g.UU) * g.inv_gram;
 }
 
-// Emulation of the documented texture linear filter: the fraction of the
-// texel coordinate is held with 8 fractional bits (CUDA C Programming Guide,
-// "Texture Fetching", linear filtering).  Round-to-nearest is assumed.
-inline double tex_frac(double f) { return std::nearbyint(f * 256.0) / 256.0; }
+// Emulation of the texture unit's linear filter, which the reference's FDK
+// backprojection (tex2D) and Joseph projector (tex3D) read through: the
+// fraction of the texel coordinate is held with 8 fractional bits (CUDA C
+// Programming Guide, "Texture Fetching", linear filtering).  The rounding is
+// to nearest with ties upward, alpha = floor(256 f + 0.5) / 256: measured on a
+// B200 by fetching a ramp texture at 327680 coordinates, in 2D and 3D, which
+// this rule reproduces exactly.
+inline double tex_frac(double f) { return std::floor(f * 256.0 + 0.5) / 256.0; }
 
 template <typename T>
 inline double bilerp_zero(const T* img, int w, int h, double x, double y,

@@ -1,0 +1,141 @@
+"""ctypes wrapper of oracle/_ref/libykref.so, the reference YKCBCT CUDA build
+(oracle/ref_build.py, oracle/ref_driver.cu).  TEST INFRASTRUCTURE ONLY.
+
+The reference aborts its process on a CUDA error, so every call runs in a
+child process started with ``spawn``.  Inputs and outputs are numpy float32
+arrays: projections [view][v][u], volumes [z][y][x].
+"""
+from __future__ import annotations
+
+import ctypes as C
+import multiprocessing as mp
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_ref", "libykref.so")
+
+
+def available() -> bool:
+    return os.path.exists(LIB)
+
+
+def _load():
+    lib = C.CDLL(LIB)
+    lib.ykref_last_error.restype = C.c_char_p
+    for name in ("ykref_fdk", "ykref_fdk_stages", "ykref_fdk_time", "ykref_joseph_fp",
+                 "ykref_joseph_bp"):
+        getattr(lib, name).restype = C.c_int
+    return lib
+
+
+def _fp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def _child(op, scan_kw, grid_kw, filt_kw, paths, opts, q):
+    try:
+        from fdk_cuda_impl_b200.geometry import CircularScan, RampFilter, VolumeGrid
+        arrays = [np.load(p, mmap_mode="r") for p in paths]
+        scan = CircularScan(**scan_kw)
+        grid = VolumeGrid(**grid_kw)
+        lib = _load()
+        s = scan.spec()
+        v = grid.struct()
+        dev = C.c_int(opts.get("device", 0))
+        nproj = (scan.total_views, scan.rows, scan.channels)
+        if op == "fdk":
+            f = RampFilter(**filt_kw).struct()
+            proj = np.ascontiguousarray(arrays[0], dtype=np.float32)
+            out = np.zeros(grid.shape, dtype=np.float32)
+            rc = lib.ykref_fdk(C.byref(s), C.byref(v), C.byref(f), _fp(proj), _fp(out),
+                               C.c_int(opts.get("batch_views", 0)), dev)
+            res = out
+        elif op == "fdk_stages":
+            f = RampFilter(**filt_kw).struct()
+            proj = np.ascontiguousarray(arrays[0], dtype=np.float32)
+            out = np.zeros(grid.shape, dtype=np.float32)
+            pw = np.zeros((32, scan.rows, scan.channels), dtype=np.float32)
+            fl = np.zeros_like(pw)
+            first, count = C.c_int(0), C.c_int(0)
+            rc = lib.ykref_fdk_stages(C.byref(s), C.byref(v), C.byref(f), _fp(proj), _fp(out),
+                                      _fp(pw), _fp(fl), C.byref(first), C.byref(count), dev)
+            res = (out, pw[:count.value], fl[:count.value], first.value)
+        elif op == "fdk_time":
+            f = RampFilter(**filt_kw).struct()
+            proj = np.ascontiguousarray(arrays[0], dtype=np.float32)
+            ms = (C.c_float * 2)()
+            rc = lib.ykref_fdk_time(C.byref(s), C.byref(v), C.byref(f), _fp(proj),
+                                    C.c_int(opts["warmup"]), C.c_int(opts["reps"]), ms, dev)
+            res = (ms[0], ms[1])
+        else:
+            x = np.ascontiguousarray(arrays[0], dtype=np.float32)
+            out = np.zeros(nproj if op == "fp" else grid.shape, dtype=np.float32)
+            ms = C.c_float(0.0)
+            fn = lib.ykref_joseph_fp if op == "fp" else lib.ykref_joseph_bp
+            rc = fn(C.byref(s), C.byref(v), _fp(x), _fp(out), C.c_int(opts.get("warmup", 0)),
+                    C.c_int(opts.get("reps", 0)), C.byref(ms), dev)
+            res = (out, ms.value)
+        if rc != 0:
+            q.put(("error", lib.ykref_last_error().decode()))
+        else:
+            q.put(("ok", res))
+    except Exception as e:  # reported to the parent
+        q.put(("error", repr(e)))
+
+
+def _run(op, scan, grid, filt, arrays, **opts):
+    import dataclasses
+    import shutil
+    import tempfile
+    # inputs travel to the child as .npy files (they can be GBs)
+    tmp_root = os.path.join(HERE, "_ref", "tmp")
+    os.makedirs(tmp_root, exist_ok=True)
+    tmp = tempfile.mkdtemp(dir=tmp_root)
+    try:
+        paths = []
+        for i, a in enumerate(arrays):
+            paths.append(os.path.join(tmp, f"in{i}.npy"))
+            np.save(paths[-1], np.ascontiguousarray(a, dtype=np.float32))
+        ctx = mp.get_context("spawn")
+        q = ctx.Queue()
+        filt_kw = dataclasses.asdict(filt) if filt is not None else None
+        p = ctx.Process(target=_child, args=(op, dataclasses.asdict(scan), dataclasses.asdict(grid),
+                                             filt_kw, paths, opts, q))
+        p.start()
+        try:
+            status, res = q.get(timeout=opts.get("timeout", 900))
+        finally:
+            p.join(timeout=60)
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    if status != "ok":
+        raise RuntimeError(f"reference {op} failed: {res} (exit code {p.exitcode})")
+    return res
+
+
+def fdk(scan, grid, filt, proj, batch_views=0):
+    """Reference FdkPipeline FDK of host projections -> volume."""
+    return _run("fdk", scan, grid, filt, [proj], batch_views=batch_views)
+
+
+def fdk_stages(scan, grid, filt, proj):
+    """Reference FDK plus its last chunk's stage buffers:
+    (volume, preweighted rows, filtered rows, first view of that chunk)."""
+    return _run("fdk_stages", scan, grid, filt, [proj])
+
+
+def fdk_time(scan, grid, filt, proj, warmup=2, reps=5, timeout=900):
+    """(device-resident ms, host-input ms) per full FDK sequence."""
+    return _run("fdk_time", scan, grid, filt, [proj], warmup=warmup, reps=reps, timeout=timeout)
+
+
+def joseph_fp(scan, grid, volume, warmup=0, reps=0):
+    """Reference FP_Joseph: (projections, ms per call when reps > 0)."""
+    return _run("fp", scan, grid, None, [volume], warmup=warmup, reps=reps)
+
+
+def joseph_bp(scan, grid, proj, warmup=0, reps=0):
+    """Reference BP_Joseph (clear volume): (volume, ms per call when reps > 0)."""
+    return _run("bp", scan, grid, None, [proj], warmup=warmup, reps=reps)
