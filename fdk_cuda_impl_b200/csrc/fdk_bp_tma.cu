@@ -11,6 +11,12 @@
 //     multicast) into a ring of shared-memory stages guarded by full/empty
 //     mbarriers.  Out-of-detector box elements are zero-filled by TMA, which
 //     is the reference's Border addressing;
+//   * filtered rows arrive either as plain floats or as tap pairs, element
+//     (v, kPairLead + u) = (f[v][u], f[v][u+1]), zero outside the detector
+//     (written so by the filter epilogues).  With pairs one 8-byte shared
+//     load returns both
+//     horizontal taps of a detector row, and the vertical lerp runs as one
+//     packed f32x2 operation on the (left, right) pair;
 //   * consumers read the four taps from shared memory without bounds checks:
 //     the box is sized by a pre-pass over all (tile, view) pairs with the same
 //     footprint function, and each (column, view) checks its end points.
@@ -40,9 +46,9 @@ constexpr int kErrAlign = 4;
 
 // a TMA tile copy writes shared memory at 128-byte aligned addresses: each
 // stage starts on a 128-byte boundary
-__host__ __device__ constexpr int stage_stride_floats(int bw, int bh)
+__host__ __device__ constexpr int stage_stride_floats(int bw, int bh, bool pair)
 {
-    return (bw * bh + 31) / 32 * 32;
+    return (bw * bh * (pair ? 2 : 1) + 31) / 32 * 32;
 }
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p)
@@ -143,6 +149,14 @@ __device__ __forceinline__ float lds(uint32_t addr)
 {
     float v;
     asm("ld.shared.f32 %0, [%1+%2];" : "=f"(v) : "r"(addr), "n"(OFF));
+    return v;
+}
+// one tap pair (8-byte aligned)
+template <int OFF>
+__device__ __forceinline__ f2 lds2(uint32_t addr)
+{
+    f2 v;
+    asm("ld.shared.b64 %0, [%1+%2];" : "=l"(v) : "r"(addr), "n"(OFF));
     return v;
 }
 
@@ -250,8 +264,11 @@ __global__ void box_extent_kernel(const FdkViewCoef* __restrict__ coef, int n_vi
     atomicMax(out + 1, h);
 }
 
-template <int BW, bool AXIAL>
-__global__ void __launch_bounds__(NTHREADS, 3) fdk_bp_tma_kernel(const __grid_constant__ CUtensorMap map,
+// Shared-memory ring budget of one CTA; two CTAs share an SM.
+constexpr size_t kRingBudget = 108 * 1024;
+
+template <int BW, bool AXIAL, bool PAIR>
+__global__ void __launch_bounds__(NTHREADS, 2) fdk_bp_tma_kernel(const __grid_constant__ CUtensorMap map,
     const FdkViewCoef* __restrict__ coef, int n_views, VolumeGrid g, int BH, int stages,
     float* __restrict__ vol, int accumulate, int* __restrict__ err)
 {
@@ -259,8 +276,8 @@ __global__ void __launch_bounds__(NTHREADS, 3) fdk_bp_tma_kernel(const __grid_co
     // 128-byte aligned base (the launch requests 128 bytes of slack)
     unsigned char* smem = reinterpret_cast<unsigned char*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~static_cast<uintptr_t>(127));
-    const int stage_floats = stage_stride_floats(BW, BH);
-    const uint32_t box_bytes = static_cast<uint32_t>(BW * BH * sizeof(float));
+    const int stage_floats = stage_stride_floats(BW, BH, PAIR);
+    const uint32_t box_bytes = static_cast<uint32_t>(BW * BH * (PAIR ? 8 : 4));
     const size_t ring_bytes = static_cast<size_t>(stage_floats) * sizeof(float) * stages;
     float* ring = reinterpret_cast<float*>(smem);
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + ring_bytes);
@@ -292,9 +309,8 @@ __global__ void __launch_bounds__(NTHREADS, 3) fdk_bp_tma_kernel(const __grid_co
         // lanes 0..7 project one tile corner each; lane 0 owns the barriers
         int issued = 0;
         bool ok = true;
-        for (int k = 0; k < n_views; ++k) {
-            const int s = k % stages;
-            const int use = k / stages;
+        int s = 0, use = 0;  // stage of view k and how often it was used before
+        for (int k = 0; k < n_views; ++k, (++s == stages ? (s = 0, ++use) : 0)) {
             int go = 1;
             if (lane == 0) {
                 if (use > 0 && !mbar_wait(&empty[s], (use - 1) & 1)) go = 0;
@@ -324,7 +340,7 @@ __global__ void __launch_bounds__(NTHREADS, 3) fdk_bp_tma_kernel(const __grid_co
                 } else {
                     boxes[s] = make_int4(b.c0, b.r0, b.c1, b.r1);
                     mbar_arrive_expect_tx(&full[s], box_bytes);
-                    tma_load_3d(dst, &map, &full[s], b.c0, b.r0, k);
+                    tma_load_3d(dst, &map, &full[s], b.c0 + (PAIR ? kPairLead : 0), b.r0, k);
                 }
             }
             aligned = __shfl_sync(0xffffffffu, aligned, 0);
@@ -346,7 +362,12 @@ __global__ void __launch_bounds__(NTHREADS, 3) fdk_bp_tma_kernel(const __grid_co
     }
 
     // --------------------------------------------------------- consumers ---
-    const int lx = tid % TX, ly = tid / TX;
+    // a warp covers an 8x4 block of columns, each half-warp a 4x4 block: the
+    // detector footprint of 16 lanes then spans few columns, so the 16-lane
+    // phases of 8-byte shared loads (and 32-lane 4-byte ones) rarely share
+    // a bank
+    const int lx = 8 * (warp & 1) + 4 * (lane >> 4) + (lane & 3);
+    const int ly = 4 * (warp >> 1) + ((lane >> 2) & 3);
     const int x = blockIdx.x * TX + lx, y = blockIdx.y * TY + ly;
     const int z0 = blockIdx.z * ZT;
     const bool active = x < g.nx && y < g.ny;
@@ -354,16 +375,14 @@ __global__ void __launch_bounds__(NTHREADS, 3) fdk_bp_tma_kernel(const __grid_co
     float acc[ZT];
 #pragma unroll
     for (int i = 0; i < ZT; ++i) acc[i] = 0.f;
-    f2 acc2[ZT / 2];
-#pragma unroll
-    for (int j = 0; j < ZT / 2; ++j) acc2[j] = 0ull;
     bool bad = false;
     ColTerms cur{};
     if (AXIAL) cur = axial_terms(coef[0], X, Y, Z0, g.vz);
 
-    for (int k = 0; k < n_views; ++k) {
-        const int s = k % stages;
-        if (!mbar_wait(&full[s], (k / stages) & 1)) {
+    int s = 0;
+    uint32_t phase = 0;
+    for (int k = 0; k < n_views; ++k, (++s == stages ? (s = 0, phase ^= 1u) : 0)) {
+        if (!mbar_wait(&full[s], phase)) {
             atomicOr(err, kErrTimeout);
             *(volatile int*)&abort_flag = 1;
             return;
@@ -397,27 +416,56 @@ __global__ void __launch_bounds__(NTHREADS, 3) fdk_bp_tma_kernel(const __grid_co
             }
             // smem byte address of tap (row n, col) = n*4BW + base, n taken
             // from the rounding word (wrapping 32-bit arithmetic)
-            const uint32_t base = smem_addr(S) + 4u * static_cast<uint32_t>(col) -
-                4u * BW * (static_cast<uint32_t>(b.y) + kRoundMagicBits);
-            const f2 vs2 = f2pack(vs, vs), vb2 = f2pack(vbq, vbq);
-            const f2 au2 = f2pack(au, au), w2 = f2pack(w, w);
+            constexpr uint32_t ES = PAIR ? 8u : 4u;  // bytes per staged element
+            const uint32_t base = smem_addr(S) + ES * static_cast<uint32_t>(col) -
+                ES * BW * (static_cast<uint32_t>(b.y) + kRoundMagicBits);
+            // the column's horizontal weights, with the view weight folded in
+            const float w1 = w * au, w0 = w - w1;
             const f2 M2 = f2pack(kRoundMagic, kRoundMagic), H2 = f2pack(0.5f, 0.5f);
+            if constexpr (PAIR) {
+#pragma unroll
+                for (int j = 0; j < ZT / 2; ++j) {
+                    const f2 vq = f2pack(fmaf(2.f * j, vs, vbq), fmaf(2.f * j + 1.f, vs, vbq));
+                    const f2 t = f2add(vq, M2);
+                    const f2 fr = f2add(f2sub(vq, f2sub(t, M2)), H2);
+                    float t0, t1, f0, f1;
+                    f2unpack(t, t0, t1);
+                    f2unpack(fr, f0, f1);
+                    const uint32_t a0 = __float_as_uint(t0) * (8u * BW) + base;
+                    const uint32_t a1 = __float_as_uint(t1) * (8u * BW) + base;
+                    // rows n and n+1, each (left, right): lerp down as a pair,
+                    // then weight across into the voxel's sum
+                    const f2 A0 = lds2<0>(a0), B0 = lds2<8 * BW>(a0);
+                    const f2 A1 = lds2<0>(a1), B1 = lds2<8 * BW>(a1);
+                    float l0, r0, l1, r1;
+                    f2unpack(f2fma(f2pack(f0, f0), f2sub(B0, A0), A0), l0, r0);
+                    f2unpack(f2fma(f2pack(f1, f1), f2sub(B1, A1), A1), l1, r1);
+                    acc[2 * j] = fmaf(w1, r0, fmaf(w0, l0, acc[2 * j]));
+                    acc[2 * j + 1] = fmaf(w1, r1, fmaf(w0, l1, acc[2 * j + 1]));
+                }
+            } else {
 #pragma unroll
             for (int j = 0; j < ZT / 2; ++j) {
-                const f2 vq = f2fma(f2pack(2.f * j, 2.f * j + 1.f), vs2, vb2);
+                // rows and vertical weights of z = 2j, 2j+1 in packed pairs;
+                // the taps themselves stay scalar so that no load result has
+                // to be moved into a register pair
+                const f2 vq = f2pack(fmaf(2.f * j, vs, vbq), fmaf(2.f * j + 1.f, vs, vbq));
                 const f2 t = f2add(vq, M2);
-                const f2 fr = f2add(f2sub(vq, f2sub(t, M2)), H2);
-                float t0, t1;
+                const f2 d = f2sub(vq, f2sub(t, M2));  // in [-1/2, 1/2]
+                const f2 fr = f2add(d, H2), gr = f2sub(H2, d);
+                float t0, t1, f0, f1, g0, g1;
                 f2unpack(t, t0, t1);
+                f2unpack(fr, f0, f1);
+                f2unpack(gr, g0, g1);
                 const uint32_t a0 = __float_as_uint(t0) * (4u * BW) + base;
                 const uint32_t a1 = __float_as_uint(t1) * (4u * BW) + base;
-                const f2 p00 = f2pack(lds<0>(a0), lds<0>(a1));
-                const f2 p10 = f2pack(lds<4>(a0), lds<4>(a1));
-                const f2 p01 = f2pack(lds<4 * BW>(a0), lds<4 * BW>(a1));
-                const f2 p11 = f2pack(lds<4 * BW + 4>(a0), lds<4 * BW + 4>(a1));
-                const f2 r0 = f2fma(au2, f2sub(p10, p00), p00);
-                const f2 r1 = f2fma(au2, f2sub(p11, p01), p01);
-                acc2[j] = f2fma(w2, f2fma(fr, f2sub(r1, r0), r0), acc2[j]);
+                const float h00 = fmaf(w1, lds<4>(a0), w0 * lds<0>(a0));
+                const float h01 = fmaf(w1, lds<4 * BW + 4>(a0), w0 * lds<4 * BW>(a0));
+                const float h10 = fmaf(w1, lds<4>(a1), w0 * lds<0>(a1));
+                const float h11 = fmaf(w1, lds<4 * BW + 4>(a1), w0 * lds<4 * BW>(a1));
+                acc[2 * j] = fmaf(f0, h01, fmaf(g0, h00, acc[2 * j]));
+                acc[2 * j + 1] = fmaf(f1, h11, fmaf(g1, h10, acc[2 * j + 1]));
+            }
             }
             cur = nxt;
         } else {
@@ -463,7 +511,14 @@ __global__ void __launch_bounds__(NTHREADS, 3) fdk_bp_tma_kernel(const __grid_co
                 const float fu = floorf(u), fv = floorf(v);
                 const int a = static_cast<int>(fv) * BW + static_cast<int>(fu) + cb;
                 const float au = u - fu, av = v - fv;
-                const float p00 = S[a], p10 = S[a + 1], p01 = S[a + BW], p11 = S[a + BW + 1];
+                float p00, p10, p01, p11;
+                if constexpr (PAIR) {
+                    const float2* S2 = reinterpret_cast<const float2*>(S);
+                    const float2 A = S2[a], B = S2[a + BW];
+                    p00 = A.x; p10 = A.y; p01 = B.x; p11 = B.y;
+                } else {
+                    p00 = S[a]; p10 = S[a + 1]; p01 = S[a + BW]; p11 = S[a + BW + 1];
+                }
                 const float r0 = fmaf(au, p10 - p00, p00);
                 const float r1 = fmaf(au, p11 - p01, p01);
                 acc[i] = fmaf(w, fmaf(av, r1 - r0, r0), acc[i]);
@@ -474,10 +529,6 @@ __global__ void __launch_bounds__(NTHREADS, 3) fdk_bp_tma_kernel(const __grid_co
     }
     if (bad) atomicOr(err, kErrFootprint);
     if (!active) return;
-    if (AXIAL) {
-#pragma unroll
-        for (int j = 0; j < ZT / 2; ++j) f2unpack(acc2[j], acc[2 * j], acc[2 * j + 1]);
-    }
     const long plane = static_cast<long>(g.nx) * g.ny;
     float* dst = vol + static_cast<long>(y) * g.nx + x;
 #pragma unroll
@@ -506,26 +557,43 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
 
 constexpr int kWidths[] = {36, 52, 68, 100, 132, 196, 256};
 
-template <int BW>
+template <int BW, bool PAIR>
 cudaError_t launch_bw(const CUtensorMap& map, const FdkViewCoef* coef, int n_views,
     const VolumeGrid& g, int BH, int stages, size_t smem, bool axial, float* vol, int accumulate,
     int* err, cudaStream_t s)
 {
     const dim3 grid((g.nx + TX - 1) / TX, (g.ny + TY - 1) / TY, (g.nz + ZT - 1) / ZT);
     if (axial) {
-        auto k = fdk_bp_tma_kernel<BW, true>;
+        auto k = fdk_bp_tma_kernel<BW, true, PAIR>;
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
             static_cast<int>(smem));
         if (e != cudaSuccess) return e;
         k<<<grid, NTHREADS, smem, s>>>(map, coef, n_views, g, BH, stages, vol, accumulate, err);
     } else {
-        auto k = fdk_bp_tma_kernel<BW, false>;
+        auto k = fdk_bp_tma_kernel<BW, false, PAIR>;
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
             static_cast<int>(smem));
         if (e != cudaSuccess) return e;
         k<<<grid, NTHREADS, smem, s>>>(map, coef, n_views, g, BH, stages, vol, accumulate, err);
     }
     return cudaGetLastError();
+}
+
+template <bool PAIR>
+cudaError_t launch_layout(const CUtensorMap& map, const FdkViewCoef* coef, int n_views,
+    const VolumeGrid& g, int bw, int bh, int stages, size_t smem, bool axial, float* vol,
+    int accumulate, int* err, cudaStream_t s)
+{
+    switch (bw) {
+    case 36: return launch_bw<36, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, s);
+    case 52: return launch_bw<52, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, s);
+    case 68: return launch_bw<68, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, s);
+    case 100: return launch_bw<100, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, s);
+    case 132: return launch_bw<132, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, s);
+    case 196: return launch_bw<196, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, s);
+    case 256: return launch_bw<256, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, s);
+    default: return cudaErrorInvalidValue;
+    }
 }
 
 } // namespace
@@ -552,49 +620,75 @@ cudaError_t fdk_tma_box(const FdkViewCoef* coef, int n_views, const VolumeGrid& 
     return cudaSuccess;
 }
 
-// Stages that fit the shared-memory budget for a box (0 when none).
-int fdk_tma_stages(int bw, int bh)
+// Stages that fit the shared-memory budget for a box (0 when fewer than 2).
+int fdk_tma_stages(int bw, int bh, int layout)
 {
-    const size_t stage = static_cast<size_t>(stage_stride_floats(bw, bh)) * sizeof(float);
-    const size_t budget = 72 * 1024;  // three CTAs per SM
-    int s = static_cast<int>(budget / std::max<size_t>(stage, 1));
+    const size_t stage = static_cast<size_t>(
+        stage_stride_floats(bw, bh, layout == kFilteredPairs)) * sizeof(float);
+    int s = static_cast<int>(kRingBudget / std::max<size_t>(stage, 1));
     s = std::min(s, 8);
     return s >= 2 ? s : 0;
 }
 
 bool fdk_tma_available() { return encode_fn() != nullptr; }
 
-cudaError_t launch_fdk_backproject_tma(const float* filtered, int ld, int rows_total_views,
-    const FdkViewCoef* coef, int n_views, int nu, int nv, const VolumeGrid& g, bool axial,
-    int bw, int bh, float* vol, int accumulate, int* err, cudaStream_t s)
+cudaError_t launch_fdk_backproject_tma(const float* filtered, int layout, int ld,
+    int rows_total_views, const FdkViewCoef* coef, int n_views, int nu, int nv,
+    const VolumeGrid& g, bool axial, int bw, int bh, float* vol, int accumulate, int* err,
+    cudaStream_t s)
 {
     auto enc = encode_fn();
     if (!enc) return cudaErrorNotSupported;
+    const bool pair = layout == kFilteredPairs;
+    const size_t esz = pair ? 8 : 4;  // a tap pair moves as one 8-byte element
     CUtensorMap map;
-    const cuuint64_t dims[3] = {static_cast<cuuint64_t>(nu), static_cast<cuuint64_t>(nv),
+    const cuuint64_t dims[3] = {static_cast<cuuint64_t>(pair ? nu + kPairLead : nu),
+                                static_cast<cuuint64_t>(nv),
                                 static_cast<cuuint64_t>(rows_total_views)};
-    const cuuint64_t strides[2] = {static_cast<cuuint64_t>(ld) * sizeof(float),
-                                   static_cast<cuuint64_t>(ld) * nv * sizeof(float)};
+    const cuuint64_t strides[2] = {static_cast<cuuint64_t>(ld) * esz,
+                                   static_cast<cuuint64_t>(ld) * nv * esz};
     const cuuint32_t box[3] = {static_cast<cuuint32_t>(bw), static_cast<cuuint32_t>(bh), 1};
     const cuuint32_t estr[3] = {1, 1, 1};
-    const CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(filtered),
-        dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-        CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    const CUresult r = enc(&map,
+        pair ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
+        const_cast<float*>(filtered), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+        CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
-    const int stages = fdk_tma_stages(bw, bh);
+    const int stages = fdk_tma_stages(bw, bh, layout);
     if (stages == 0) return cudaErrorInvalidConfiguration;
-    const size_t ring = static_cast<size_t>(stage_stride_floats(bw, bh)) * sizeof(float) * stages;
+    const size_t ring = static_cast<size_t>(stage_stride_floats(bw, bh, pair)) * sizeof(float) * stages;
     const size_t smem = 128 + ring + 2 * stages * sizeof(uint64_t) + stages * sizeof(int4) + 16;
-    switch (bw) {
-    case 36: return launch_bw<36>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, s);
-    case 52: return launch_bw<52>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, s);
-    case 68: return launch_bw<68>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, s);
-    case 100: return launch_bw<100>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, s);
-    case 132: return launch_bw<132>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, s);
-    case 196: return launch_bw<196>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, s);
-    case 256: return launch_bw<256>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, s);
-    default: return cudaErrorInvalidValue;
+    return pair ? launch_layout<true>(map, coef, n_views, g, bw, bh, stages, smem, axial, vol,
+                      accumulate, err, s)
+                : launch_layout<false>(map, coef, n_views, g, bw, bh, stages, smem, axial, vol,
+                      accumulate, err, s);
+}
+
+// Scalar filtered rows [rows][ld_in] -> tap pairs [rows][ldp]: element
+// kPairLead + u = (f[u], f[u+1]) for u in [-kPairLead, nu), zero outside the
+// row -- the layout the filter epilogues write directly.
+__global__ void pairify_kernel(const float* __restrict__ in, int ld_in, long rows, int nu,
+    float2* __restrict__ out, int ldp)
+{
+    const int width = nu + kPairLead;
+    const long n = rows * width;
+    for (long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long>(gridDim.x) * blockDim.x) {
+        const long r = i / width;
+        const int u = static_cast<int>(i - r * width) - kPairLead;
+        const float* row = in + r * ld_in;
+        out[r * ldp + u + kPairLead] = make_float2(u >= 0 ? row[u] : 0.f,
+            u + 1 >= 0 && u + 1 < nu ? row[u + 1] : 0.f);
     }
+}
+
+cudaError_t launch_fdk_pairify(const float* in, int ld_in, long rows, int nu, float* out,
+    int ldp, cudaStream_t s)
+{
+    if (rows <= 0) return cudaSuccess;
+    pairify_kernel<<<148 * 8, 256, 0, s>>>(in, ld_in, rows, nu, reinterpret_cast<float2*>(out), ldp);
+    return cudaGetLastError();
 }
 
 } // namespace ykb

@@ -107,7 +107,7 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar)
                  ::"r"(smem_u32(bar)) : "memory");
 }
 
-template <int TN>
+template <int TN, bool PAIR>
 __global__ void __launch_bounds__(128, 1) ramp_tc_kernel(
     const __grid_constant__ CUtensorMap map_a_hi, const __grid_constant__ CUtensorMap map_a_lo,
     const __grid_constant__ CUtensorMap map_t_hi, const __grid_constant__ CUtensorMap map_t_lo,
@@ -220,11 +220,22 @@ __global__ void __launch_bounds__(128, 1) ramp_tc_kernel(
                      : "r"(taddr));
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
         if (row_ok) {
-            float* dst = C + m * ldc;
+            float* dst = C + m * (PAIR ? 2 : 1) * ldc + (PAIR ? 2 * kPairLead : 0);
 #pragma unroll
             for (int i = 0; i < 16; ++i) {
                 const int j = n0 + c + i;
-                if (j < nu) dst[j] = (j >= out_lo && j < out_hi) ? __uint_as_float(r[i]) : 0.f;
+                if (j >= nu) continue;
+                const float v = (j >= out_lo && j < out_hi) ? __uint_as_float(r[i]) : 0.f;
+                if constexpr (!PAIR) {
+                    dst[j] = v;
+                } else {
+                    // tap pairs: left of pair j, right of pair j-1; the pairs
+                    // around the row are zero where they reach outside it
+                    dst[2 * j] = v;
+                    dst[2 * j - 1] = v;
+                    if (j == 0) dst[-2] = dst[-3] = dst[-4] = 0.f;
+                    if (j == nu - 1) dst[2 * j + 1] = 0.f;
+                }
             }
         }
     }
@@ -296,13 +307,13 @@ bool make_map(CUtensorMap* map, const void* base, long inner, long outer, long l
                CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-template <int TN>
+template <int TN, bool PAIR>
 cudaError_t launch_tn(const CUtensorMap& ah, const CUtensorMap& al, const CUtensorMap& th,
     const CUtensorMap& tl, long rows, int nu, int nv, int kchunks, const FdkPreweightView* pwv,
     float* C, int ldc, int* err, cudaStream_t s)
 {
     const size_t smem = 1024 + STAGES * (kAStageBytes + TN * TK * 2) + (2 * STAGES + 1) * 8 + 16;
-    auto k = ramp_tc_kernel<TN>;
+    auto k = ramp_tc_kernel<TN, PAIR>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
         static_cast<int>(smem));
     if (e != cudaSuccess) return e;
@@ -342,7 +353,7 @@ cudaError_t launch_fdk_preweight_split_bf16(const void* proj, int proj_dtype,
 
 cudaError_t launch_fdk_ramp_tcgen05(const __nv_bfloat16* a_hi, const __nv_bfloat16* a_lo,
     const __nv_bfloat16* t_hi, const __nv_bfloat16* t_lo, int rows, int nu, int ld,
-    const FdkPreweightView* pwv, int nv, float* out, int ldc, int* err, cudaStream_t s)
+    const FdkPreweightView* pwv, int nv, float* out, int layout, int ldc, int* err, cudaStream_t s)
 {
     if (rows <= 0) return cudaSuccess;
     const int tn = tc_filter_tile_n(nu);
@@ -352,11 +363,16 @@ cudaError_t launch_fdk_ramp_tcgen05(const __nv_bfloat16* a_hi, const __nv_bfloat
         !make_map(&th, t_hi, nu, nu, ld, TK, tn) || !make_map(&tl, t_lo, nu, nu, ld, TK, tn))
         return cudaErrorInvalidValue;
     const int kchunks = (nu + TK - 1) / TK;
+    const bool pair = layout == kFilteredPairs;
     switch (tn) {
-    case 256: return launch_tn<256>(ah, al, th, tl, rows, nu, nv, kchunks, pwv, out, ldc, err, s);
-    case 192: return launch_tn<192>(ah, al, th, tl, rows, nu, nv, kchunks, pwv, out, ldc, err, s);
-    case 128: return launch_tn<128>(ah, al, th, tl, rows, nu, nv, kchunks, pwv, out, ldc, err, s);
-    default: return launch_tn<64>(ah, al, th, tl, rows, nu, nv, kchunks, pwv, out, ldc, err, s);
+    case 256: return pair ? launch_tn<256, true>(ah, al, th, tl, rows, nu, nv, kchunks, pwv, out, ldc, err, s)
+                          : launch_tn<256, false>(ah, al, th, tl, rows, nu, nv, kchunks, pwv, out, ldc, err, s);
+    case 192: return pair ? launch_tn<192, true>(ah, al, th, tl, rows, nu, nv, kchunks, pwv, out, ldc, err, s)
+                          : launch_tn<192, false>(ah, al, th, tl, rows, nu, nv, kchunks, pwv, out, ldc, err, s);
+    case 128: return pair ? launch_tn<128, true>(ah, al, th, tl, rows, nu, nv, kchunks, pwv, out, ldc, err, s)
+                          : launch_tn<128, false>(ah, al, th, tl, rows, nu, nv, kchunks, pwv, out, ldc, err, s);
+    default: return pair ? launch_tn<64, true>(ah, al, th, tl, rows, nu, nv, kchunks, pwv, out, ldc, err, s)
+                         : launch_tn<64, false>(ah, al, th, tl, rows, nu, nv, kchunks, pwv, out, ldc, err, s);
     }
 }
 

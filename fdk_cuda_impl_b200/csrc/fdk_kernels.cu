@@ -52,10 +52,10 @@ __global__ void __launch_bounds__(128) preweight_kernel(const TIn* __restrict__ 
 // for a k-tile in registers.
 constexpr int RBM = 64, RBN = 128, RBK = 32;
 
-template <typename TOut>
+template <bool PAIR>
 __global__ void __launch_bounds__(256) ramp_fp32_kernel(const float* __restrict__ A,
     const float* __restrict__ h, const FdkPreweightView* __restrict__ pwv, long rows,
-    int nu, int nv, TOut* __restrict__ C, int ldc)
+    int nu, int nv, float* __restrict__ C, int ldc)
 {
     __shared__ __align__(16) float As[RBK][RBM + 4];
     __shared__ float hs[RBN + RBK];
@@ -114,8 +114,17 @@ __global__ void __launch_bounds__(256) ramp_fp32_kernel(const float* __restrict_
             const int j = j0 + tx * 8 + q;
             if (j >= nu) continue;
             const float v = (j >= p.out_lo && j < p.out_hi) ? acc[i][q] : 0.f;
-            if constexpr (sizeof(TOut) == 4) C[m * ldc + j] = v;
-            else C[m * ldc + j] = __float2bfloat16_rn(v);
+            if constexpr (!PAIR) {
+                C[m * ldc + j] = v;
+            } else {
+                // tap pairs: left of pair j, right of pair j-1; the pairs
+                // around the row are zero where they reach outside it
+                float* row = C + m * 2 * ldc + 2 * kPairLead;
+                row[2 * j] = v;
+                row[2 * j - 1] = v;
+                if (j == 0) row[-2] = row[-3] = row[-4] = 0.f;
+                if (j == nu - 1) row[2 * j + 1] = 0.f;
+            }
         }
     }
 }
@@ -251,18 +260,16 @@ cudaError_t launch_fdk_preweight(const void* proj, int proj_dtype,
 }
 
 cudaError_t launch_fdk_ramp_fp32(const float* pw_rows, const float* h_dev,
-    const FdkPreweightView* pwv, int n_views, int nu, int nv, void* out, int out_dtype,
+    const FdkPreweightView* pwv, int n_views, int nu, int nv, float* out, int layout,
     int ldc, cudaStream_t s)
 {
     const long rows = static_cast<long>(n_views) * nv;
     if (rows <= 0) return cudaSuccess;
     const dim3 grid((nu + RBN - 1) / RBN, static_cast<unsigned>((rows + RBM - 1) / RBM));
-    if (out_dtype == YKB_DTYPE_BF16)
-        ramp_fp32_kernel<__nv_bfloat16><<<grid, 256, 0, s>>>(pw_rows, h_dev, pwv, rows, nu, nv,
-            static_cast<__nv_bfloat16*>(out), ldc);
+    if (layout == kFilteredPairs)
+        ramp_fp32_kernel<true><<<grid, 256, 0, s>>>(pw_rows, h_dev, pwv, rows, nu, nv, out, ldc);
     else
-        ramp_fp32_kernel<float><<<grid, 256, 0, s>>>(pw_rows, h_dev, pwv, rows, nu, nv,
-            static_cast<float*>(out), ldc);
+        ramp_fp32_kernel<false><<<grid, 256, 0, s>>>(pw_rows, h_dev, pwv, rows, nu, nv, out, ldc);
     return cudaGetLastError();
 }
 

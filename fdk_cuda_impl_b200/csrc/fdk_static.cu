@@ -108,7 +108,7 @@ extern "C" YKB_API ykb_status ykb_fdk_filter_static(const ykb_cone_view* views, 
             static_cast<size_t>(c) * nu * nv * in_elem;
         YKB_TRY_CUDA(launch_fdk_preweight(in, proj_dtype, d_records + c, cnt, nu, nv, d_rows, s));
         YKB_TRY_CUDA(launch_fdk_ramp_fp32(d_rows, d_lags, d_records + c, cnt, nu, nv,
-            d_filtered + static_cast<size_t>(c) * nu * nv, YKB_DTYPE_F32, nu, s));
+            d_filtered + static_cast<size_t>(c) * nu * nv, kFilteredScalar, nu, s));
     }
     // the host-side tables were copied from pageable memory: the copies have
     // left the host buffers when cudaMemcpyAsync returns

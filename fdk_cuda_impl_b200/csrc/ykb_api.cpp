@@ -73,8 +73,9 @@ size_t volume_elems(const ykb_volume& v)
 // about 4 GiB whatever the scan length.
 int chunk_capacity(int n_views, int nu, int nv)
 {
-    const size_t per_view = static_cast<size_t>(nu) * nv * (sizeof(float) * 2);
-    const size_t budget = size_t(4) << 30;
+    // preweighted rows (4 B) + filtered tap pairs (8 B) per detector pixel
+    const size_t per_view = static_cast<size_t>(nu) * nv * 12;
+    const size_t budget = size_t(8) << 30;
     const size_t cap = std::max<size_t>(1, budget / std::max<size_t>(per_view, 1));
     return static_cast<int>(std::min<size_t>(n_views, cap));
 }
@@ -146,20 +147,16 @@ YKB_API ykb_status ykb_fdk_plan_create(const ykb_cone_view* views, int n_views, 
     std::vector<float> hf(h.begin(), h.end());
 
     p->batch_capacity = chunk_capacity(n_views, nu, nv);
-    // filtered rows padded to 16 bytes: the pitch a TMA tensor map needs
-    p->ld = (nu + 7) / 8 * 8;
     p->tc_filter = precision == YKB_PRECISION_BF16 && tcgen05_filter_supported(nu);
     p->lda = p->tc_filter ? tc_filter_lda(nu) : nu;
     // work_a holds the preweighted rows: float, or bf16 hi + bf16 lo
     const size_t chunk_elems = static_cast<size_t>(p->batch_capacity) * p->lda * nv;
-    const size_t filt_bytes = static_cast<size_t>(p->batch_capacity) * p->ld * nv * sizeof(float);
     cudaError_t e;
     if ((e = p->coef.alloc(sizeof(FdkViewCoef) * n_views)) != cudaSuccess ||
         (e = p->pwv.alloc(sizeof(FdkPreweightView) * n_views)) != cudaSuccess ||
         (e = p->ramp.alloc(sizeof(float) * hf.size())) != cudaSuccess ||
         (e = p->err_flag.alloc(4 * sizeof(int))) != cudaSuccess ||
-        (e = p->work_a.alloc(chunk_elems * sizeof(float))) != cudaSuccess ||
-        (e = p->work_filtered.alloc(filt_bytes)) != cudaSuccess) {
+        (e = p->work_a.alloc(chunk_elems * sizeof(float))) != cudaSuccess) {
         delete p;
         return cuda_status(e, "cudaMalloc (FDK plan workspace)");
     }
@@ -208,7 +205,23 @@ YKB_API ykb_status ykb_fdk_plan_create(const ykb_cone_view* views, int n_views, 
             delete p;
             return cuda_status(e, "backprojection box pre-pass");
         }
-        p->use_tma = p->tma_bw > 0 && fdk_tma_stages(p->tma_bw, p->tma_bh) > 0;
+        p->use_tma = p->tma_bw > 0 && fdk_tma_stages(p->tma_bw, p->tma_bh, kFilteredScalar) > 0;
+    }
+    // YKB_FDK_BP_PATH=rows|global selects the plain-row TMA or the global-load
+    // backprojection instead of the default (tests compare the three paths)
+    const char* path = std::getenv("YKB_FDK_BP_PATH");
+    const bool force_rows = path && std::strcmp(path, "rows") == 0;
+    if (path && std::strcmp(path, "global") == 0) p->use_tma = false;
+    // filtered workspace: tap pairs when their box fits the shared-memory
+    // ring, else plain rows; both with 16-byte row pitch (TMA)
+    p->layout = p->use_tma && !force_rows &&
+        fdk_tma_stages(p->tma_bw, p->tma_bh, kFilteredPairs) > 0 ? kFilteredPairs : kFilteredScalar;
+    p->ld = p->layout == kFilteredPairs ? (nu + kPairLead + 1) / 2 * 2 : (nu + 7) / 8 * 8;
+    const size_t filt_bytes = static_cast<size_t>(p->batch_capacity) * p->ld * nv *
+        (p->layout == kFilteredPairs ? 8 : 4);
+    if ((e = p->work_filtered.alloc(filt_bytes)) != cudaSuccess) {
+        delete p;
+        return cuda_status(e, "cudaMalloc (FDK filtered workspace)");
     }
     *plan_out = p;
     return YKB_OK;
@@ -247,9 +260,9 @@ ykb_status check_range(const ykb_fdk_plan* p, const void* buf, int dtype, int vi
 size_t dtype_bytes(int dtype) { return dtype == YKB_DTYPE_BF16 ? 2 : 4; }
 
 // preweight + ramp for views [first, first+count) of the plan, input rows at
-// proj, output into dst (plan dtype)
+// proj, output into dst (FilteredLayout `layout`, row pitch ldc elements)
 ykb_status filter_chunk(ykb_fdk_plan* p, const void* proj, int proj_dtype, int first, int count,
-    void* dst, int ldc, cudaStream_t s)
+    float* dst, int layout, int ldc, cudaStream_t s)
 {
     const FdkPreweightView* pwv = p->pwv.as<FdkPreweightView>() + first;
     if (p->tc_filter) {
@@ -260,32 +273,36 @@ ykb_status filter_chunk(ykb_fdk_plan* p, const void* proj, int proj_dtype, int f
             p->lda, a_hi, a_lo, s));
         YKB_TRY_CUDA(launch_fdk_ramp_tcgen05(a_hi, a_lo, p->toeplitz_hi.as<__nv_bfloat16>(),
             p->toeplitz_lo.as<__nv_bfloat16>(), count * p->nv, p->nu, p->lda, pwv, p->nv,
-            static_cast<float*>(dst), ldc, p->err_flag.as<int>(), s));
+            dst, layout, ldc, p->err_flag.as<int>(), s));
         return YKB_OK;
     }
     YKB_TRY_CUDA(launch_fdk_preweight(proj, proj_dtype, pwv, count, p->nu, p->nv,
         p->work_a.as<float>(), s));
     YKB_TRY_CUDA(launch_fdk_ramp_fp32(p->work_a.as<float>(), p->ramp.as<float>(), pwv, count,
-        p->nu, p->nv, dst, YKB_DTYPE_F32, ldc, s));
+        p->nu, p->nv, dst, layout, ldc, s));
     return YKB_OK;
 }
 
-// weighted backprojection of `count` filtered views (row pitch ld) starting
-// at plan view `first`
-ykb_status backproject_chunk(ykb_fdk_plan* p, const void* filtered, int dtype, int ld, int first,
+// weighted backprojection of `count` filtered views (FilteredLayout
+// `layout`, row pitch ld elements) starting at plan view `first`
+ykb_status backproject_chunk(ykb_fdk_plan* p, const void* filtered, int layout, int ld, int first,
     int count, float* vol, int accumulate, cudaStream_t s)
 {
     const VolumeGrid grid = make_grid(p->volume);
     const FdkViewCoef* coef = p->coef.as<FdkViewCoef>() + first;
-    const bool tma_ok = p->use_tma && dtype == YKB_DTYPE_F32 && ld % 4 == 0 &&
-        (reinterpret_cast<uintptr_t>(filtered) & 15) == 0;
-    if (tma_ok)
-        YKB_TRY_CUDA(launch_fdk_backproject_tma(static_cast<const float*>(filtered), ld, count, coef,
-            count, p->nu, p->nv, grid, p->axial, p->tma_bw, p->tma_bh, vol, accumulate,
-            p->err_flag.as<int>(), s));
-    else
-        YKB_TRY_CUDA(launch_fdk_backproject(filtered, dtype, coef, count, p->nu, p->nv, ld, grid,
-            p->axial, vol, accumulate, s));
+    const bool aligned = (reinterpret_cast<uintptr_t>(filtered) & 15) == 0;
+    if (layout == kFilteredPairs) {
+        YKB_TRY_CUDA(launch_fdk_backproject_tma(static_cast<const float*>(filtered), layout, ld,
+            count, coef, count, p->nu, p->nv, grid, p->axial, p->tma_bw, p->tma_bh, vol,
+            accumulate, p->err_flag.as<int>(), s));
+    } else if (p->use_tma && ld % 4 == 0 && aligned) {
+        YKB_TRY_CUDA(launch_fdk_backproject_tma(static_cast<const float*>(filtered), layout, ld,
+            count, coef, count, p->nu, p->nv, grid, p->axial, p->tma_bw, p->tma_bh, vol,
+            accumulate, p->err_flag.as<int>(), s));
+    } else {
+        YKB_TRY_CUDA(launch_fdk_backproject(filtered, YKB_DTYPE_F32, coef, count, p->nu, p->nv,
+            ld, grid, p->axial, vol, accumulate, s));
+    }
     return YKB_OK;
 }
 
@@ -304,8 +321,9 @@ YKB_API ykb_status ykb_fdk_filter(ykb_fdk_plan* p, const void* d_proj, int proj_
     for (int c = 0; c < n_views; c += p->batch_capacity) {
         const int cnt = std::min(p->batch_capacity, n_views - c);
         const char* in = static_cast<const char*>(d_proj) + c * view_elems * dtype_bytes(proj_dtype);
-        char* out = static_cast<char*>(d_filtered) + c * view_elems * out_b;
-        if (const ykb_status st = filter_chunk(p, in, proj_dtype, view_offset + c, cnt, out, p->nu, s))
+        float* out = reinterpret_cast<float*>(static_cast<char*>(d_filtered) + c * view_elems * out_b);
+        if (const ykb_status st = filter_chunk(p, in, proj_dtype, view_offset + c, cnt, out,
+                kFilteredScalar, p->nu, s))
             return st;
     }
     return YKB_OK;
@@ -321,8 +339,27 @@ YKB_API ykb_status ykb_fdk_backproject(ykb_fdk_plan* p, const void* d_filtered,
     if (!d_volume) return fail(YKB_ERR_INVALID_BUFFER, "null volume buffer");
     DeviceGuard guard(p->device);
     const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    return backproject_chunk(p, d_filtered, filtered_dtype, p->nu, view_offset, n_views, d_volume,
-        clear_output ? 0 : 1, s);
+    if (filtered_dtype == YKB_DTYPE_BF16) {
+        YKB_TRY_CUDA(launch_fdk_backproject(d_filtered, YKB_DTYPE_BF16,
+            p->coef.as<FdkViewCoef>() + view_offset, n_views, p->nu, p->nv, p->nu,
+            make_grid(p->volume), p->axial, d_volume, clear_output ? 0 : 1, s));
+        return YKB_OK;
+    }
+    if (p->layout != kFilteredPairs)
+        return backproject_chunk(p, d_filtered, kFilteredScalar, p->nu, view_offset, n_views,
+            d_volume, clear_output ? 0 : 1, s);
+    // plain rows from the caller: re-laid as tap pairs in the plan workspace
+    const size_t view_elems = static_cast<size_t>(p->nu) * p->nv;
+    for (int c = 0; c < n_views; c += p->batch_capacity) {
+        const int cnt = std::min(p->batch_capacity, n_views - c);
+        YKB_TRY_CUDA(launch_fdk_pairify(static_cast<const float*>(d_filtered) + c * view_elems,
+            p->nu, static_cast<long>(cnt) * p->nv, p->nu, p->work_filtered.as<float>(), p->ld, s));
+        const int accumulate = (c == 0 && clear_output) ? 0 : 1;
+        if (const ykb_status st = backproject_chunk(p, p->work_filtered.ptr, kFilteredPairs, p->ld,
+                view_offset + c, cnt, d_volume, accumulate, s))
+            return st;
+    }
+    return YKB_OK;
 }
 
 YKB_API ykb_status ykb_fdk_execute(ykb_fdk_plan* p, const void* d_proj, int proj_dtype,
@@ -334,15 +371,14 @@ YKB_API ykb_status ykb_fdk_execute(ykb_fdk_plan* p, const void* d_proj, int proj
     DeviceGuard guard(p->device);
     const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const size_t view_elems = static_cast<size_t>(p->nu) * p->nv;
-    const int filt_dtype = YKB_DTYPE_F32;
     for (int c = 0; c < n_views; c += p->batch_capacity) {
         const int cnt = std::min(p->batch_capacity, n_views - c);
         const char* in = static_cast<const char*>(d_proj) + c * view_elems * dtype_bytes(proj_dtype);
         if (const ykb_status st = filter_chunk(p, in, proj_dtype, view_offset + c, cnt,
-                p->work_filtered.ptr, p->ld, s))
+                p->work_filtered.as<float>(), p->layout, p->ld, s))
             return st;
         const int accumulate = (c == 0 && clear_output) ? 0 : 1;
-        if (const ykb_status st = backproject_chunk(p, p->work_filtered.ptr, filt_dtype, p->ld,
+        if (const ykb_status st = backproject_chunk(p, p->work_filtered.ptr, p->layout, p->ld,
                 view_offset + c, cnt, d_volume, accumulate, s))
             return st;
     }

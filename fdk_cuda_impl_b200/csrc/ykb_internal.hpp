@@ -152,19 +152,27 @@ struct VolumeGrid {
 VolumeGrid make_grid(const ykb_volume& v);
 
 // FDK
+// Layouts of filtered rows: plain floats [row][ld], or tap pairs
+// [row][ld] float2 where element kPairLead + u = (f[u], f[u+1]) for
+// u in [-kPairLead, nu) with f outside [0, nu) = 0.  The TMA
+// backprojection reads a row's two horizontal taps with one 8-byte load;
+// the two leading pairs keep the TMA box origin 16-byte aligned while
+// u = -1 still sees (0, f[0]).
+enum FilteredLayout : int { kFilteredScalar = 0, kFilteredPairs = 1 };
+constexpr int kPairLead = 2;
 cudaError_t launch_fdk_preweight(const void* proj, int proj_dtype,
     const FdkPreweightView* pw, int n_views, int nu, int nv, float* out,
     cudaStream_t s);
 cudaError_t launch_fdk_ramp_fp32(const float* pw_rows, const float* h_dev,
-    const FdkPreweightView* pwv, int n_views, int nu, int nv, void* out,
-    int out_dtype, int ldc, cudaStream_t s);
+    const FdkPreweightView* pwv, int n_views, int nu, int nv, float* out,
+    int layout, int ldc, cudaStream_t s);
 cudaError_t launch_fdk_preweight_split_bf16(const void* proj, int proj_dtype,
     const FdkPreweightView* pw, int n_views, int nu, int nv, int ld,
     __nv_bfloat16* hi, __nv_bfloat16* lo, cudaStream_t s);
 cudaError_t launch_fdk_ramp_tcgen05(const __nv_bfloat16* a_hi,
     const __nv_bfloat16* a_lo, const __nv_bfloat16* t_hi,
     const __nv_bfloat16* t_lo, int rows, int nu, int ld,
-    const FdkPreweightView* pwv, int nv, float* out, int ldc, int* err_flag,
+    const FdkPreweightView* pwv, int nv, float* out, int layout, int ldc, int* err_flag,
     cudaStream_t s);
 bool tcgen05_filter_supported(int nu);
 int tc_filter_lda(int nu);
@@ -174,12 +182,15 @@ cudaError_t launch_fdk_backproject(const void* filtered, int dtype,
     cudaStream_t s);
 // TMA-staged backprojection (fdk_bp_tma.cu)
 bool fdk_tma_available();
-int fdk_tma_stages(int bw, int bh);
+int fdk_tma_stages(int bw, int bh, int layout);
 cudaError_t fdk_tma_box(const FdkViewCoef* coef, int n_views, const VolumeGrid& g,
     int* scratch2, int* bw, int* bh, cudaStream_t s);
-cudaError_t launch_fdk_backproject_tma(const float* filtered, int ld, int views_in_buffer,
-    const FdkViewCoef* coef, int n_views, int nu, int nv, const VolumeGrid& g, bool axial,
-    int bw, int bh, float* vol, int accumulate, int* err, cudaStream_t s);
+cudaError_t launch_fdk_backproject_tma(const float* filtered, int layout, int ld,
+    int views_in_buffer, const FdkViewCoef* coef, int n_views, int nu, int nv,
+    const VolumeGrid& g, bool axial, int bw, int bh, float* vol, int accumulate, int* err,
+    cudaStream_t s);
+cudaError_t launch_fdk_pairify(const float* in, int ld_in, long rows, int nu, float* out,
+    int ldp, cudaStream_t s);
 
 // Joseph
 cudaError_t launch_joseph_transpose(const float* vol, int nx, int ny, int nz,
@@ -208,6 +219,7 @@ struct ykb_fdk_plan {
     bool tc_filter = false;
     int batch_capacity = 0;      // views the workspace holds
     int ld = 0;                  // row pitch (elements) of the filtered workspace
+    int layout = 0;              // FilteredLayout of the filtered workspace
     int lda = 0;                 // row pitch of the bf16 GEMM operands (tensor-core filter)
     bool use_tma = false;        // TMA-staged backprojection
     int tma_bw = 0, tma_bh = 0;  // its projection box
@@ -217,7 +229,7 @@ struct ykb_fdk_plan {
     ykb::DeviceBuffer ramp;      // float[2*nu-1]
     ykb::DeviceBuffer toeplitz_hi, toeplitz_lo;  // bf16 [nu][ld] (BF16 plans)
     ykb::DeviceBuffer work_a;    // preweighted rows: float, or bf16 hi then lo
-    ykb::DeviceBuffer work_filtered;  // filtered projections (plan dtype)
+    ykb::DeviceBuffer work_filtered;  // filtered projections (layout, pitch ld)
     ykb::DeviceBuffer err_flag;  // int[4]: device error word, box pre-pass scratch
 };
 

@@ -172,24 +172,38 @@ def test_fdk_backproject_stage_unaligned_pitch(oracle, cuda_device):
 
 
 def test_fdk_tma_matches_global_path(oracle, cuda_device):
-    # the staged (TMA) and the global-load backprojections give the same
-    # volume: the same weights applied in the same order
+    # the three backprojection paths -- TMA-staged tap pairs (default),
+    # TMA-staged plain rows, global loads -- give the same volume: the same
+    # weights applied in the same order, up to FP32 rounding of the lerps
+    import os
     import torch
     from fdk_cuda_impl_b200.projectors import FdkPlan
     case = K.c1_small()
     views = case.scan.views()
     p = torch.from_numpy(K.projections(oracle, case, views)).cuda()
-    fp32 = FdkPlan(views, 96, 64, case.scan.scan_range, case.grid, case.filt)
-    filtered = fp32.filter(p)
-    staged = fp32.backproject(filtered)  # 16-byte aligned buffer -> TMA path
-    # the same values 4 bytes off a 16-byte boundary: no tensor map possible
-    flat = torch.empty(filtered.numel() + 1, device="cuda")
-    shifted = flat[1:].view(filtered.shape)
-    shifted.copy_(filtered)
-    assert shifted.data_ptr() % 16 != 0
-    direct = fp32.backproject(shifted)
-    fp32.check()
-    assert K.rel_rmse(staged.cpu().numpy(), direct.cpu().numpy()) < 1e-6
+    out = {}
+    for path in ("pairs", "rows", "global"):
+        if path == "pairs":
+            os.environ.pop("YKB_FDK_BP_PATH", None)
+        else:
+            os.environ["YKB_FDK_BP_PATH"] = path
+        try:
+            plan = FdkPlan(views, 96, 64, case.scan.scan_range, case.grid, case.filt)
+        finally:
+            os.environ.pop("YKB_FDK_BP_PATH", None)
+        out[path] = plan.execute(p).cpu().numpy()
+        filtered = plan.filter(p)
+        # the stage entry with a buffer 4 bytes off a 16-byte boundary
+        flat = torch.empty(filtered.numel() + 1, device="cuda")
+        shifted = flat[1:].view(filtered.shape)
+        shifted.copy_(filtered)
+        assert shifted.data_ptr() % 16 != 0
+        staged = plan.backproject(shifted).cpu().numpy()
+        plan.check()
+        assert K.rel_rmse(staged, out[path]) < 1e-6, path
+        plan.close()
+    assert K.rel_rmse(out["rows"], out["pairs"]) < 1e-6
+    assert K.rel_rmse(out["global"], out["pairs"]) < 1e-6
 
 
 @pytest.mark.parametrize("nu,nv,views", [(96, 64, 12), (53, 41, 7), (192, 24, 5), (384, 8, 3)])
