@@ -385,6 +385,57 @@ YKB_API ykb_status ykb_fdk_execute(ykb_fdk_plan* p, const void* d_proj, int proj
     return YKB_OK;
 }
 
+YKB_API ykb_status ykb_fdk_execute_host(ykb_fdk_plan* p, const void* h_proj, int proj_dtype,
+    int view_offset, int n_views, float* d_volume, int clear_output, ykb_stream stream)
+{
+    clear_error();
+    if (const ykb_status st = check_range(p, h_proj, proj_dtype, view_offset, n_views)) return st;
+    if (!d_volume) return fail(YKB_ERR_INVALID_BUFFER, "null volume buffer");
+    DeviceGuard guard(p->device);
+    const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const size_t view_bytes = static_cast<size_t>(p->nu) * p->nv * dtype_bytes(proj_dtype);
+    // batches of about an eighth of the views (at least 16): the first
+    // batch's copy is the only one left exposed
+    const int batch = std::min(p->batch_capacity, std::max(16, (p->n_views + 7) / 8));
+    if (p->stage_views < batch || p->stage_in.bytes < 2 * batch * static_cast<size_t>(p->nu) * p->nv * 4) {
+        if (p->copy_stream) YKB_TRY_CUDA(cudaStreamSynchronize(p->copy_stream));
+        YKB_TRY_CUDA(cudaStreamSynchronize(s));
+        YKB_TRY_CUDA(p->stage_in.alloc(2 * static_cast<size_t>(batch) * p->nu * p->nv * 4));
+        p->stage_views = batch;
+    }
+    if (!p->copy_stream) {
+        YKB_TRY_CUDA(cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking));
+        for (int i = 0; i < 2; ++i) {
+            YKB_TRY_CUDA(cudaEventCreateWithFlags(&p->copied[i], cudaEventDisableTiming));
+            YKB_TRY_CUDA(cudaEventCreateWithFlags(&p->consumed[i], cudaEventDisableTiming));
+        }
+    }
+    // the copy stream starts after work already queued on `stream` that may
+    // still read the staging slots (a previous call)
+    YKB_TRY_CUDA(cudaEventRecord(p->consumed[0], s));
+    YKB_TRY_CUDA(cudaEventRecord(p->consumed[1], s));
+    const size_t slot_bytes = static_cast<size_t>(p->stage_views) * view_bytes;
+    for (int c = 0, b = 0; c < n_views; c += batch, ++b) {
+        const int cnt = std::min(batch, n_views - c);
+        const int slot = b & 1;
+        char* dst = static_cast<char*>(p->stage_in.ptr) + slot * slot_bytes;
+        YKB_TRY_CUDA(cudaStreamWaitEvent(p->copy_stream, p->consumed[slot], 0));
+        YKB_TRY_CUDA(cudaMemcpyAsync(dst, static_cast<const char*>(h_proj) + c * view_bytes,
+            cnt * view_bytes, cudaMemcpyHostToDevice, p->copy_stream));
+        YKB_TRY_CUDA(cudaEventRecord(p->copied[slot], p->copy_stream));
+        YKB_TRY_CUDA(cudaStreamWaitEvent(s, p->copied[slot], 0));
+        if (const ykb_status st = filter_chunk(p, dst, proj_dtype, view_offset + c, cnt,
+                p->work_filtered.as<float>(), p->layout, p->ld, s))
+            return st;
+        YKB_TRY_CUDA(cudaEventRecord(p->consumed[slot], s));
+        const int accumulate = (c == 0 && clear_output) ? 0 : 1;
+        if (const ykb_status st = backproject_chunk(p, p->work_filtered.ptr, p->layout, p->ld,
+                view_offset + c, cnt, d_volume, accumulate, s))
+            return st;
+    }
+    return YKB_OK;
+}
+
 YKB_API ykb_status ykb_fdk_check(ykb_fdk_plan* p, ykb_stream stream)
 {
     clear_error();

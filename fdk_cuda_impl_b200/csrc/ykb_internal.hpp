@@ -231,6 +231,18 @@ struct ykb_fdk_plan {
     ykb::DeviceBuffer work_a;    // preweighted rows: float, or bf16 hi then lo
     ykb::DeviceBuffer work_filtered;  // filtered projections (layout, pitch ld)
     ykb::DeviceBuffer err_flag;  // int[4]: device error word, box pre-pass scratch
+    // host-input streaming (ykb_fdk_execute_host), created on first use
+    ykb::DeviceBuffer stage_in;  // two batches of input views
+    int stage_views = 0;         // views per batch slot
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t copied[2] = {nullptr, nullptr};    // batch slot filled
+    cudaEvent_t consumed[2] = {nullptr, nullptr};  // batch slot read by the filter
+    ~ykb_fdk_plan()
+    {
+        for (cudaEvent_t e : copied) if (e) cudaEventDestroy(e);
+        for (cudaEvent_t e : consumed) if (e) cudaEventDestroy(e);
+        if (copy_stream) cudaStreamDestroy(copy_stream);
+    }
 };
 
 struct ykb_joseph_plan {

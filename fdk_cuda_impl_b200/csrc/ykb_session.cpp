@@ -292,17 +292,7 @@ private:
 
     bool run_fdk_(const SExecutionRequest& r, int offset, int count)
     {
-        const size_t proj_bytes = static_cast<size_t>(nu_) * nv_ * count * sizeof(float);
         const size_t vol_bytes = static_cast<size_t>(volume_.nx) * volume_.ny * volume_.nz * sizeof(float);
-        const float* d_proj = r.projection.data;
-        if (r.projection.location == EMemoryLocation::Host) {
-            if (!proj_scratch_.ensure(proj_bytes))
-                return fail_(EApiErrorCode::CudaError, "device projection staging allocation failed");
-            cudaError_t e = cudaMemcpyAsync(proj_scratch_.ptr, r.projection.data, proj_bytes,
-                cudaMemcpyHostToDevice, stream_);
-            if (e != cudaSuccess) return cuda_fail_(e, "projection upload");
-            d_proj = static_cast<const float*>(proj_scratch_.ptr);
-        }
         float* d_vol = r.volume.data;
         if (r.volume.location == EMemoryLocation::Host) {
             // a host volume accumulates in device scratch across batches and is
@@ -311,9 +301,15 @@ private:
                 return fail_(EApiErrorCode::CudaError, "device volume scratch allocation failed");
             d_vol = static_cast<float*>(vol_scratch_.ptr);
         }
-        if (ykb_fdk_execute(fdk_, d_proj, YKB_DTYPE_F32, offset, count, d_vol,
-                r.clear_output ? 1 : 0, stream_) != YKB_OK)
-            return fail_(EApiErrorCode::CudaError, ykb_last_error());
+        // host projections stream in batches, their copies overlapping the
+        // kernels of earlier batches (the reference copies each 32-view chunk
+        // synchronously: YkFdkPipeline.hpp:454-457)
+        const ykb_status st = r.projection.location == EMemoryLocation::Host
+            ? ykb_fdk_execute_host(fdk_, r.projection.data, YKB_DTYPE_F32, offset, count, d_vol,
+                  r.clear_output ? 1 : 0, stream_)
+            : ykb_fdk_execute(fdk_, r.projection.data, YKB_DTYPE_F32, offset, count, d_vol,
+                  r.clear_output ? 1 : 0, stream_);
+        if (st != YKB_OK) return fail_(EApiErrorCode::CudaError, ykb_last_error());
         if (r.volume.location == EMemoryLocation::Host && received_ + count == view_count_) {
             const cudaError_t e = cudaMemcpyAsync(r.volume.data, d_vol, vol_bytes,
                 cudaMemcpyDeviceToHost, stream_);

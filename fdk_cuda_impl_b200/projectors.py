@@ -91,6 +91,25 @@ class FdkPlan:
                                          1 if clear else 0, _stream_handle(self.device)))
         return volume
 
+    def execute_host(self, proj: torch.Tensor, volume: torch.Tensor | None = None,
+                     view_offset: int = 0, clear: bool = True) -> torch.Tensor:
+        """FDK of projections held in host memory (pin them for copy/compute
+        overlap): batches stream to the device while earlier ones are filtered
+        and backprojected.  Asynchronous on the current stream; `proj` must
+        stay alive and unchanged until that stream has run the work."""
+        n = proj.shape[0]
+        if proj.device.type != "cpu" or not proj.is_contiguous():
+            raise ValueError("projections must be a contiguous host tensor")
+        if tuple(proj.shape) != (n, self.nv, self.nu) or proj.dtype not in (torch.float32,
+                                                                              torch.bfloat16):
+            raise ValueError(f"projections must be float32/bfloat16 [n][{self.nv}][{self.nu}]")
+        volume = self._vol_out(volume)
+        L.check(self.lib.ykb_fdk_execute_host(self._h, C.c_void_p(proj.data_ptr()),
+                                              _dtype_code(proj), view_offset, n,
+                                              C.c_void_p(volume.data_ptr()), 1 if clear else 0,
+                                              _stream_handle(self.device)))
+        return volume
+
     def filter(self, proj: torch.Tensor, view_offset: int = 0) -> torch.Tensor:
         n = proj.shape[0]
         _check_tensor(proj, (n, self.nv, self.nu), (torch.float32, torch.bfloat16), self.device,

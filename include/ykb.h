@@ -152,6 +152,20 @@ YKB_API ykb_status ykb_fdk_execute(ykb_fdk_plan* plan, const void* d_proj,
     int proj_dtype, int view_offset, int n_views, float* d_volume,
     int clear_output, ykb_stream stream);
 
+/* The same FDK with the projections in HOST memory: the views are copied
+ * to the device in batches on an internal copy stream, double-buffered, so
+ * that the copy of batch b+1 overlaps the filter and backprojection of
+ * batch b on `stream`.  Pinned (page-locked) h_proj gives full overlap; a
+ * pageable buffer works but each batch copy first passes through the
+ * driver's staging on the calling thread.  Returns once the work is
+ * enqueued; h_proj must stay valid and unchanged until `stream` has
+ * completed it.  Replaces the host-projection path of FdkPipeline::enqueueBatch
+ * (YkFdkPipeline.hpp:388-488, chunk uploads :454-457), which copies each
+ * 32-view chunk synchronously in between its kernels. */
+YKB_API ykb_status ykb_fdk_execute_host(ykb_fdk_plan* plan, const void* h_proj,
+    int proj_dtype, int view_offset, int n_views, float* d_volume,
+    int clear_output, ykb_stream stream);
+
 /* Stage entry: preweight + ramp filter only; d_filtered receives
  * [n_views][nv][nu] float.  Replaces PreweightProcessor::apply +
  * FilterProcessor::apply (.../FDK/YkFDKPreWeightProcessor.hpp,
