@@ -73,6 +73,9 @@ SIGNATURES = {
     "ykb_fdk_plan_create": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_float,
                                       C.POINTER(Volume), C.POINTER(Filter), C.c_int, C.c_int,
                                       C.POINTER(_P)]),
+    "ykb_fdk_plan_create_ex": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float,
+                                         C.c_int, C.POINTER(Volume), C.POINTER(Filter), C.c_int,
+                                         C.c_int, C.c_int, C.POINTER(_P)]),
     "ykb_fdk_plan_destroy": (C.c_int, [_P]),
     "ykb_fdk_execute": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_int, _P, C.c_int, _P]),
     "ykb_fdk_execute_host": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_int, _P, C.c_int, _P]),

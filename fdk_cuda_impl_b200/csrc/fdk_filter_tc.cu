@@ -248,8 +248,8 @@ __global__ void __launch_bounds__(128, 1) ramp_tc_kernel(
 
 // preweighted rows split into bf16 hi and lo parts, rows padded to lda
 __global__ void __launch_bounds__(128) preweight_split_kernel(const void* __restrict__ in, int in_bf16,
-    const FdkPreweightView* __restrict__ pw, int nu, int nv, int lda, __nv_bfloat16* __restrict__ hi,
-    __nv_bfloat16* __restrict__ lo)
+    const FdkPreweightView* __restrict__ pw, const float* __restrict__ parker, int nu, int nv,
+    int lda, __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo)
 {
     const long row = blockIdx.x;
     const int view = static_cast<int>(row / nv);
@@ -271,7 +271,9 @@ __global__ void __launch_bounds__(128) preweight_split_kernel(const void* __rest
             const float v = in_bf16
                 ? __bfloat162float(static_cast<const __nv_bfloat16*>(in)[row * nu + iu])
                 : static_cast<const float*>(in)[row * nu + iu];
-            x = v * static_cast<float>(scale * r);
+            float wt = static_cast<float>(scale * r);
+            if (parker) wt *= parker[static_cast<long>(view) * nu + iu];
+            x = v * wt;
         }
         const __nv_bfloat16 h = __float2bfloat16_rn(x);
         hi[row * lda + iu] = h;
@@ -341,13 +343,13 @@ bool tcgen05_filter_supported(int nu) { return tma_encode() != nullptr && nu >= 
 int tc_filter_lda(int nu) { return (nu + TK - 1) / TK * TK; }
 
 cudaError_t launch_fdk_preweight_split_bf16(const void* proj, int proj_dtype,
-    const FdkPreweightView* pw, int n_views, int nu, int nv, int ld, __nv_bfloat16* hi,
-    __nv_bfloat16* lo, cudaStream_t s)
+    const FdkPreweightView* pw, const float* parker, int n_views, int nu, int nv, int ld,
+    __nv_bfloat16* hi, __nv_bfloat16* lo, cudaStream_t s)
 {
     const long rows = static_cast<long>(n_views) * nv;
     if (rows <= 0) return cudaSuccess;
     preweight_split_kernel<<<static_cast<unsigned>(rows), 128, 0, s>>>(proj,
-        proj_dtype == YKB_DTYPE_BF16 ? 1 : 0, pw, nu, nv, ld, hi, lo);
+        proj_dtype == YKB_DTYPE_BF16 ? 1 : 0, pw, parker, nu, nv, ld, hi, lo);
     return cudaGetLastError();
 }
 

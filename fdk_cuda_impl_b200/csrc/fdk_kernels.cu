@@ -20,7 +20,8 @@ template <> __device__ __forceinline__ float load_as_float<__nv_bfloat16>(const 
 // 1/|q| by an FP32 rsqrt refined with one FP64 Newton step.
 template <typename TIn>
 __global__ void __launch_bounds__(128) preweight_kernel(const TIn* __restrict__ in,
-    const FdkPreweightView* __restrict__ pw, int nu, int nv, float* __restrict__ out)
+    const FdkPreweightView* __restrict__ pw, const float* __restrict__ parker, int nu, int nv,
+    float* __restrict__ out)
 {
     const long row = blockIdx.x;
     const int view = static_cast<int>(row / nv);
@@ -40,7 +41,9 @@ __global__ void __launch_bounds__(128) preweight_kernel(const TIn* __restrict__ 
         double r = rsqrtf(static_cast<float>(r2));
         r = r * (1.5 - 0.5 * r2 * r * r);
         const bool placed = iu >= p.in_lo && iu < p.in_hi;
-        dst[iu] = placed ? load_as_float(src + iu) * static_cast<float>(scale * r) : 0.f;
+        float wt = static_cast<float>(scale * r);
+        if (parker) wt *= parker[static_cast<long>(view) * nu + iu];
+        dst[iu] = placed ? load_as_float(src + iu) * wt : 0.f;
     }
 }
 
@@ -246,16 +249,17 @@ __global__ void __launch_bounds__(256) fdk_bp_kernel(const T* __restrict__ proj,
 } // namespace
 
 cudaError_t launch_fdk_preweight(const void* proj, int proj_dtype,
-    const FdkPreweightView* pw, int n_views, int nu, int nv, float* out, cudaStream_t s)
+    const FdkPreweightView* pw, const float* parker, int n_views, int nu, int nv, float* out,
+    cudaStream_t s)
 {
     const long rows = static_cast<long>(n_views) * nv;
     if (rows <= 0) return cudaSuccess;
     if (proj_dtype == YKB_DTYPE_BF16)
         preweight_kernel<__nv_bfloat16><<<static_cast<unsigned>(rows), 128, 0, s>>>(
-            static_cast<const __nv_bfloat16*>(proj), pw, nu, nv, out);
+            static_cast<const __nv_bfloat16*>(proj), pw, parker, nu, nv, out);
     else
         preweight_kernel<float><<<static_cast<unsigned>(rows), 128, 0, s>>>(
-            static_cast<const float*>(proj), pw, nu, nv, out);
+            static_cast<const float*>(proj), pw, parker, nu, nv, out);
     return cudaGetLastError();
 }
 

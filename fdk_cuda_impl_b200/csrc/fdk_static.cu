@@ -106,7 +106,8 @@ extern "C" YKB_API ykb_status ykb_fdk_filter_static(const ykb_cone_view* views, 
         const int cnt = std::min(chunk, n_views - c);
         const char* in = static_cast<const char*>(d_proj) +
             static_cast<size_t>(c) * nu * nv * in_elem;
-        YKB_TRY_CUDA(launch_fdk_preweight(in, proj_dtype, d_records + c, cnt, nu, nv, d_rows, s));
+        YKB_TRY_CUDA(launch_fdk_preweight(in, proj_dtype, d_records + c, nullptr, cnt, nu, nv,
+            d_rows, s));
         YKB_TRY_CUDA(launch_fdk_ramp_fp32(d_rows, d_lags, d_records + c, cnt, nu, nv,
             d_filtered + static_cast<size_t>(c) * nu * nv, kFilteredScalar, nu, s));
     }

@@ -115,8 +115,21 @@ YKB_API ykb_status ykb_fdk_plan_create(const ykb_cone_view* views, int n_views, 
     float scan_range_rad, const ykb_volume* volume, const ykb_filter* filter, int precision,
     int device, ykb_fdk_plan** plan_out)
 {
+    return ykb_fdk_plan_create_ex(views, n_views, nu, nv, scan_range_rad, 0.f, 1, volume, filter,
+        precision, YKB_PARKER_DISABLED, device, plan_out);
+}
+
+YKB_API ykb_status ykb_fdk_plan_create_ex(const ykb_cone_view* views, int n_views, int nu, int nv,
+    float scan_range_rad, float start_angle_rad, int rotation_direction, const ykb_volume* volume,
+    const ykb_filter* filter, int precision, int parker_mode, int device, ykb_fdk_plan** plan_out)
+{
     clear_error();
     if (!plan_out) return fail(YKB_ERR_INVALID_BUFFER, "null plan output");
+    if (parker_mode != YKB_PARKER_AUTO && parker_mode != YKB_PARKER_DISABLED &&
+        parker_mode != YKB_PARKER_ENABLED)
+        return fail(YKB_ERR_INVALID_CONFIG, "unknown Parker mode");
+    if (rotation_direction != 1 && rotation_direction != -1)
+        return fail(YKB_ERR_INVALID_CONFIG, "rotation direction must be +1 or -1");
     *plan_out = nullptr;
     if (!views || n_views <= 0 || nu <= 0 || nv <= 0)
         return fail(YKB_ERR_INVALID_CONFIG, "views, view count and detector size must be positive");
@@ -134,6 +147,16 @@ YKB_API ykb_status ykb_fdk_plan_create(const ykb_cone_view* views, int n_views, 
     p->precision = precision;
     std::string why;
     if (!derive_fdk_geometry(views, n_views, nu, nv, scan_range_rad, p->derived, why)) {
+        delete p;
+        return fail(YKB_ERR_INVALID_GEOMETRY, why);
+    }
+    // Parker weighting: Enabled, or Auto on a short scan
+    // (include/YKCBCT/interface/YkSystemReconstruction.hpp:29-39)
+    const bool parker = parker_mode == YKB_PARKER_ENABLED ||
+        (parker_mode == YKB_PARKER_AUTO && scan_range_rad < 6.28318530717958647692f - 1e-5f);
+    std::vector<float> parker_w;
+    if (parker && !build_parker_weights(p->derived, views, nu, nv, scan_range_rad,
+            start_angle_rad, rotation_direction, parker_w, why)) {
         delete p;
         return fail(YKB_ERR_INVALID_GEOMETRY, why);
     }
@@ -169,6 +192,13 @@ YKB_API ykb_status ykb_fdk_plan_create(const ykb_cone_view* views, int n_views, 
         (e = cudaMemset(p->err_flag.ptr, 0, 4 * sizeof(int))) != cudaSuccess) {
         delete p;
         return cuda_status(e, "cudaMemcpy (FDK plan tables)");
+    }
+    if (!parker_w.empty() &&
+        ((e = p->parker.alloc(parker_w.size() * sizeof(float))) != cudaSuccess ||
+         (e = cudaMemcpy(p->parker.ptr, parker_w.data(), parker_w.size() * sizeof(float),
+              cudaMemcpyHostToDevice)) != cudaSuccess)) {
+        delete p;
+        return cuda_status(e, "Parker weight table");
     }
     if (p->tc_filter) {
         // Toeplitz operand T[j][k] = h(j-k) split into bf16 hi and lo parts
@@ -240,7 +270,8 @@ YKB_API size_t ykb_fdk_workspace_bytes(const ykb_fdk_plan* p)
 {
     if (!p) return 0;
     return p->coef.bytes + p->pwv.bytes + p->ramp.bytes + p->toeplitz_hi.bytes +
-        p->toeplitz_lo.bytes + p->work_a.bytes + p->work_filtered.bytes + p->err_flag.bytes;
+        p->toeplitz_lo.bytes + p->work_a.bytes + p->work_filtered.bytes + p->err_flag.bytes +
+        p->parker.bytes + p->stage_in.bytes;
 }
 
 namespace {
@@ -265,18 +296,20 @@ ykb_status filter_chunk(ykb_fdk_plan* p, const void* proj, int proj_dtype, int f
     float* dst, int layout, int ldc, cudaStream_t s)
 {
     const FdkPreweightView* pwv = p->pwv.as<FdkPreweightView>() + first;
+    const float* parker = p->parker.ptr ? p->parker.as<float>() + static_cast<size_t>(first) * p->nu
+                                        : nullptr;
     if (p->tc_filter) {
         const size_t half = static_cast<size_t>(p->batch_capacity) * p->nv * p->lda;
         __nv_bfloat16* a_hi = p->work_a.as<__nv_bfloat16>();
         __nv_bfloat16* a_lo = a_hi + half;
-        YKB_TRY_CUDA(launch_fdk_preweight_split_bf16(proj, proj_dtype, pwv, count, p->nu, p->nv,
+        YKB_TRY_CUDA(launch_fdk_preweight_split_bf16(proj, proj_dtype, pwv, parker, count, p->nu, p->nv,
             p->lda, a_hi, a_lo, s));
         YKB_TRY_CUDA(launch_fdk_ramp_tcgen05(a_hi, a_lo, p->toeplitz_hi.as<__nv_bfloat16>(),
             p->toeplitz_lo.as<__nv_bfloat16>(), count * p->nv, p->nu, p->lda, pwv, p->nv,
             dst, layout, ldc, p->err_flag.as<int>(), s));
         return YKB_OK;
     }
-    YKB_TRY_CUDA(launch_fdk_preweight(proj, proj_dtype, pwv, count, p->nu, p->nv,
+    YKB_TRY_CUDA(launch_fdk_preweight(proj, proj_dtype, pwv, parker, count, p->nu, p->nv,
         p->work_a.as<float>(), s));
     YKB_TRY_CUDA(launch_fdk_ramp_fp32(p->work_a.as<float>(), p->ramp.as<float>(), pwv, count,
         p->nu, p->nv, dst, layout, ldc, s));

@@ -229,6 +229,75 @@ bool derive_fdk_geometry(const ykb_cone_view* views, int n, int nu, int nv,
 // Affine projection rows in FP64 (the algebra of fdk_precompute_coeffs_kernel,
 // .../FDK/kernels/YkFDKBpPrecompute.cu:14-138, kept in double) and the
 // per-view preweight/placement records.
+// Parker short-scan weights per (view, column), FP64, with the range/pi
+// scale folded in.  Restates .../FDK/kernels/YkFDKParkerKernels.cu:46-110
+// (fan angle of column u on the centre row against the radial ray, Gamma =
+// the larger edge |fan| of the view, sin^2 ramps of width 2(Gamma +- gamma)),
+// the relative angle of pk_uploadAngles (:117-138) and the coverage check of
+// FdkPipeline::validateParkerCoverage_ (YkFdkPipeline.hpp:597-635).
+bool build_parker_weights(const std::vector<FdkDerived>& g, const ykb_cone_view* views, int nu,
+    int nv, double scan_range, double start_angle, int direction, std::vector<float>& w,
+    std::string& why)
+{
+    const double pi = 3.14159265358979323846;
+    if (direction != 1 && direction != -1) { why = "rotation direction must be +1 or -1"; return false; }
+    if (scan_range >= 2.0 * pi - 1e-5) {
+        why = "Parker weighting needs a short scan (range below 2 pi)";
+        return false;
+    }
+    const int n = static_cast<int>(g.size());
+    const double cv = 0.5 * (nv - 1);
+    double max_fan = 0.0;
+    for (const FdkDerived& d : g) {
+        const double cu = 0.5 * (nu - 1);
+        const double px = d.detS.x + cu * d.detU.x + cv * d.detV.x - d.src.x;
+        const double py = d.detS.y + cu * d.detU.y + cv * d.detV.y - d.src.y;
+        for (double u : {0.0, static_cast<double>(nu - 1)}) {
+            const double rx = d.detS.x + u * d.detU.x + cv * d.detV.x - d.src.x;
+            const double ry = d.detS.y + u * d.detU.y + cv * d.detV.y - d.src.y;
+            max_fan = std::max(max_fan, std::fabs(std::atan2(rx * py - ry * px, rx * px + ry * py)));
+        }
+    }
+    if (scan_range + 1e-5 < pi + 2.0 * max_fan) {
+        why = "short scan too short for Parker weighting (needs pi + 2 x fan angle)";
+        return false;
+    }
+    const double scale = scan_range / pi, eps = 1e-6;
+    w.assign(static_cast<size_t>(n) * nu, 0.f);
+    for (int i = 0; i < n; ++i) {
+        const FdkDerived& d = g[i];
+        auto fan = [&](double u) {
+            const double rx = d.detS.x + u * d.detU.x + cv * d.detV.x - d.src.x;
+            const double ry = d.detS.y + u * d.detU.y + cv * d.detV.y - d.src.y;
+            return std::atan2(rx * d.radial.y - ry * d.radial.x, rx * d.radial.x + ry * d.radial.y);
+        };
+        const double Gamma = std::max(std::fabs(fan(0.0)), std::fabs(fan(nu - 1.0)));
+        double beta = direction * (static_cast<double>(views[i].angle.x) - start_angle);
+        while (beta < 0.0) beta += 2.0 * pi;
+        while (beta >= 2.0 * pi) beta -= 2.0 * pi;
+        for (int u = 0; u < nu; ++u) {
+            const double gamma = direction * fan(u);
+            const double t1 = 2.0 * (Gamma + gamma), t2 = pi + 2.0 * gamma, t3 = pi + 2.0 * Gamma;
+            double x = 0.0;
+            if (beta <= 0.0) {
+                x = 0.0;
+            } else if (beta < t1) {
+                const double dd = Gamma + gamma;
+                const double sn = std::sin(0.25 * pi * beta / (std::fabs(dd) > eps ? dd : eps));
+                x = sn * sn;
+            } else if (beta <= t2) {
+                x = 1.0;
+            } else if (beta < t3) {
+                const double dd = Gamma - gamma;
+                const double sn = std::sin(0.25 * pi * (t3 - beta) / (std::fabs(dd) > eps ? dd : eps));
+                x = sn * sn;
+            }
+            w[static_cast<size_t>(i) * nu + u] = static_cast<float>(x * scale);
+        }
+    }
+    return true;
+}
+
 void build_fdk_coefficients(const std::vector<FdkDerived>& g, int nu,
     std::vector<FdkViewCoef>& coef, std::vector<FdkPreweightView>& pw, bool& axial)
 {

@@ -117,6 +117,9 @@ struct alignas(16) FdkPreweightView {
     int out_lo, out_hi; // outputs [out_lo, out_hi) fall inside the padded row
 };
 
+bool build_parker_weights(const std::vector<FdkDerived>& g, const ykb_cone_view* views, int nu,
+    int nv, double scan_range, double start_angle, int direction, std::vector<float>& w,
+    std::string& why);
 void build_fdk_coefficients(const std::vector<FdkDerived>& g, int nu,
     std::vector<FdkViewCoef>& coef, std::vector<FdkPreweightView>& pw,
     bool& axial);
@@ -160,14 +163,16 @@ VolumeGrid make_grid(const ykb_volume& v);
 // u = -1 still sees (0, f[0]).
 enum FilteredLayout : int { kFilteredScalar = 0, kFilteredPairs = 1 };
 constexpr int kPairLead = 2;
+// parker: per-(view, column) weights [n_views][nu] multiplied in after the
+// cosine weight (short scans), or nullptr
 cudaError_t launch_fdk_preweight(const void* proj, int proj_dtype,
-    const FdkPreweightView* pw, int n_views, int nu, int nv, float* out,
+    const FdkPreweightView* pw, const float* parker, int n_views, int nu, int nv, float* out,
     cudaStream_t s);
 cudaError_t launch_fdk_ramp_fp32(const float* pw_rows, const float* h_dev,
     const FdkPreweightView* pwv, int n_views, int nu, int nv, float* out,
     int layout, int ldc, cudaStream_t s);
 cudaError_t launch_fdk_preweight_split_bf16(const void* proj, int proj_dtype,
-    const FdkPreweightView* pw, int n_views, int nu, int nv, int ld,
+    const FdkPreweightView* pw, const float* parker, int n_views, int nu, int nv, int ld,
     __nv_bfloat16* hi, __nv_bfloat16* lo, cudaStream_t s);
 cudaError_t launch_fdk_ramp_tcgen05(const __nv_bfloat16* a_hi,
     const __nv_bfloat16* a_lo, const __nv_bfloat16* t_hi,
@@ -227,6 +232,7 @@ struct ykb_fdk_plan {
     ykb::DeviceBuffer coef;      // FdkViewCoef[n_views]
     ykb::DeviceBuffer pwv;       // FdkPreweightView[n_views]
     ykb::DeviceBuffer ramp;      // float[2*nu-1]
+    ykb::DeviceBuffer parker;    // float[n_views][nu] short-scan weights, or empty
     ykb::DeviceBuffer toeplitz_hi, toeplitz_lo;  // bf16 [nu][ld] (BF16 plans)
     ykb::DeviceBuffer work_a;    // preweighted rows: float, or bf16 hi then lo
     ykb::DeviceBuffer work_filtered;  // filtered projections (layout, pitch ld)

@@ -18,17 +18,6 @@ bool has_bytes(uint32_t actual, size_t required) { return actual >= required; }
 
 bool valid_location(EMemoryLocation l) { return l == EMemoryLocation::Host || l == EMemoryLocation::Device; }
 
-// resolveParkerEnabled (include/YKCBCT/interface/YkSystemReconstruction.hpp:29-39)
-bool parker_enabled(const SSystemConfig& g, const SReconstructionSpec& r)
-{
-    if (r.fdk.parker.mode == EParkerMode::Enabled) return true;
-    if (r.fdk.parker.mode == EParkerMode::Disabled) return false;
-    constexpr float kTwoPi = 6.28318530717958647692f;
-    const float range = kTwoPi * static_cast<float>(g.circular.total_views) /
-        static_cast<float>(g.circular.views_per_turn);
-    return range < kTwoPi - 1e-5f;
-}
-
 // SRigidTransform::aroundEulerPoint(centre, rx, ry, rz).inverse() applied to
 // a view (include/YKCBCT/geometry/YkRigidTransform.hpp,
 // transformProjectionGeometry in YkProjectionGeometry.hpp:229-247)
@@ -180,16 +169,15 @@ public:
                 views_.clear();
                 return fail_(EApiErrorCode::InvalidGeometry, "invalid analytic filter parameters");
             }
-            if (parker_enabled(g, r)) {
-                views_.clear();
-                return fail_(EApiErrorCode::UnsupportedCombination,
-                    "short-scan (Parker) FDK is not provided by this library");
-            }
             const ykb_filter filt{static_cast<int>(f.type), f.cutoff, f.gain, f.butterworth_order,
                 f.kaiser_beta, f.tukey_alpha};
             const float range = ykb_regular_scan_range(spec.total_views, spec.views_per_turn);
-            if (ykb_fdk_plan_create(views_.data(), spec.total_views, nu_, nv_, range, &volume_, &filt,
-                    YKB_PRECISION_FP32, device_, &fdk_) != YKB_OK) {
+            // Parker: EParkerMode values map one to one; Auto weights short
+            // scans (resolveParkerEnabled, YkSystemReconstruction.hpp:29-39)
+            if (ykb_fdk_plan_create_ex(views_.data(), spec.total_views, nu_, nv_, range,
+                    spec.start_angle_rad, spec.rotation_direction, &volume_, &filt,
+                    YKB_PRECISION_FP32, static_cast<int>(r.fdk.parker.mode), device_,
+                    &fdk_) != YKB_OK) {
                 const std::string msg = ykb_last_error();
                 release();
                 return fail_(EApiErrorCode::InvalidGeometry, msg.c_str());

@@ -39,12 +39,20 @@ def _dtype_code(t: torch.Tensor) -> int:
     return L.DTYPE_BF16 if t.dtype == torch.bfloat16 else L.DTYPE_F32
 
 
+PARKER_MODES = {"auto": 0, "disabled": 1, "enabled": 2}
+
+
 class FdkPlan:
-    """FDK for a fixed view sequence (ykb_fdk_plan_create)."""
+    """FDK for a fixed view sequence (ykb_fdk_plan_create_ex).
+
+    parker: None (no short-scan weighting) or "auto" / "enabled" / "disabled"
+    (YK::EParkerMode); the short-scan weights measure each view's position
+    from start_angle_rad in rotation_direction (+1/-1)."""
 
     def __init__(self, views: np.ndarray, nu: int, nv: int, scan_range: float,
                  grid: VolumeGrid, filt: RampFilter | None = None, precision: str = "fp32",
-                 device: int = 0):
+                 device: int = 0, parker: str | None = None, start_angle_rad: float = 0.0,
+                 rotation_direction: int = 1):
         self.lib = L.load()
         self.views = np.ascontiguousarray(views, dtype=L.VIEW_DTYPE)
         self.nu, self.nv, self.grid, self.device = nu, nv, grid, device
@@ -53,9 +61,11 @@ class FdkPlan:
         self._vol = grid.struct()
         self._flt = self.filt.struct()
         h = C.c_void_p()
-        L.check(self.lib.ykb_fdk_plan_create(L.views_ptr(self.views), len(self.views), nu, nv,
-                                             scan_range, C.byref(self._vol), C.byref(self._flt),
-                                             self.precision, device, C.byref(h)))
+        mode = PARKER_MODES["disabled" if parker is None else parker]
+        L.check(self.lib.ykb_fdk_plan_create_ex(L.views_ptr(self.views), len(self.views), nu, nv,
+                                                scan_range, start_angle_rad, rotation_direction,
+                                                C.byref(self._vol), C.byref(self._flt),
+                                                self.precision, mode, device, C.byref(h)))
         self._h = h
 
     @property

@@ -141,6 +141,28 @@ YKB_API ykb_status ykb_fdk_plan_create(const ykb_cone_view* views, int n_views,
     int nu, int nv, float scan_range_rad, const ykb_volume* volume,
     const ykb_filter* filter, int precision, int device, ykb_fdk_plan** plan);
 
+/* Parker short-scan weighting (YK::EParkerMode values, include/YKCBCT/
+ * algorithms/analytic/YkFdkParams.hpp): AUTO weights scans shorter than 2 pi. */
+typedef enum {
+    YKB_PARKER_AUTO = 0,
+    YKB_PARKER_DISABLED = 1,
+    YKB_PARKER_ENABLED = 2
+} ykb_parker_mode;
+
+/* ykb_fdk_plan_create with Parker weighting for short scans: views keep the
+ * scan's start angle and rotation direction (+1/-1), from which each view's
+ * position along the scan is measured.  Enabled (or Auto below 2 pi) on a
+ * scan shorter than pi + 2 x fan angle, or on a full turn, is
+ * YKB_ERR_INVALID_GEOMETRY, as the reference's prepare rejects it
+ * (src/Reconstruction/Analytic/Circular/Flat/FDK/YkFdkPipeline.hpp:597-635).
+ * The weights are those of .../FDK/kernels/YkFDKParkerKernels.cu:46-138,
+ * applied between the cosine preweight and the ramp filter.
+ * ykb_fdk_plan_create is this call with YKB_PARKER_DISABLED. */
+YKB_API ykb_status ykb_fdk_plan_create_ex(const ykb_cone_view* views, int n_views,
+    int nu, int nv, float scan_range_rad, float start_angle_rad,
+    int rotation_direction, const ykb_volume* volume, const ykb_filter* filter,
+    int precision, int parker_mode, int device, ykb_fdk_plan** plan);
+
 YKB_API ykb_status ykb_fdk_plan_destroy(ykb_fdk_plan* plan);
 
 /* Cosine preweight + ramp filter + weighted backprojection of views

@@ -576,11 +576,83 @@ int orc_ramp_kernel(int nu, double du, const orc_filter* f, double* h)
     return 0;
 }
 
+// Parker short-scan weights, restating
+// .../FDK/kernels/YkFDKParkerKernels.cu:46-110 (weight per column, sin^2 ramps
+// of width 2(Gamma +- gamma)), pk_uploadAngles :117-138 (beta), the
+// processor's scale range/pi (.../FDK/YkFDKParkerWeightProcessor.hpp:30-40)
+// and the coverage check of YkFdkPipeline.hpp:597-635.
+int orc_parker_weights(const orc_view* views, int n, int nu, int nv, float range,
+    float start_angle, int direction, double* w)
+{
+    if (!views || !w || n <= 0 || nu <= 0 || nv <= 0 || (direction != 1 && direction != -1))
+        return -1;
+    std::vector<Derived> g;
+    if (!derive(views, n, nu, nv, range, g)) return -2;
+    const double pi = kPi;
+    if (static_cast<double>(range) >= 2.0 * pi - 1e-5) return -3;
+    const double cv = 0.5 * (nv - 1);
+    // coverage: pi + 2 * the largest edge fan angle against the principal ray
+    double max_fan = 0.0;
+    for (int i = 0; i < n; ++i) {
+        const Derived& d = g[i];
+        const d3 c = addd(d.detS, addd(scaled(d.detU, 0.5 * (nu - 1)), scaled(d.detV, cv)));
+        const double px = c.x - d.src.x, py = c.y - d.src.y;
+        for (double u : {0.0, static_cast<double>(nu - 1)}) {
+            const d3 e = addd(d.detS, addd(scaled(d.detU, u), scaled(d.detV, cv)));
+            const double rx = e.x - d.src.x, ry = e.y - d.src.y;
+            max_fan = std::max(max_fan, std::fabs(std::atan2(rx * py - ry * px, rx * px + ry * py)));
+        }
+    }
+    if (static_cast<double>(range) + 1e-5 < pi + 2.0 * max_fan) return -3;
+    const double scale = static_cast<double>(range) / pi;
+    const double eps = 1e-6;
+    for (int i = 0; i < n; ++i) {
+        const Derived& d = g[i];
+        auto fan = [&](double u) {
+            const double rx = d.detS.x + u * d.detU.x + cv * d.detV.x - d.src.x;
+            const double ry = d.detS.y + u * d.detU.y + cv * d.detV.y - d.src.y;
+            return std::atan2(rx * d.radial.y - ry * d.radial.x, rx * d.radial.x + ry * d.radial.y);
+        };
+        const double Gamma = std::max(std::fabs(fan(0.0)), std::fabs(fan(nu - 1.0)));
+        double beta = direction * (static_cast<double>(views[i].angle[0]) - start_angle);
+        while (beta < 0.0) beta += 2.0 * pi;
+        while (beta >= 2.0 * pi) beta -= 2.0 * pi;
+        for (int u = 0; u < nu; ++u) {
+            const double gamma = direction * fan(u);
+            const double t1 = 2.0 * (Gamma + gamma), t2 = pi + 2.0 * gamma, t3 = pi + 2.0 * Gamma;
+            double x;
+            if (beta <= 0.0) {
+                x = 0.0;
+            } else if (beta < t1) {
+                const double dd = Gamma + gamma;
+                const double sn = std::sin(0.25 * pi * beta / (std::fabs(dd) > eps ? dd : eps));
+                x = sn * sn;
+            } else if (beta <= t2) {
+                x = 1.0;
+            } else if (beta < t3) {
+                const double dd = Gamma - gamma;
+                const double sn = std::sin(0.25 * pi * (t3 - beta) / (std::fabs(dd) > eps ? dd : eps));
+                x = sn * sn;
+            } else {
+                x = 0.0;
+            }
+            w[static_cast<size_t>(i) * nu + u] = x * scale;
+        }
+    }
+    return 0;
+}
+
 // Preweight (.../FDK/kernels/YkFDKPreWeightKernels.cu:374-402) followed by the
 // padded circular convolution (.../FDK/kernels/YkFDKFilterKernels.cu:32-125),
 // written as its equivalent masked Toeplitz product.
 int orc_fdk_filter(const orc_view* views, int n, int nu, int nv, float range,
     const orc_filter* filter, const float* proj, double* filtered)
+{
+    return orc_fdk_filter_weighted(views, n, nu, nv, range, filter, proj, nullptr, filtered);
+}
+
+int orc_fdk_filter_weighted(const orc_view* views, int n, int nu, int nv, float range,
+    const orc_filter* filter, const float* proj, const double* row_weights, double* filtered)
 {
     if (!filter || !proj || !filtered) return -1;
     std::vector<Derived> g;
@@ -604,7 +676,8 @@ int orc_fdk_filter(const orc_view* views, int n, int nu, int nv, float range,
                 const d3 q = subd(addd(d.detS, addd(scaled(d.detU, iu), scaled(d.detV, iv))), d.src);
                 const double wcos = d.dsd / std::sqrt(std::max(dotd(q, q), 1e-20));
                 const bool placed = (iu + d.startU) >= 0 && (iu + d.startU) < N;
-                row[iu] = placed ? static_cast<double>(src[iu]) * wcos * wgeom : 0.0;
+                const double extra = row_weights ? row_weights[static_cast<size_t>(i) * nu + iu] : 1.0;
+                row[iu] = placed ? static_cast<double>(src[iu]) * wcos * wgeom * extra : 0.0;
             }
             double* dst = filtered + static_cast<size_t>(r) * nu;
             for (int j = 0; j < nu; ++j) {
@@ -657,9 +730,16 @@ int orc_fdk(const orc_view* views, int n, int nu, int nv, float range,
     const orc_volume* vol, const orc_filter* filter, const float* proj,
     double* volume_out, int flags)
 {
+    return orc_fdk_weighted(views, n, nu, nv, range, vol, filter, proj, nullptr, volume_out, flags);
+}
+
+int orc_fdk_weighted(const orc_view* views, int n, int nu, int nv, float range,
+    const orc_volume* vol, const orc_filter* filter, const float* proj,
+    const double* row_weights, double* volume_out, int flags)
+{
     if (!valid_volume(vol)) return -1;
     std::vector<double> flt(static_cast<size_t>(n) * nu * nv);
-    int rc = orc_fdk_filter(views, n, nu, nv, range, filter, proj, flt.data());
+    int rc = orc_fdk_filter_weighted(views, n, nu, nv, range, filter, proj, row_weights, flt.data());
     if (rc) return rc;
     std::fill(volume_out, volume_out + static_cast<size_t>(vol->nx) * vol->ny * vol->nz, 0.0);
     return orc_fdk_backproject(views, n, nu, nv, range, vol, flt.data(), volume_out, flags);

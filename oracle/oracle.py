@@ -69,6 +69,11 @@ def lib():
             "orc_fdk_filter": [P, C.c_int, C.c_int, C.c_int, C.c_float, C.POINTER(Filter), P, P],
             "orc_fdk_backproject": [P, C.c_int, C.c_int, C.c_int, C.c_float, C.POINTER(Volume), P, P, C.c_int],
             "orc_fdk": [P, C.c_int, C.c_int, C.c_int, C.c_float, C.POINTER(Volume), C.POINTER(Filter), P, P, C.c_int],
+            "orc_fdk_weighted": [P, C.c_int, C.c_int, C.c_int, C.c_float, C.POINTER(Volume),
+                                 C.POINTER(Filter), P, P, P, C.c_int],
+            "orc_fdk_filter_weighted": [P, C.c_int, C.c_int, C.c_int, C.c_float, C.POINTER(Filter),
+                                        P, P, P],
+            "orc_parker_weights": [P, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int, P],
             "orc_fdk_fp32": [P, C.c_int, C.c_int, C.c_int, C.c_float, C.POINTER(Volume), C.POINTER(Filter), P, P],
             "orc_fdk_derived": [P, C.c_int, C.c_int, C.c_int, C.c_float, P],
             "orc_ramp_kernel": [C.c_int, C.c_double, C.POINTER(Filter), P],
@@ -160,6 +165,36 @@ def fdk(views, nu, nv, scan_range, vol: Volume, filt: Filter, proj, flags=0) -> 
     out = np.zeros((vol.nz, vol.ny, vol.nx), dtype=np.float64)
     _check(lib().orc_fdk(_ptr(views), len(views), nu, nv, scan_range, C.byref(vol),
                          C.byref(filt), _ptr(proj), _ptr(out), flags), "fdk")
+    return out
+
+
+def parker_weights(views, nu, nv, scan_range, start_angle_rad=0.0, direction=1) -> np.ndarray:
+    """Parker short-scan weights [n_views][nu] (FP64, range/pi scale included);
+    raises when the scan does not qualify (full turn or coverage < pi + 2 fan)."""
+    out = np.zeros((len(views), nu), dtype=np.float64)
+    _check(lib().orc_parker_weights(_ptr(views), len(views), nu, nv, scan_range,
+                                    start_angle_rad, direction, _ptr(out)), "parker_weights")
+    return out
+
+
+def fdk_weighted(views, nu, nv, scan_range, vol: Volume, filt: Filter, proj, row_weights,
+                 flags=0) -> np.ndarray:
+    proj = np.ascontiguousarray(proj, dtype=np.float32)
+    w = None if row_weights is None else np.ascontiguousarray(row_weights, dtype=np.float64)
+    out = np.zeros((vol.nz, vol.ny, vol.nx), dtype=np.float64)
+    _check(lib().orc_fdk_weighted(_ptr(views), len(views), nu, nv, scan_range, C.byref(vol),
+                                  C.byref(filt), _ptr(proj), _ptr(w) if w is not None else None,
+                                  _ptr(out), flags), "fdk_weighted")
+    return out
+
+
+def fdk_filter_weighted(views, nu, nv, scan_range, filt: Filter, proj, row_weights) -> np.ndarray:
+    proj = np.ascontiguousarray(proj, dtype=np.float32)
+    w = np.ascontiguousarray(row_weights, dtype=np.float64)
+    out = np.zeros(proj.shape, dtype=np.float64)
+    _check(lib().orc_fdk_filter_weighted(_ptr(views), len(views), nu, nv, scan_range,
+                                         C.byref(filt), _ptr(proj), _ptr(w), _ptr(out)),
+           "fdk_filter_weighted")
     return out
 
 

@@ -256,3 +256,65 @@ def test_fdk_execute_host_matches_device(oracle, cuda_device, pinned, precision)
     torch.cuda.current_stream().synchronize()
     assert K.rel_rmse(vol.cpu().numpy(), dev) < 1e-6
     plan.close()
+
+
+def _short_scan_case(start=0.3, direction=-1):
+    from fdk_cuda_impl_b200.geometry import CircularScan
+    case = K.c1_small()
+    # 40 views of a 60-view turn: 240 degrees >= 180 + 2 x 4.4 degrees of fan
+    case.scan = CircularScan(40, 60, 500.0, 1000.0, 96, 64, 1.6, 1.6, start_angle_rad=start,
+                             rotation_direction=direction)
+    return case
+
+
+@pytest.mark.parametrize("precision,tol", [("fp32", FP32_TOL), ("bf16", BF16_TOL)])
+@pytest.mark.parametrize("direction", [1, -1])
+def test_fdk_parker_short_scan(oracle, cuda_device, precision, tol, direction):
+    # short-scan FDK with Parker weights (Auto on a 240-degree scan) against
+    # the oracle's restatement of the reference weights
+    import torch
+    from fdk_cuda_impl_b200.projectors import FdkPlan
+    case = _short_scan_case(direction=direction)
+    sc = case.scan
+    views = sc.views()
+    p = K.projections(oracle, case, views)
+    plan = FdkPlan(views, 96, 64, sc.scan_range, case.grid, case.filt, precision, parker="auto",
+                   start_angle_rad=sc.start_angle_rad, rotation_direction=direction)
+    out = plan.execute(torch.from_numpy(p).cuda()).cpu().numpy()
+    plan.check()
+    w = oracle.parker_weights(views, 96, 64, sc.scan_range, sc.start_angle_rad, direction)
+    ref = oracle.fdk_weighted(views, 96, 64, sc.scan_range, K.oracle_volume(oracle, case.grid),
+                              K.oracle_filter(oracle, case.filt), p, w)
+    assert K.rel_rmse(out, ref) <= tol
+    plan.close()
+
+
+def test_fdk_parker_modes(oracle, cuda_device):
+    import torch
+    from fdk_cuda_impl_b200 import _lib as L
+    from fdk_cuda_impl_b200.projectors import FdkPlan
+    case = _short_scan_case()
+    sc = case.scan
+    views = sc.views()
+    p = K.projections(oracle, case, views)
+    # Disabled: plain FDK of the short scan
+    plan = FdkPlan(views, 96, 64, sc.scan_range, case.grid, case.filt, parker="disabled",
+                   start_angle_rad=sc.start_angle_rad, rotation_direction=-1)
+    out = plan.execute(torch.from_numpy(p).cuda()).cpu().numpy()
+    ref = oracle.fdk(views, 96, 64, sc.scan_range, K.oracle_volume(oracle, case.grid),
+                     K.oracle_filter(oracle, case.filt), p)
+    assert K.rel_rmse(out, ref) <= FP32_TOL
+    plan.close()
+    # Enabled on a full turn, or on a scan shorter than pi + 2 fan: invalid geometry
+    full = K.c1_small()
+    with pytest.raises(L.YkbError) as e:
+        FdkPlan(full.scan.views(), 96, 64, full.scan.scan_range, full.grid, parker="enabled")
+    assert e.value.code == L.ERR_INVALID_GEOMETRY
+    from fdk_cuda_impl_b200.geometry import CircularScan
+    half = CircularScan(30, 60, 500.0, 1000.0, 96, 64, 1.6, 1.6)
+    with pytest.raises(L.YkbError) as e:
+        FdkPlan(half.views(), 96, 64, half.scan_range, full.grid, parker="auto")
+    assert e.value.code == L.ERR_INVALID_GEOMETRY
+    # Auto on a full turn: no weights
+    plan = FdkPlan(full.scan.views(), 96, 64, full.scan.scan_range, full.grid, parker="auto")
+    plan.close()

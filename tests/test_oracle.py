@@ -194,3 +194,63 @@ def test_mt19937_stream_matches_reference_generator(oracle):
     assert x.min() >= -1 and x.max() < 1
     assert abs(x.mean()) < 0.1
     assert not np.array_equal(x, oracle.mt19937_uniform_pm1(1000, 54321))
+
+
+# ---------------------------------------------------------------- Parker ---
+
+def _short_case(total=40, per_turn=60):
+    from fdk_cuda_impl_b200.geometry import CircularScan
+    case = K.c1_small()
+    case.scan = CircularScan(total, per_turn, 500.0, 1000.0, 96, 64, 1.6, 1.6)
+    return case
+
+
+def test_parker_conjugate_rays_sum_to_one(oracle):
+    # w(beta, gamma) + w(beta + pi + 2 gamma, -gamma) = 1 (before the range/pi
+    # scale): on the central column (gamma = 0, odd detector, no offsets) of a
+    # scan sampled every 0.9 degrees the conjugate of view i is view i + 200
+    # (YkFDKParkerKernels.cu:46-110; the Parker 1982 condition)
+    from fdk_cuda_impl_b200.geometry import CircularScan
+    sc = CircularScan(260, 400, 500.0, 1000.0, 97, 8, 1.6, 1.6)
+    views = sc.views()
+    w = oracle.parker_weights(views, 97, 8, sc.scan_range)
+    scale = sc.scan_range / np.pi
+    c = w[:, 48] / scale
+    assert np.all((w >= 0) & (w <= scale + 1e-12))
+    pairs = c[:60] + c[200:260]
+    # the view angles are floats (ulp 5e-7 rad at 4 rad)
+    assert np.max(np.abs(pairs - 1.0)) < 1e-5
+    assert c[0] == 0.0 and np.all(c[80:120] == 1.0)
+
+
+def test_parker_needs_a_qualifying_short_scan(oracle):
+    from fdk_cuda_impl_b200.geometry import CircularScan
+    full = CircularScan(60, 60, 500.0, 1000.0, 96, 64, 1.6, 1.6)
+    with pytest.raises(RuntimeError):
+        oracle.parker_weights(full.views(), 96, 64, full.scan_range)
+    # 180 degrees do not cover pi + 2 x fan angle (fan half-angle 4.4 degrees)
+    short = CircularScan(30, 60, 500.0, 1000.0, 96, 64, 1.6, 1.6)
+    with pytest.raises(RuntimeError):
+        oracle.parker_weights(short.views(), 96, 64, short.scan_range)
+
+
+def test_short_scan_fdk_matches_full_scan(oracle):
+    # Parker-weighted short scan (240 of 360 degrees) reconstructs the same
+    # object as the full scan: the weights and the range/pi x 2pi/range
+    # normalisation pin the short-scan path
+    full = K.c1_small()
+    short = _short_case()
+    ph = K.phantom(oracle, full)
+    vol = K.oracle_volume(oracle, full.grid)
+    filt = K.oracle_filter(oracle, full.filt)
+    pf = K.projections(oracle, full, ph=ph)
+    ref = oracle.fdk(full.scan.views(), 96, 64, full.scan.scan_range, vol, filt, pf)
+    sv = short.scan.views()
+    ps = K.projections(oracle, short, ph=ph)
+    w = oracle.parker_weights(sv, 96, 64, short.scan.scan_range)
+    rec = oracle.fdk_weighted(sv, 96, 64, short.scan.scan_range, vol, filt, ps, w)
+    assert K.cosine(rec, ref) > 0.99
+    assert K.rel_rmse(rec, ref) < 0.15
+    # without the weights the short scan is visibly wrong
+    plain = oracle.fdk(sv, 96, 64, short.scan.scan_range, vol, filt, ps)
+    assert K.rel_rmse(plain, ref) > 2 * K.rel_rmse(rec, ref)

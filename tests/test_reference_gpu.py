@@ -212,3 +212,45 @@ def test_reference_joseph_bp(oracle, cuda_device, name, data):
         eb = K.rel_rmse(b, r)
         print(f"{name}/{data}: ykb BP vs ref {eb:.3e}")
         assert eb <= (2e-5 if data == "constant" else 2e-4), eb
+
+
+def _short_scan(name):
+    from fdk_cuda_impl_b200.geometry import CircularScan
+    case = CASES[name]()
+    sc = case.scan
+    # two thirds of a turn: 240 degrees cover pi + 2 x fan angle in both cases
+    case.scan = CircularScan(sc.total_views * 2 // 3, sc.views_per_turn, sc.sid_mm, sc.sdd_mm,
+                             sc.channels, sc.rows, sc.channel_size_mm, sc.row_size_mm,
+                             sc.start_angle_rad, sc.rotation_direction, sc.z_mm,
+                             sc.source_offset_mm, sc.offset_unv_mm, sc.tilt_rad)
+    return case
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_reference_fdk_parker(oracle, cuda_device, name):
+    """Short scan (Parker Auto) through the reference FdkPipeline vs the
+    oracle's restatement of its Parker weights: smooth projections with the
+    None filter pin the weights and normalisation; the phantom case bounds
+    the texture-weight noise as for full scans."""
+    case = _short_scan(name)
+    sc = case.scan
+    views = sc.views()
+    w = oracle.parker_weights(views, sc.channels, sc.rows, sc.scan_range, sc.start_angle_rad,
+                              sc.rotation_direction)
+    vol = K.oracle_volume(oracle, case.grid)
+    none = RampFilter(type=0)
+    sm = _smooth_proj(sc)
+    r = ref.fdk(sc, case.grid, none, sm)
+    o = oracle.fdk_weighted(views, sc.channels, sc.rows, sc.scan_range, vol,
+                            K.oracle_filter(oracle, none), sm, w)
+    e_smooth = K.rel_rmse(r, o)
+    proj = K.projections(oracle, case)
+    r2 = ref.fdk(sc, case.grid, case.filt, proj)
+    o2 = oracle.fdk_weighted(views, sc.channels, sc.rows, sc.scan_range, vol,
+                             K.oracle_filter(oracle, case.filt), proj, w, flags=1)
+    e_tex = K.rel_rmse(r2, o2)
+    print(f"{name}: Parker smooth ref vs oracle {e_smooth:.3e}, phantom ref vs oracle(texture) {e_tex:.3e}")
+    # the reference evaluates the fan angles and ramps in FP32 (atan2f, sinf)
+    # on top of its FP32 geometry: 1e-5 (centred) to 5e-5 (tilted/offset)
+    assert e_smooth <= 1e-4, e_smooth
+    assert e_tex <= 5e-4, e_tex
