@@ -32,6 +32,10 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+# the headline metric: FDK GUPS is `value`; the FP+BP gradient step of the
+# differentiable Joseph pair is reported beside it ("joseph")
+METRIC = "FDK backprojection GUPS (voxel\u00d7view/s) & FP+BP grad step ms at stated RMSE"
+
 # the workload the metric is quoted on, and a small case of the same kernels
 # (inputs still larger than L2) used for profiler captures
 CONFIGS = {
@@ -67,6 +71,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-bf16", action="store_true")
+    ap.add_argument("--no-joseph", action="store_true")
     ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
     return ap.parse_args()
 
@@ -160,6 +165,55 @@ def cpu_baseline(n_views_sample=96, z_slab=64):
                       f"backprojected into a 512x512x{z_slab} slab, FP64, {dt:.1f} s"}
 
 
+# Differentiable Joseph pair (the metric's "FP+BP grad step"): 256^3 of
+# 0.5 mm voxels, 360 views of a 384x384 detector of 0.8 mm at 500/1000 mm
+J_VOX, J_VIEWS, J_DET, J_VOX_MM, J_PIX_MM = 256, 360, 384, 0.5, 0.8
+
+
+def joseph_workload():
+    from fdk_cuda_impl_b200 import CircularScan, VolumeGrid
+    scan = CircularScan(J_VIEWS, J_VIEWS, SID, SDD, J_DET, J_DET, J_PIX_MM, J_PIX_MM)
+    return scan, VolumeGrid.cube(J_VOX, J_VOX_MM)
+
+
+def joseph_step(local: int, steps: int, warmup: int, timed_fn):
+    """One gradient step of 1/2 |A x - b|^2 through the autograd Joseph pair:
+    y = A x (forward projector), then x.grad = A^T (y - b) (matched
+    backprojector); plus the dot-product adjoint test <Ax, y> = <x, A^T y>."""
+    import torch
+    from fdk_cuda_impl_b200.autograd import JosephProjector
+    from fdk_cuda_impl_b200.projectors import JosephPlan
+    scan, grid = joseph_workload()
+    plan = JosephPlan(scan.views(), J_DET, J_DET, grid, device=local)
+    op = JosephProjector(plan)
+    gen = torch.Generator(device=f"cuda:{local}")
+    gen.manual_seed(11)
+    x = torch.rand(grid.shape, device=f"cuda:{local}", generator=gen).requires_grad_(True)
+    b = torch.randn(plan.proj_shape, device=f"cuda:{local}", generator=gen)
+
+    def step():
+        x.grad = None
+        r = op(x) - b
+        r.backward(r)  # d(1/2 |r|^2)/dr = r
+
+    for _ in range(warmup):
+        step()
+    ms = timed_fn(step, steps)
+    fp_ms = timed_fn(lambda: plan.forward(x.detach()), steps)
+    bp_ms = timed_fn(lambda: plan.adjoint(b), steps)
+    with torch.no_grad():
+        ax = plan.forward(x.detach())
+        aty = plan.adjoint(b)
+        lhs = (ax.double() * b.double()).sum().item()
+        rhs = (x.detach().double() * aty.double()).sum().item()
+    samples = J_VIEWS * J_DET * J_DET * J_VOX  # rays x main-axis steps
+    plan.close()
+    return {"workload": f"joseph-{J_VOX}^3-{J_VIEWS}v-{J_DET}^2", "grad_step_ms": ms,
+            "fp_ms": fp_ms, "bp_ms": bp_ms, "adjoint_rel": abs(lhs - rhs) / abs(lhs),
+            "samples_per_op": samples, "fp_gsamples": samples / (fp_ms * 1e-3) / 1e9,
+            "bp_gsamples": samples / (bp_ms * 1e-3) / 1e9}
+
+
 def make_workload(rank: int, local: int):
     """The benchmark's seeded inputs on cuda:local: ellipsoid phantom (one
     independent object per rank), Joseph forward projection, Poisson noise."""
@@ -195,11 +249,12 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    import numpy as np
     from oracle import ref as R
     cfg = {"workload": WORKLOAD, "volume": [N_VOX] * 3, "voxel_mm": VOX_MM, "views": N_VIEWS,
            "detector": [N_DET, N_DET], "pixel_mm": PIX_MM, "sid_sdd_mm": [SID, SDD],
            "ellipsoids": N_ELL, "noise_i0": I0, "filter": "ramlak"}
-    line = {"metric": "FDK backprojection GUPS (voxel x view updates/s)", "unit": "GUPS",
+    line = {"metric": METRIC, "unit": "GUPS",
             "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "data": "synthetic", "impl": "reference"}
     import torch
@@ -213,6 +268,19 @@ def run_reference(args):
                                      reps=args.steps, timeout=1800)
         value = UPDATES / (ms_dev * 1e-3) / 1e9
         cb = cpu_baseline(n_views_sample=24, z_slab=32)
+        # the reference's FP_Joseph / BP_Joseph operators on the same Joseph
+        # workload (each call re-uploads its texture, as its stock apply does)
+        jscan, jgrid = joseph_workload()
+        gen = np.random.default_rng(11)
+        jx = gen.random(jgrid.shape, dtype=np.float32)
+        jy = gen.standard_normal((J_VIEWS, J_DET, J_DET)).astype(np.float32)
+        _, fp_ms = R.joseph_fp(jscan, jgrid, jx, warmup=args.warmup, reps=args.steps)
+        _, bp_ms = R.joseph_bp(jscan, jgrid, jy, warmup=args.warmup, reps=args.steps)
+        samples = J_VIEWS * J_DET * J_DET * J_VOX
+        joseph = {"workload": f"joseph-{J_VOX}^3-{J_VIEWS}v-{J_DET}^2", "fp_ms": fp_ms,
+                  "bp_ms": bp_ms, "grad_step_ms": fp_ms + bp_ms,
+                  "fp_gsamples": samples / (fp_ms * 1e-3) / 1e9,
+                  "bp_gsamples": samples / (bp_ms * 1e-3) / 1e9}
         line.update({
             "value": value, "ms_per_step": ms_dev, "dtype": "f32",
             "config": dict(cfg, implementation="reference CUDA build (YKCBCT FdkPipeline, "
@@ -222,6 +290,7 @@ def run_reference(args):
                     "ms_per_step": ms_host, "h2d_bytes_per_step": int(h_proj.nbytes),
                     "d2h_bytes_per_step": int(4 * N_VOX ** 3)},
             "cpu_baseline": cb,
+            "joseph": joseph,
             "gpu_launches": None,
         })
     else:
@@ -363,14 +432,22 @@ def main():
         plan_b.close()
         del ref_vol, vb, d_in_b, h_proj_b
 
+    joseph = joseph_step(local, args.steps, args.warmup, timed) if not args.no_joseph else None
+
     peaks, peak_src = measured_peaks()
     # HBM roofline of the dominant kernel (backprojection): compulsory bytes
     # per launch = filtered projections read once + volume written once.
     bp_bytes = 4.0 * N_VIEWS * N_DET * N_DET + 4.0 * N_VOX ** 3
     achieved = bp_bytes / (ms_bp * 1e-3) / 1e9
+    # DRAM traffic of one launch: ncu (dram__bytes_read + write) on the
+    # 256^3 x 360 x 384^2 case gave 830.8 MB against 279.4 MB compulsory
+    # (tap-pair rows are 8 B per sample; L2 misses re-read some rows);
+    # scaled by the compulsory bytes, which grow in proportion
+    traffic = 830.8e6 * bp_bytes / (4.0 * 360 * 384 * 384 + 4.0 * 256 ** 3)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                "frac": achieved / peaks["hbm_gbs"], "traffic": None, "peak_source": peak_src,
-                "kernel": "fdk_bp_kernel", "kernel_ms": ms_bp,
+                "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "peak_source": peak_src,
+                "traffic_source": "ncu 256^3x360x384^2 capture scaled by compulsory bytes",
+                "kernel": "fdk_bp_tma_kernel<52,1,1> (TMA-staged tap pairs)", "kernel_ms": ms_bp,
                 "algorithmic_bytes_per_launch": bp_bytes}
     # on-chip view of the same kernel: 16 B of bilinear taps per update
     sm_mhz = clock_info.get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
@@ -381,7 +458,7 @@ def main():
               "bp_gups": UPDATES / (ms_bp * 1e-3) / 1e9}
 
     line = {
-        "metric": "FDK backprojection GUPS (voxel x view updates/s)",
+        "metric": METRIC,
         "value": value, "unit": "GUPS", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -398,6 +475,7 @@ def main():
                 "h2d_bytes_per_step": int(h_proj.numel() * 4),
                 "d2h_bytes_per_step": int(h_vol.numel() * 4)},
         "bf16": bf16,
+        "joseph": joseph,
         "gpu_launches": 3 * args.steps,
         "clocks": clock_info,
     }
