@@ -166,17 +166,43 @@ __global__ void transpose_xzy_kernel(const float* __restrict__ in, int nx, int n
 // ---------------------------------------------------------------------------
 struct ViewProj { float m[12]; };  // (u*w, v*w, w) = M (x', y', z', 1)
 
-__global__ void __launch_bounds__(256) joseph_bp_kernel(const float* __restrict__ proj,
-    const float4* __restrict__ rays, const float* __restrict__ lens,
-    const ViewProj* __restrict__ vp, const JosephView* __restrict__ views, int n_views,
-    int nu, int nv, int nx, int ny, int nz, float* __restrict__ vol, int accumulate)
+// Ray values weighted by their chord length: the backprojector gathers
+// value * len * (bilinear weight) per ray, and this pass forms value * len
+// once per ray instead of once per (voxel, ray) hit.
+__global__ void joseph_weight_rays_kernel(const float* __restrict__ proj,
+    const float* __restrict__ lens, long n, float* __restrict__ out)
+{
+    for (long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long>(gridDim.x) * blockDim.x)
+        out[i] = proj[i] * lens[i];
+}
+
+// Weight with which a sample at minor coordinate f reaches voxel j:
+// 1 - w when floor(f) = j, w when floor(f) = j - 1, with w = f - floor(f).
+// Both cases take w with the forward projector's own subtraction f - floor(f)
+// (jf = j, jm = j - 1 as floats), so the weights are bit-identical to
+// joseph_fp_kernel's without a float-to-int conversion.  f - (j - 1) is exact
+// except for j = 0 (f just below 0), where it may round up to 1 -- as the
+// forward projector's w does, which then gives voxel 0 the full weight 1:
+// hence e <= 1 (e = 1 with floor(f) = j is caught by the first case).
+__device__ __forceinline__ float hat_weight(float f, float jf, float jm)
+{
+    const float d = f - jf;   // floor(f) = j      <=> 0 <= d < 1
+    const float e = f - jm;   // floor(f) = j - 1  <=> 0 <= e <= 1
+    return (d >= 0.f && d < 1.f) ? 1.f - d : ((e >= 0.f && e <= 1.f) ? e : 0.f);
+}
+
+__global__ void __launch_bounds__(256) joseph_bp_kernel(const float* __restrict__ vl,
+    const float4* __restrict__ rays, const ViewProj* __restrict__ vp,
+    const JosephView* __restrict__ views, int n_views, int nu, int nv, int nx, int ny, int nz,
+    float* __restrict__ vol, int accumulate)
 {
     const int x = blockIdx.x * 32 + threadIdx.x;
     const int y = blockIdx.y * 8 + threadIdx.y;
     const int z = blockIdx.z;
     if (x >= nx || y >= ny) return;
     const long view_elems = static_cast<long>(nu) * nv;
-    double acc = 0.0;  // FP64 voxel sum (see joseph_fp_kernel)
+    double acc = 0.0;  // FP64 over views; each view's few hits summed in FP32
     for (int k = 0; k < n_views; ++k) {
         const JosephView& j = views[k];
         int s, j1, j2;
@@ -184,7 +210,7 @@ __global__ void __launch_bounds__(256) joseph_bp_kernel(const float* __restrict_
         else if (j.axis == 1) { s = y; j1 = x; j2 = z; }
         else { s = z; j1 = x; j2 = y; }
         const float c0 = static_cast<float>(s) - 0.5f * (j.n0 - 1);
-        // detector bounding box of the slice square
+        // detector bounding box of the slice square [j1-1,j1+1]x[j2-1,j2+1]
         const ViewProj& m = vp[k];
         float umin = 1e30f, umax = -1e30f, vmin = 1e30f, vmax = -1e30f;
 #pragma unroll
@@ -197,7 +223,8 @@ __global__ void __launch_bounds__(256) joseph_bp_kernel(const float* __restrict_
             else if (j.axis == 1) { px = q1; py = c0; pz = q2; }
             else { px = q1; py = q2; pz = c0; }
             const float w = fmaf(m.m[8], px, fmaf(m.m[9], py, fmaf(m.m[10], pz, m.m[11])));
-            const float rw = 1.f / w;
+            // the box only needs a few 1e-6 px: correctly rounded reciprocal
+            const float rw = __frcp_rn(w);
             const float u = fmaf(m.m[0], px, fmaf(m.m[1], py, fmaf(m.m[2], pz, m.m[3]))) * rw;
             const float v = fmaf(m.m[4], px, fmaf(m.m[5], py, fmaf(m.m[6], pz, m.m[7]))) * rw;
             umin = fminf(umin, u); umax = fmaxf(umax, u);
@@ -208,22 +235,20 @@ __global__ void __launch_bounds__(256) joseph_bp_kernel(const float* __restrict_
         const int u1 = min(nu - 1, static_cast<int>(floorf(umax + margin)));
         const int v0 = max(0, static_cast<int>(ceilf(vmin - margin)));
         const int v1 = min(nv - 1, static_cast<int>(floorf(vmax + margin)));
+        const float j1f = static_cast<float>(j1), j1m = static_cast<float>(j1 - 1);
+        const float j2f = static_cast<float>(j2), j2m = static_cast<float>(j2 - 1);
         const long base = k * view_elems;
+        float accv = 0.f;
         for (int iv = v0; iv <= v1; ++iv) {
+            const long row = base + static_cast<long>(iv) * nu;
             for (int iu = u0; iu <= u1; ++iu) {
-                const long idx = base + static_cast<long>(iv) * nu + iu;
-                const float4 r = __ldg(rays + idx);
-                const float f1 = fmaf(r.x, c0, r.y);
-                const float f2 = fmaf(r.z, c0, r.w);
-                const float fl1 = floorf(f1), fl2 = floorf(f2);
-                const int i1 = static_cast<int>(fl1), i2 = static_cast<int>(fl2);
-                const float w1 = f1 - fl1, w2 = f2 - fl2;
-                const float wa = (i1 == j1) ? 1.f - w1 : ((i1 + 1 == j1) ? w1 : 0.f);
-                const float wb = (i2 == j2) ? 1.f - w2 : ((i2 + 1 == j2) ? w2 : 0.f);
-                const float w = wa * wb;
-                if (w != 0.f) acc += static_cast<double>(__ldg(proj + idx) * __ldg(lens + idx) * w);
+                const float4 r = __ldg(rays + row + iu);
+                const float w = hat_weight(fmaf(r.x, c0, r.y), j1f, j1m) *
+                    hat_weight(fmaf(r.z, c0, r.w), j2f, j2m);
+                if (w != 0.f) accv = fmaf(__ldg(vl + row + iu), w, accv);
             }
         }
+        acc += static_cast<double>(accv);
     }
     float* dst = vol + (static_cast<long>(z) * ny + y) * nx + x;
     *dst = accumulate ? static_cast<float>(*dst + acc) : static_cast<float>(acc);
@@ -289,10 +314,14 @@ cudaError_t launch_joseph_ray_table(const JosephView* views, int n_views, int nu
 
 cudaError_t launch_joseph_bp(const float* proj, const float4* rays, const float* lens,
     const float* view_proj, const JosephView* views, int n_views, int nu, int nv,
-    const ykb_volume& vol, float* out, int accumulate, cudaStream_t s)
+    const ykb_volume& vol, float* weighted, float* out, int accumulate, cudaStream_t s)
 {
+    const long n = static_cast<long>(n_views) * nu * nv;
+    joseph_weight_rays_kernel<<<148 * 8, 256, 0, s>>>(proj, lens, n, weighted);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
     const dim3 grid((vol.nx + 31) / 32, (vol.ny + 7) / 8, vol.nz);
-    joseph_bp_kernel<<<grid, dim3(32, 8), 0, s>>>(proj, rays, lens,
+    joseph_bp_kernel<<<grid, dim3(32, 8), 0, s>>>(weighted, rays,
         reinterpret_cast<const ViewProj*>(view_proj), views, n_views, nu, nv, vol.nx, vol.ny,
         vol.nz, out, accumulate);
     return cudaGetLastError();

@@ -552,6 +552,7 @@ YKB_API ykb_status ykb_joseph_plan_create(const ykb_cone_view* views, int n_view
         (e = p->view_proj.alloc(sizeof(float) * vp.size())) != cudaSuccess ||
         (e = p->rays.alloc(sizeof(float4) * rays)) != cudaSuccess ||
         (e = p->lens.alloc(sizeof(float) * rays)) != cudaSuccess ||
+        (e = p->weighted.alloc(sizeof(float) * rays)) != cudaSuccess ||
         (need_y && (e = p->slab_y.alloc(vol_bytes)) != cudaSuccess) ||
         (need_x && (e = p->slab_x.alloc(vol_bytes)) != cudaSuccess)) {
         delete p;
@@ -595,7 +596,7 @@ YKB_API size_t ykb_joseph_workspace_bytes(const ykb_joseph_plan* p)
 {
     if (!p) return 0;
     return p->views.bytes + p->view_proj.bytes + p->rays.bytes + p->lens.bytes +
-        p->slab_x.bytes + p->slab_y.bytes;
+        p->weighted.bytes + p->slab_x.bytes + p->slab_y.bytes;
 }
 
 YKB_API ykb_status ykb_joseph_fp(ykb_joseph_plan* p, const float* d_volume, float* d_proj,
@@ -625,7 +626,7 @@ YKB_API ykb_status ykb_joseph_bp(ykb_joseph_plan* p, const float* d_proj, float*
     const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     YKB_TRY_CUDA(launch_joseph_bp(d_proj, p->rays.as<float4>(), p->lens.as<float>(),
         p->view_proj.as<float>(), p->views.as<JosephView>(), p->n_views, p->nu, p->nv, p->volume,
-        d_volume, accumulate ? 1 : 0, s));
+        p->weighted.as<float>(), d_volume, accumulate ? 1 : 0, s));
     return YKB_OK;
 }
 

@@ -205,10 +205,9 @@ cudaError_t launch_joseph_fp(const float* slabs[3], const JosephView* views,
     int accumulate, cudaStream_t s);
 cudaError_t launch_joseph_ray_table(const JosephView* views, int n_views,
     int nu, int nv, float4* rays, float* lens, cudaStream_t s);
-cudaError_t launch_joseph_bp(const float* proj, const float4* rays,
-    const float* lens, const float* view_proj, const JosephView* views,
-    int n_views, int nu, int nv, const ykb_volume& vol, float* out,
-    int accumulate, cudaStream_t s);
+cudaError_t launch_joseph_bp(const float* proj, const float4* rays, const float* lens,
+    const float* view_proj, const JosephView* views, int n_views, int nu, int nv,
+    const ykb_volume& vol, float* weighted, float* out, int accumulate, cudaStream_t s);
 
 } // namespace ykb
 
@@ -261,5 +260,6 @@ struct ykb_joseph_plan {
     ykb::DeviceBuffer view_proj; // float[n][12]: voxel-space 3x4 projection
     ykb::DeviceBuffer rays;      // float4[n*nv*nu]: (a1, e1, a2, e2)
     ykb::DeviceBuffer lens;      // float[n*nv*nu]: chord length per step
+    ykb::DeviceBuffer weighted;  // float[n*nv*nu]: backprojector input x chord length
     ykb::DeviceBuffer slab_y, slab_x;  // transposed volume copies
 };
