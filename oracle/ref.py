@@ -25,7 +25,7 @@ def _load():
     lib = C.CDLL(LIB)
     lib.ykref_last_error.restype = C.c_char_p
     for name in ("ykref_fdk", "ykref_fdk_stages", "ykref_fdk_time", "ykref_joseph_fp",
-                 "ykref_joseph_bp"):
+                 "ykref_joseph_bp", "ykref_cgls"):
         getattr(lib, name).restype = C.c_int
     return lib
 
@@ -62,6 +62,14 @@ def _child(op, scan_kw, grid_kw, filt_kw, paths, opts, q):
             rc = lib.ykref_fdk_stages(C.byref(s), C.byref(v), C.byref(f), _fp(proj), _fp(out),
                                       _fp(pw), _fp(fl), C.byref(first), C.byref(count), dev)
             res = (out, pw[:count.value], fl[:count.value], first.value)
+        elif op == "cgls":
+            proj = np.ascontiguousarray(arrays[0], dtype=np.float32)
+            out = np.zeros(grid.shape, dtype=np.float32)
+            ms = C.c_float(0.0)
+            rc = lib.ykref_cgls(C.byref(s), C.byref(v), _fp(proj), _fp(out),
+                                C.c_int(opts["n_iter"]), C.c_int(opts.get("matched", 1)),
+                                C.byref(ms), dev)
+            res = (out, ms.value)
         elif op == "fdk_time":
             f = RampFilter(**filt_kw).struct()
             proj = np.ascontiguousarray(arrays[0], dtype=np.float32)
@@ -129,6 +137,13 @@ def fdk_stages(scan, grid, filt, proj):
 def fdk_time(scan, grid, filt, proj, warmup=2, reps=5, timeout=900):
     """(device-resident ms, host-input ms) per full FDK sequence."""
     return _run("fdk_time", scan, grid, filt, [proj], warmup=warmup, reps=reps, timeout=timeout)
+
+
+def cgls(scan, grid, proj, n_iter, matched=True, timeout=900):
+    """Reference CglsAstraBackend from a zero volume with FP_Joseph and
+    BP_Joseph (matched) or BP_FDK_PseudoMatched: (volume, run() ms)."""
+    return _run("cgls", scan, grid, None, [proj], n_iter=n_iter, matched=int(matched),
+                timeout=timeout)
 
 
 def joseph_fp(scan, grid, volume, warmup=0, reps=0):

@@ -31,7 +31,8 @@ ROOT = os.path.dirname(HERE)
 OUT = os.path.join(HERE, "_ref")
 DEFAULT_REFERENCE = "/root/reference"
 
-# translation units of the FDK pipeline and the flat FP/BP operators
+# translation units of the FDK pipeline, the flat FP/BP operators and the
+# iterative vector kernels their CGLS uses
 SOURCES = [
     "src/Reconstruction/Analytic/Circular/Flat/FDK/kernels/YkFDKBpKernels.cu",
     "src/Reconstruction/Analytic/Circular/Flat/FDK/kernels/YkFDKBpPrecompute.cu",
@@ -46,6 +47,7 @@ SOURCES = [
     "src/FlatFpBp/BP/kernels/YkBpFdkKernel.cu",
     "src/FlatFpBp/BP/kernels/YkBPJosephKernel.cu",
     "src/FlatFpBp/BP/kernels/YkBPSiddonKernel.cu",
+    "src/Reconstruction/Iterative/Common/kernels/YkIterKernels.cu",
     "src/global/YkLog.cpp",
 ]
 

@@ -29,6 +29,7 @@
 #include <vector>
 
 #include "Reconstruction/Analytic/Circular/Flat/FDK/YkFdkPipeline.hpp"
+#include "Reconstruction/Iterative/Flat/YkCglsBackends.hpp"
 #include "common/YkExecutionContext.hpp"
 #include "common/YkOperatorTypes.hpp"
 #include "common/YkProjectionOperators.hpp"
@@ -301,6 +302,51 @@ int joseph(int mode, const ykb_circular_flat* scan, const ykb_volume* volume, co
 }
 
 } // namespace
+
+// The reference's CGLS (CglsAstraBackend, src/Reconstruction/Iterative/Flat/
+// YkCglsBackends.hpp:22-196) for n_iter iterations from a zero volume, with
+// FP_Joseph and, per `matched`, BP_Joseph (1) or its default
+// BP_FDK_PseudoMatched (0).  ms (optional) receives the device time of run().
+__attribute__((visibility("default"))) int ykref_cgls(const ykb_circular_flat* scan,
+    const ykb_volume* volume, const float* h_proj, float* h_vol, int n_iter, int matched,
+    float* ms, int device)
+{
+    if (!scan || !volume || !h_proj || !h_vol || n_iter <= 0) return fail("bad argument");
+    if (cudaSetDevice(device) != cudaSuccess) return fail("cudaSetDevice");
+    const YK::SSystemConfig sys = make_system(*scan, *volume);
+    YK::PreparedGeometry geometry;
+    if (!geometry.initialize(sys)) return fail("PreparedGeometry::initialize");
+    Stream stream;
+    const size_t nvox = size_t(volume->nx) * volume->ny * volume->nz;
+    const size_t nproj = size_t(scan->channels) * scan->rows * scan->total_views;
+    Dev<float> d_proj(nproj), d_vol(nvox);
+    if (!d_proj.p || !d_vol.p) return fail("cudaMalloc");
+    if (cudaMemcpy(d_proj.p, h_proj, nproj * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemset(d_vol.p, 0, nvox * sizeof(float)) != cudaSuccess)
+        return fail("upload");
+    YK::CglsAstraBackend cgls;
+    YK::CglsAstraBackend::Config cfg{};
+    cfg.n_iter = n_iter;
+    cfg.fp_task = YK::ETask::FP_Joseph;
+    cfg.bp_task = matched ? YK::ETask::BP_Joseph : YK::ETask::BP_FDK_PseudoMatched;
+    if (!cgls.init(geometry.base(), cfg, geometry.allGeometry(), stream.s, device))
+        return fail("CglsAstraBackend::init");
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, stream.s);
+    const bool ok = cgls.run(d_proj.p, d_vol.p, geometry.base(), stream.s);
+    cudaEventRecord(e1, stream.s);
+    cudaEventSynchronize(e1);
+    if (ms) *ms = elapsed(e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (!ok) return fail("CglsAstraBackend::run");
+    if (cudaMemcpy(h_vol, d_vol.p, nvox * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return fail("download");
+    cgls.release();
+    return 0;
+}
 
 // Joseph forward projection (FP_Joseph) of a host volume; optional timing
 // (ms != NULL, reps > 0) of the operator call on the device-resident volume.
