@@ -38,9 +38,16 @@ METRIC = "FDK backprojection GUPS (voxel\u00d7view/s) & FP+BP grad step ms at st
 
 # the workload the metric is quoted on, and a small case of the same kernels
 # (inputs still larger than L2) used for profiler captures
+# "large": the 1024^3 x 1440-view x 1536^2 FDK with BF16-stored projections
+# (6.8 GB), tensor-core BF16 filter and FP32 backprojection; its phantom adds
+# 200 small high-contrast spheres and it is noise-free
 CONFIGS = {
-    "c2": dict(N_VOX=512, N_VIEWS=720, N_DET=768, VOX_MM=0.25, PIX_MM=0.4),
-    "small": dict(N_VOX=256, N_VIEWS=360, N_DET=384, VOX_MM=0.5, PIX_MM=0.8),
+    "c2": dict(N_VOX=512, N_VIEWS=720, N_DET=768, VOX_MM=0.25, PIX_MM=0.4, N_ELL=20, N_SPH=0,
+               I0=1e5, PRECISION="fp32"),
+    "small": dict(N_VOX=256, N_VIEWS=360, N_DET=384, VOX_MM=0.5, PIX_MM=0.8, N_ELL=20, N_SPH=0,
+                  I0=1e5, PRECISION="fp32"),
+    "large": dict(N_VOX=1024, N_VIEWS=1440, N_DET=1536, VOX_MM=0.125, PIX_MM=0.2, N_ELL=40,
+                  N_SPH=200, I0=None, PRECISION="bf16"),
 }
 N_VOX = 512
 N_VIEWS = 720
@@ -49,18 +56,27 @@ VOX_MM = 0.25
 PIX_MM = 0.4
 SID, SDD = 500.0, 1000.0
 N_ELL = 20
+N_SPH = 0
 I0 = 1e5
+PRECISION = "fp32"
 UPDATES = N_VOX ** 3 * N_VIEWS
 WORKLOAD = "fdk-512^3-720v-768^2"
 
 
 def select_config(name: str) -> None:
-    global N_VOX, N_VIEWS, N_DET, VOX_MM, PIX_MM, UPDATES, WORKLOAD
+    global N_VOX, N_VIEWS, N_DET, VOX_MM, PIX_MM, N_ELL, N_SPH, I0, PRECISION, UPDATES, WORKLOAD
     c = CONFIGS[name]
     N_VOX, N_VIEWS, N_DET, VOX_MM, PIX_MM = (c["N_VOX"], c["N_VIEWS"], c["N_DET"], c["VOX_MM"],
                                              c["PIX_MM"])
+    N_ELL, N_SPH, I0, PRECISION = c["N_ELL"], c["N_SPH"], c["I0"], c["PRECISION"]
     UPDATES = N_VOX ** 3 * N_VIEWS
-    WORKLOAD = f"fdk-{N_VOX}^3-{N_VIEWS}v-{N_DET}^2"
+    WORKLOAD = f"fdk-{N_VOX}^3-{N_VIEWS}v-{N_DET}^2" + ("-bf16" if PRECISION == "bf16" else "")
+
+
+def chunk_views() -> int:
+    """Views per workspace chunk of an FDK plan: a budget of 8 GiB at 12 bytes
+    per detector pixel (preweighted rows + filtered tap pairs)."""
+    return max(1, min(N_VIEWS, (8 << 30) // (12 * N_DET * N_DET)))
 
 
 def parse():
@@ -146,7 +162,7 @@ def measured_peaks():
 def cpu_baseline(n_views_sample=96, z_slab=64):
     """FP64 oracle FDK on a bounded sample of the same workload: a subset of
     views (full 768x768 projections: preweight + filter) backprojected into
-    a z-slab of the 512^3 volume.  Returns GUPS on the host cores."""
+    a z-slab of the volume.  Returns GUPS on the host cores."""
     import numpy as np
     from oracle import oracle as O
     views_all = O.build_circular_flat(N_VIEWS, N_VIEWS, SID, SDD, N_DET, N_DET, PIX_MM, PIX_MM)
@@ -161,8 +177,8 @@ def cpu_baseline(n_views_sample=96, z_slab=64):
     dt = time.perf_counter() - t0
     updates = n_views_sample * z_slab * N_VOX * N_VOX
     return {"value": updates / dt / 1e9, "unit": "GUPS", "cores": O.num_threads(), "kind": "port",
-            "sample": f"{n_views_sample} of 720 views (full 768x768 preweight+ramp filter) "
-                      f"backprojected into a 512x512x{z_slab} slab, FP64, {dt:.1f} s"}
+            "sample": f"{n_views_sample} of {N_VIEWS} views (full {N_DET}x{N_DET} preweight+ramp "
+                      f"filter) backprojected into a {N_VOX}x{N_VOX}x{z_slab} slab, FP64, {dt:.1f} s"}
 
 
 # Differentiable Joseph pair (the metric's "FP+BP grad step"): 256^3 of
@@ -221,17 +237,32 @@ def make_workload(rank: int, local: int):
     from fdk_cuda_impl_b200 import CircularScan, VolumeGrid
     from fdk_cuda_impl_b200 import phantom as PH
     from fdk_cuda_impl_b200.projectors import JosephPlan
+    import numpy as np
     scan = CircularScan(N_VIEWS, N_VIEWS, SID, SDD, N_DET, N_DET, PIX_MM, PIX_MM)
     grid = VolumeGrid.cube(N_VOX, VOX_MM)
     views = scan.views()
     ell = PH.random_ellipsoids(1000 + rank, N_ELL)
+    if N_SPH:
+        ell = np.concatenate([ell, PH.random_spheres(1000 + rank, N_SPH)])
     phantom = PH.voxelize(grid, ell, device=f"cuda:{local}")
-    jp = JosephPlan(views, N_DET, N_DET, grid, device=local)
-    proj = jp.forward(phantom)
-    jp.close()
-    del jp, phantom
-    PH.poisson_noise_(proj, I0, seed=7 + rank)
+    dtype = torch.bfloat16 if PRECISION == "bf16" else torch.float32
+    proj = torch.empty((N_VIEWS, N_DET, N_DET), dtype=dtype, device=f"cuda:{local}")
+    # Joseph projection in view chunks (its plan holds a 20-byte ray record
+    # per detector pixel of its views)
+    step = max(1, min(N_VIEWS, (4 << 30) // (20 * N_DET * N_DET)))
+    for v0 in range(0, N_VIEWS, step):
+        jp = JosephPlan(views[v0:v0 + step], N_DET, N_DET, grid, device=local)
+        part = jp.forward(phantom)
+        if I0 is not None and dtype != torch.float32:
+            PH.poisson_noise_(part, I0, seed=7 + rank + v0)
+        proj[v0:v0 + step] = part
+        jp.close()
+        del jp, part
+    del phantom
+    if I0 is not None and dtype == torch.float32:
+        PH.poisson_noise_(proj, I0, seed=7 + rank)
     torch.cuda.synchronize()
+    torch.cuda.empty_cache()
     return scan, grid, views, proj
 
 
@@ -261,7 +292,7 @@ def run_reference(args):
     if R.available() and torch.cuda.is_available():
         from fdk_cuda_impl_b200 import RampFilter
         scan, grid, _, proj = make_workload(0, 0)
-        h_proj = proj.cpu().numpy()
+        h_proj = proj.float().cpu().numpy()  # the reference takes FP32 projections
         del proj
         torch.cuda.empty_cache()
         ms_dev, ms_host = R.fdk_time(scan, grid, RampFilter(), h_proj, warmup=args.warmup,
@@ -335,7 +366,8 @@ def main():
 
     scan, grid, views, proj = make_workload(rank, local)
 
-    plan = FdkPlan(views, N_DET, N_DET, scan.scan_range, grid, RampFilter(), "fp32", device=local)
+    plan = FdkPlan(views, N_DET, N_DET, scan.scan_range, grid, RampFilter(), PRECISION,
+                   device=local)
     vol = torch.empty(grid.shape, dtype=torch.float32, device=f"cuda:{local}")
     stream = torch.cuda.current_stream()
 
@@ -381,7 +413,7 @@ def main():
     # end to end through the C-ABI with pinned host buffers: the projections
     # stream host -> device in batches overlapping the kernels, the volume
     # comes back to the host, all inside the timed region
-    h_proj = torch.empty(proj.shape, dtype=torch.float32, pin_memory=True)
+    h_proj = torch.empty(proj.shape, dtype=proj.dtype, pin_memory=True)
     h_proj.copy_(proj)
     h_vol = torch.empty(grid.shape, dtype=torch.float32, pin_memory=True)
     d_in = proj
@@ -400,8 +432,23 @@ def main():
     # device), Shepp-Logan window, tcgen05 split hi/lo Toeplitz filter, the
     # same backprojection.  Its error is taken against the FP32 form (itself
     # within 1e-5 of the FP64 oracle) on the same BF16-stored projections.
-    bf16 = None
-    if not args.no_bf16:
+    bf16 = fp32_form = None
+    if PRECISION == "bf16":
+        # the FP32 form on the same BF16-stored projections: the error of the
+        # tensor-core filter, and the speed-up it buys
+        plan_s = FdkPlan(views, N_DET, N_DET, scan.scan_range, grid, RampFilter(), "fp32",
+                         device=local)
+        vs = torch.empty_like(vol)
+        for _ in range(max(1, args.warmup - 1)):
+            plan_s.execute(d_in, vs)
+        ms_s = timed(lambda: plan_s.execute(d_in, vs), args.steps)
+        plan.execute(d_in, vol)
+        diff = (vol.double() - vs.double()).pow(2).mean().sqrt() / vs.double().pow(2).mean().sqrt()
+        fp32_form = {"ms_per_step": ms_s, "gups": world * UPDATES / (ms_s * 1e-3) / 1e9,
+                     "bf16_speedup": ms_s / ms, "bf16_rel_rmse_vs_fp32_form": float(diff)}
+        plan_s.close()
+        del vs
+    elif not args.no_bf16:
         sl = RampFilter.named("shepplogan")
         plan_b = FdkPlan(views, N_DET, N_DET, scan.scan_range, grid, sl, "bf16", device=local)
         h_proj_b = torch.empty(h_proj.shape, dtype=torch.bfloat16, pin_memory=True)
@@ -432,7 +479,9 @@ def main():
         plan_b.close()
         del ref_vol, vb, d_in_b, h_proj_b
 
-    joseph = joseph_step(local, args.steps, args.warmup, timed) if not args.no_joseph else None
+    joseph = None
+    if not args.no_joseph and PRECISION == "fp32":
+        joseph = joseph_step(local, args.steps, args.warmup, timed)
 
     peaks, peak_src = measured_peaks()
     # HBM roofline of the dominant kernel (backprojection): compulsory bytes
@@ -461,27 +510,34 @@ def main():
         "metric": METRIC,
         "value": value, "unit": "GUPS", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "vs_baseline": None, "dtype": "f32" if PRECISION == "fp32" else "bf16 filter, f32 backprojection",
+        "data": "synthetic",
         "config": {"workload": WORKLOAD, "volume": [N_VOX] * 3, "voxel_mm": VOX_MM,
                    "views": N_VIEWS, "detector": [N_DET, N_DET], "pixel_mm": PIX_MM,
-                   "sid_sdd_mm": [SID, SDD], "ellipsoids": N_ELL, "noise_i0": I0,
-                   "filter": "ramlak", "precision": "fp32",
-                   "l2": "inputs larger than L2 (1.7 GB projections, 0.54 GB volume)",
+                   "sid_sdd_mm": [SID, SDD], "ellipsoids": N_ELL, "spheres": N_SPH,
+                   "noise_i0": I0, "filter": "ramlak", "precision": PRECISION,
+                   "projections": "bf16" if PRECISION == "bf16" else "f32",
+                   "l2": f"inputs larger than L2 ({h_proj.numel() * h_proj.element_size() / 1e9:.1f} GB "
+                         f"projections, {4 * N_VOX ** 3 / 1e9:.2f} GB volume)",
+                   "chunk_views": chunk_views(),
                    "parallelism": f"independent objects x{world}"},
         "stages_ms": {"filter": ms_filter, "backproject": ms_bp},
         "roofline": roofline,
         "onchip": onchip,
         "e2e": {"value": e2e_value, "unit": "GUPS", "ms_per_step": ms_e2e,
-                "h2d_bytes_per_step": int(h_proj.numel() * 4),
+                "h2d_bytes_per_step": int(h_proj.numel() * h_proj.element_size()),
                 "d2h_bytes_per_step": int(h_vol.numel() * 4)},
         "bf16": bf16,
+        "fp32_form": fp32_form,
         "joseph": joseph,
-        "gpu_launches": 3 * args.steps,
+        # preweight, filter and backprojection per workspace chunk
+        "gpu_launches": 3 * -(-N_VIEWS // chunk_views()) * args.steps,
         "clocks": clock_info,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            line["cpu_baseline"] = cpu_baseline()
+            line["cpu_baseline"] = (cpu_baseline() if N_DET <= 768 else
+                                    cpu_baseline(n_views_sample=24, z_slab=32))
         except Exception as exc:  # the baseline is reported, never required
             line["cpu_baseline"] = {"error": str(exc)}
     if rank == 0:

@@ -52,16 +52,28 @@ def voxelize(grid: VolumeGrid, ellipsoids: np.ndarray, device="cuda", slab: int 
     for z0 in range(0, grid.nz, slab):
         z1 = min(grid.nz, z0 + slab)
         zs = cz + (torch.arange(z0, z1, device=device, dtype=torch.float64) - 0.5 * (grid.nz - 1)) * vz
-        Z, Y, X = torch.meshgrid(zs, ys, xs, indexing="ij")
-        acc = torch.zeros(Z.shape, dtype=torch.float64, device=device)
+        acc = torch.zeros((z1 - z0, grid.ny, grid.nx), dtype=torch.float64, device=device)
         for e in ellipsoids:
+            # only the voxels within the largest semi-axis of the centre can
+            # be inside: q >= |d|^2 / a_max^2 > 1 beyond it
+            box = []
+            for c, axis_mm, n, origin in ((e[2], vz, z1 - z0, zs[0].item()), (e[1], vy, grid.ny, ys[0].item()),
+                                          (e[0], vx, grid.nx, xs[0].item())):
+                r = max(e[3], e[4], e[5])
+                lo = max(0, int(np.floor((c - r - origin) / axis_mm)) - 1)
+                hi = min(n, int(np.ceil((c + r - origin) / axis_mm)) + 2)
+                box.append((lo, hi))
+            (za, zb), (ya, yb), (xa, xb) = box
+            if za >= zb or ya >= yb or xa >= xb:
+                continue
+            Z, Y, X = torch.meshgrid(zs[za:zb], ys[ya:yb], xs[xa:xb], indexing="ij")
             R = torch.as_tensor(_rotation(e[6], e[7], e[8]), device=device)
             dx, dy, dz = X - e[0], Y - e[1], Z - e[2]
             lx = R[0, 0] * dx + R[1, 0] * dy + R[2, 0] * dz
             ly = R[0, 1] * dx + R[1, 1] * dy + R[2, 1] * dz
             lz = R[0, 2] * dx + R[1, 2] * dy + R[2, 2] * dz
             q = (lx / e[3]) ** 2 + (ly / e[4]) ** 2 + (lz / e[5]) ** 2
-            acc += torch.where(q <= 1.0, e[9], 0.0)
+            acc[za:zb, ya:yb, xa:xb] += torch.where(q <= 1.0, e[9], 0.0)
         out[z0:z1] = acc.float()
     return out
 

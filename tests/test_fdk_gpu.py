@@ -206,7 +206,26 @@ def test_fdk_tma_matches_global_path(oracle, cuda_device):
     assert K.rel_rmse(out["global"], out["pairs"]) < 1e-6
 
 
-@pytest.mark.parametrize("nu,nv,views", [(96, 64, 12), (53, 41, 7), (192, 24, 5), (384, 8, 3)])
+@pytest.mark.parametrize("nu", [768, 1536])
+def test_fdk_filter_stage_wide(oracle, cuda_device, nu):
+    # the FP32 Toeplitz filter at the detector widths of the 512^3 and 1024^3
+    # workloads
+    import torch
+    from fdk_cuda_impl_b200.geometry import CircularScan
+    from fdk_cuda_impl_b200.projectors import FdkPlan
+    scan = CircularScan(3, 3, 500.0, 1000.0, nu, 6, 0.4, 0.4)
+    v = scan.views()
+    case = K.c1_small()
+    p = oracle.uniform((3, 6, nu), 0.0, 2.0, 50 + nu)
+    plan = FdkPlan(v, nu, 6, scan.scan_range, case.grid, case.filt)
+    got = plan.filter(torch.from_numpy(p).cuda()).cpu().numpy()
+    plan.check()
+    ref = oracle.fdk_filter(v, nu, 6, scan.scan_range, K.oracle_filter(oracle, case.filt), p)
+    assert K.rel_rmse(got, ref) <= 5e-6
+
+
+@pytest.mark.parametrize("nu,nv,views", [(96, 64, 12), (53, 41, 7), (192, 24, 5), (384, 8, 3),
+                                         (768, 8, 2), (1536, 6, 2)])
 def test_tc_filter_stage(oracle, cuda_device, nu, nv, views):
     # tcgen05 BF16 Toeplitz filter with hi/lo split against the FP64 filter:
     # the three-product split keeps about 16 mantissa bits
