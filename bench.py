@@ -217,6 +217,11 @@ def joseph_step(local: int, steps: int, warmup: int, timed_fn):
     ms = timed_fn(step, steps)
     fp_ms = timed_fn(lambda: plan.forward(x.detach()), steps)
     bp_ms = timed_fn(lambda: plan.adjoint(b), steps)
+    # BP_FDK_PseudoMatched, the reference's default backprojector for CGLS
+    pseudo = plan.backproject_pseudo(b)
+    pseudo_ms = timed_fn(lambda: plan.backproject_pseudo(b, pseudo), steps)
+    plan.check()
+    del pseudo
     with torch.no_grad():
         ax = plan.forward(x.detach())
         aty = plan.adjoint(b)
@@ -227,7 +232,9 @@ def joseph_step(local: int, steps: int, warmup: int, timed_fn):
     return {"workload": f"joseph-{J_VOX}^3-{J_VIEWS}v-{J_DET}^2", "grad_step_ms": ms,
             "fp_ms": fp_ms, "bp_ms": bp_ms, "adjoint_rel": abs(lhs - rhs) / abs(lhs),
             "samples_per_op": samples, "fp_gsamples": samples / (fp_ms * 1e-3) / 1e9,
-            "bp_gsamples": samples / (bp_ms * 1e-3) / 1e9}
+            "bp_gsamples": samples / (bp_ms * 1e-3) / 1e9,
+            "bp_pseudo_matched_ms": pseudo_ms,
+            "bp_pseudo_matched_gups": J_VOX ** 3 * J_VIEWS / (pseudo_ms * 1e-3) / 1e9}
 
 
 def make_workload(rank: int, local: int):
@@ -307,11 +314,14 @@ def run_reference(args):
         jy = gen.standard_normal((J_VIEWS, J_DET, J_DET)).astype(np.float32)
         _, fp_ms = R.joseph_fp(jscan, jgrid, jx, warmup=args.warmup, reps=args.steps)
         _, bp_ms = R.joseph_bp(jscan, jgrid, jy, warmup=args.warmup, reps=args.steps)
+        _, pseudo_ms = R.bp_pseudo(jscan, jgrid, jy, warmup=args.warmup, reps=args.steps)
         samples = J_VIEWS * J_DET * J_DET * J_VOX
         joseph = {"workload": f"joseph-{J_VOX}^3-{J_VIEWS}v-{J_DET}^2", "fp_ms": fp_ms,
                   "bp_ms": bp_ms, "grad_step_ms": fp_ms + bp_ms,
                   "fp_gsamples": samples / (fp_ms * 1e-3) / 1e9,
-                  "bp_gsamples": samples / (bp_ms * 1e-3) / 1e9}
+                  "bp_gsamples": samples / (bp_ms * 1e-3) / 1e9,
+                  "bp_pseudo_matched_ms": pseudo_ms,
+                  "bp_pseudo_matched_gups": J_VOX ** 3 * J_VIEWS / (pseudo_ms * 1e-3) / 1e9}
         line.update({
             "value": value, "ms_per_step": ms_dev, "dtype": "f32",
             "config": dict(cfg, implementation="reference CUDA build (YKCBCT FdkPipeline, "

@@ -91,7 +91,14 @@ SIGNATURES = {
     "ykb_joseph_fp": (C.c_int, [_P, _P, _P, C.c_int, _P]),
     "ykb_joseph_bp": (C.c_int, [_P, _P, _P, C.c_int, _P]),
     "ykb_joseph_workspace_bytes": (C.c_size_t, [_P]),
+    "ykb_operator_apply": (C.c_int, [_P, C.c_int, _P, _P, C.c_int, _P]),
+    "ykb_joseph_check": (C.c_int, [_P, _P]),
 }
+
+# ykb_task == YK::ETask values
+TASK_FP_JOSEPH = 1
+TASK_BP_FDK_PSEUDO_MATCHED = 7
+TASK_BP_JOSEPH = 8
 
 _lib = None
 

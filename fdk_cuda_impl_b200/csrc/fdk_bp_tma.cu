@@ -169,25 +169,51 @@ constexpr uint32_t kRoundMagicBits = 0x4B400000u;
 
 // Per (column, view) terms of the axial path, independent of the staged box:
 // computed one view ahead so their FP64 latency overlaps the previous view.
+// PSEUDO (pseudo-matched weight ks L(i) / den^2): w = ks / den^2 and
+// L(i)^2 = alp + i (bet + i gam) along the column, the detector quadratic
+// L^2(u, v) of PseudoViewCoef evaluated at u and v(i) = vb + i vs.
 struct ColTerms {
     float u, vbq, vs, w;
+    float alp, bet, gam;
 };
 
-__device__ __forceinline__ ColTerms axial_terms(const FdkViewCoef& c, double X, double Y,
-    double Z0, double vz)
+template <bool PSEUDO>
+__device__ __forceinline__ ColTerms axial_terms(const FdkViewCoef& c, const PseudoViewCoef* pc,
+    double X, double Y, double Z0, double vz)
 {
     const double den = fma(c.cd[1], Y, fma(c.cd[0], X, c.cd[3]));
     const double rd = rcp64(den);
     const double un = fma(c.cu[1], Y, fma(c.cu[0], X, c.cu[3]));
     const double vn = fma(c.cv[2], Z0, fma(c.cv[1], Y, fma(c.cv[0], X, c.cv[3])));
-    const double dep = fma(c.cr[1], Y, fma(c.cr[0], X, c.cr[3]));
-    const double rdep = rcp64(dep);
     ColTerms t;
-    t.u = static_cast<float>(un * rd);
-    t.vbq = static_cast<float>(vn * rd - 0.5);
-    t.vs = static_cast<float>(c.cv[2] * vz * rd);
-    t.w = static_cast<float>(c.wbase * rdep * rdep);
+    const double u = un * rd, vb = vn * rd, vs = c.cv[2] * vz * rd;
+    t.u = static_cast<float>(u);
+    t.vbq = static_cast<float>(vb - 0.5);
+    t.vs = static_cast<float>(vs);
+    if constexpr (PSEUDO) {
+        const float* l = pc->l2;
+        const double A = fma(u, fma(u, static_cast<double>(l[3]), static_cast<double>(l[1])),
+                             static_cast<double>(l[0]));
+        const double B = fma(u, static_cast<double>(l[4]), static_cast<double>(l[2]));
+        const double C = l[5];
+        t.alp = static_cast<float>(fma(vb, fma(vb, C, B), A));
+        t.bet = static_cast<float>(fma(2.0 * C, vb, B) * vs);
+        t.gam = static_cast<float>(C * vs * vs);
+        t.w = static_cast<float>(static_cast<double>(pc->ks) * rd * rd);
+    } else {
+        const double dep = fma(c.cr[1], Y, fma(c.cr[0], X, c.cr[3]));
+        const double rdep = rcp64(dep);
+        t.w = static_cast<float>(c.wbase * rdep * rdep);
+        t.alp = t.bet = t.gam = 0.f;
+    }
     return t;
+}
+
+__device__ __forceinline__ float sqrt_approx(float x)
+{
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
 }
 
 // Detector box of a voxel tile for one view: columns [c0, c1], rows [r0, r1]
@@ -267,10 +293,13 @@ __global__ void box_extent_kernel(const FdkViewCoef* __restrict__ coef, int n_vi
 // Shared-memory ring budget of one CTA; two CTAs share an SM.
 constexpr size_t kRingBudget = 108 * 1024;
 
-template <int BW, bool AXIAL, bool PAIR>
+// PSEUDO: the weight of the pseudo-matched backprojection instead of the FDK
+// depth weight (tap pairs only)
+template <int BW, bool AXIAL, bool PAIR, bool PSEUDO>
 __global__ void __launch_bounds__(NTHREADS, 2) fdk_bp_tma_kernel(const __grid_constant__ CUtensorMap map,
     const FdkViewCoef* __restrict__ coef, int n_views, VolumeGrid g, int BH, int stages,
-    float* __restrict__ vol, int accumulate, int* __restrict__ err)
+    float* __restrict__ vol, int accumulate, int* __restrict__ err,
+    const PseudoViewCoef* __restrict__ pseudo)
 {
     extern __shared__ unsigned char smem_raw[];
     // 128-byte aligned base (the launch requests 128 bytes of slack)
@@ -377,7 +406,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) fdk_bp_tma_kernel(const __grid_co
     for (int i = 0; i < ZT; ++i) acc[i] = 0.f;
     bool bad = false;
     ColTerms cur{};
-    if (AXIAL) cur = axial_terms(coef[0], X, Y, Z0, g.vz);
+    if (AXIAL) cur = axial_terms<PSEUDO>(coef[0], pseudo, X, Y, Z0, g.vz);
 
     int s = 0;
     uint32_t phase = 0;
@@ -392,12 +421,15 @@ __global__ void __launch_bounds__(NTHREADS, 2) fdk_bp_tma_kernel(const __grid_co
         const FdkViewCoef& c = coef[k];
         if (AXIAL) {
             // next view's terms first: independent of this view's stage
-            const ColTerms nxt = (k + 1 < n_views) ? axial_terms(coef[k + 1], X, Y, Z0, g.vz) : cur;
+            const ColTerms nxt = (k + 1 < n_views)
+                ? axial_terms<PSEUDO>(coef[k + 1], pseudo + (PSEUDO ? k + 1 : 0), X, Y, Z0, g.vz)
+                : cur;
             const float u = cur.u;
             const float fu = floorf(u);
             const int iu = static_cast<int>(fu);
             float au = u - fu;
             float vbq = cur.vbq, vs = cur.vs, w = cur.w;
+            float alp = cur.alp, bet = cur.bet, gam = cur.gam;
             // rows of the column's end points (the rounding map is monotonic)
             const int na = static_cast<int>(__float_as_uint(vbq + kRoundMagic) - kRoundMagicBits);
             const int nb = static_cast<int>(__float_as_uint(fmaf(static_cast<float>(ZT - 1), vs, vbq) +
@@ -405,12 +437,15 @@ __global__ void __launch_bounds__(NTHREADS, 2) fdk_bp_tma_kernel(const __grid_co
             const int lo = min(na, nb), hi = max(na, nb) + 1;
             // |v| < 2^21 along the column keeps the rounding word exact
             const bool finite = fabsf(u) < 1e6f && fabsf(vbq) < 1e6f && fabsf(vs) < 3e4f &&
-                fabsf(w) < 1e30f;
+                fabsf(w) < 1e30f && (!PSEUDO || (alp > 0.f && alp < 1e30f &&
+                fmaf(static_cast<float>(ZT - 1), fmaf(static_cast<float>(ZT - 1), gam, bet), alp) > 0.f &&
+                fabsf(bet) < 1e30f && fabsf(gam) < 1e30f));
             int col = iu - b.x;
             if (!active || !finite || iu < b.x || iu + 1 > b.z || lo < b.y || hi > b.w) {
                 if (active) bad = true;
                 // no contribution; every read stays at the stage origin
                 w = 0.f; au = 0.f; vs = 0.f;
+                alp = 1.f; bet = 0.f; gam = 0.f;
                 vbq = static_cast<float>(b.y);
                 col = 0;
             }
@@ -422,7 +457,31 @@ __global__ void __launch_bounds__(NTHREADS, 2) fdk_bp_tma_kernel(const __grid_co
             // the column's horizontal weights, with the view weight folded in
             const float w1 = w * au, w0 = w - w1;
             const f2 M2 = f2pack(kRoundMagic, kRoundMagic), H2 = f2pack(0.5f, 0.5f);
-            if constexpr (PAIR) {
+            if constexpr (PSEUDO) {
+                // L(i) is a square root of a quadratic in i; the FP64 column
+                // terms keep its sqrt argument positive along the column
+#pragma unroll
+                for (int j = 0; j < ZT / 2; ++j) {
+                    const float i0 = 2.f * j, i1 = 2.f * j + 1.f;
+                    const f2 vq = f2pack(fmaf(i0, vs, vbq), fmaf(i1, vs, vbq));
+                    const f2 t = f2add(vq, M2);
+                    const f2 fr = f2add(f2sub(vq, f2sub(t, M2)), H2);
+                    float t0, t1, f0, f1;
+                    f2unpack(t, t0, t1);
+                    f2unpack(fr, f0, f1);
+                    const uint32_t a0 = __float_as_uint(t0) * (8u * BW) + base;
+                    const uint32_t a1 = __float_as_uint(t1) * (8u * BW) + base;
+                    const f2 A0 = lds2<0>(a0), B0 = lds2<8 * BW>(a0);
+                    const f2 A1 = lds2<0>(a1), B1 = lds2<8 * BW>(a1);
+                    float l0, r0, l1, r1;
+                    f2unpack(f2fma(f2pack(f0, f0), f2sub(B0, A0), A0), l0, r0);
+                    f2unpack(f2fma(f2pack(f1, f1), f2sub(B1, A1), A1), l1, r1);
+                    const float L0 = sqrt_approx(fmaf(i0, fmaf(i0, gam, bet), alp));
+                    const float L1 = sqrt_approx(fmaf(i1, fmaf(i1, gam, bet), alp));
+                    acc[2 * j] = fmaf(w * L0, fmaf(au, r0 - l0, l0), acc[2 * j]);
+                    acc[2 * j + 1] = fmaf(w * L1, fmaf(au, r1 - l1, l1), acc[2 * j + 1]);
+                }
+            } else if constexpr (PAIR) {
 #pragma unroll
                 for (int j = 0; j < ZT / 2; ++j) {
                     const f2 vq = f2pack(fmaf(2.f * j, vs, vbq), fmaf(2.f * j + 1.f, vs, vbq));
@@ -473,7 +532,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) fdk_bp_tma_kernel(const __grid_co
             const double un0 = fma(c.cu[2], Z0, fma(c.cu[1], Y, fma(c.cu[0], X, c.cu[3])));
             const double vn0 = fma(c.cv[2], Z0, fma(c.cv[1], Y, fma(c.cv[0], X, c.cv[3])));
             const double dp0 = fma(c.cr[2], Z0, fma(c.cr[1], Y, fma(c.cr[0], X, c.cr[3])));
-            const float s0 = static_cast<float>(c.wbase);
+            const float s0 = PSEUDO ? 1.f : static_cast<float>(c.wbase);
             const float dn = static_cast<float>(den0), ddn = static_cast<float>(c.cd[2] * g.vz);
             const float uu = static_cast<float>(un0), dun = static_cast<float>(c.cu[2] * g.vz);
             const float vv = static_cast<float>(vn0), dvn = static_cast<float>(c.cv[2] * g.vz);
@@ -506,8 +565,17 @@ __global__ void __launch_bounds__(NTHREADS, 2) fdk_bp_tma_kernel(const __grid_co
                 const float rden = 1.f / fmaf(fi, gddn, gdn);
                 const float u = fmaf(fi, gdun, guu) * rden;
                 const float v = fmaf(fi, gdvn, gvv) * rden;
-                const float rdep = 1.f / fmaf(fi, gddp, gdp);
-                const float w = scale * rdep * rdep;
+                float w;
+                if constexpr (PSEUDO) {
+                    // ks L / den^2 (the reference's k L^3 / |P - S|^2 on the ray)
+                    const PseudoViewCoef& pv = pseudo[k];
+                    const float L2 = fmaf(v, fmaf(v, pv.l2[5], fmaf(u, pv.l2[4], pv.l2[2])),
+                                          fmaf(u, fmaf(u, pv.l2[3], pv.l2[1]), pv.l2[0]));
+                    w = L2 > 1e-8f ? scale * pv.ks * sqrt_approx(L2) * rden * rden : 0.f;
+                } else {
+                    const float rdep = 1.f / fmaf(fi, gddp, gdp);
+                    w = scale * rdep * rdep;
+                }
                 const float fu = floorf(u), fv = floorf(v);
                 const int a = static_cast<int>(fv) * BW + static_cast<int>(fu) + cb;
                 const float au = u - fu, av = v - fv;
@@ -557,41 +625,54 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
 
 constexpr int kWidths[] = {36, 52, 68, 100, 132, 196, 256};
 
+template <typename K>
+cudaError_t launch_kernel(K k, const CUtensorMap& map, const FdkViewCoef* coef, int n_views,
+    const VolumeGrid& g, int BH, int stages, size_t smem, float* vol, int accumulate, int* err,
+    const PseudoViewCoef* pseudo, cudaStream_t s)
+{
+    const dim3 grid((g.nx + TX - 1) / TX, (g.ny + TY - 1) / TY, (g.nz + ZT - 1) / ZT);
+    const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    k<<<grid, NTHREADS, smem, s>>>(map, coef, n_views, g, BH, stages, vol, accumulate, err, pseudo);
+    return cudaGetLastError();
+}
+
 template <int BW, bool PAIR>
 cudaError_t launch_bw(const CUtensorMap& map, const FdkViewCoef* coef, int n_views,
     const VolumeGrid& g, int BH, int stages, size_t smem, bool axial, float* vol, int accumulate,
-    int* err, cudaStream_t s)
+    int* err, const PseudoViewCoef* pseudo, cudaStream_t s)
 {
-    const dim3 grid((g.nx + TX - 1) / TX, (g.ny + TY - 1) / TY, (g.nz + ZT - 1) / ZT);
-    if (axial) {
-        auto k = fdk_bp_tma_kernel<BW, true, PAIR>;
-        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-            static_cast<int>(smem));
-        if (e != cudaSuccess) return e;
-        k<<<grid, NTHREADS, smem, s>>>(map, coef, n_views, g, BH, stages, vol, accumulate, err);
+    if constexpr (PAIR) {
+        if (pseudo && axial)
+            return launch_kernel(fdk_bp_tma_kernel<BW, true, true, true>, map, coef, n_views, g,
+                BH, stages, smem, vol, accumulate, err, pseudo, s);
+        if (pseudo)
+            return launch_kernel(fdk_bp_tma_kernel<BW, false, true, true>, map, coef, n_views, g,
+                BH, stages, smem, vol, accumulate, err, pseudo, s);
     } else {
-        auto k = fdk_bp_tma_kernel<BW, false, PAIR>;
-        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-            static_cast<int>(smem));
-        if (e != cudaSuccess) return e;
-        k<<<grid, NTHREADS, smem, s>>>(map, coef, n_views, g, BH, stages, vol, accumulate, err);
+        if (pseudo) return cudaErrorInvalidValue;  // pseudo-matched input is staged as pairs
     }
-    return cudaGetLastError();
+    if (axial)
+        return launch_kernel(fdk_bp_tma_kernel<BW, true, PAIR, false>, map, coef, n_views, g, BH,
+            stages, smem, vol, accumulate, err, pseudo, s);
+    return launch_kernel(fdk_bp_tma_kernel<BW, false, PAIR, false>, map, coef, n_views, g, BH,
+        stages, smem, vol, accumulate, err, pseudo, s);
 }
 
 template <bool PAIR>
 cudaError_t launch_layout(const CUtensorMap& map, const FdkViewCoef* coef, int n_views,
     const VolumeGrid& g, int bw, int bh, int stages, size_t smem, bool axial, float* vol,
-    int accumulate, int* err, cudaStream_t s)
+    int accumulate, int* err, const PseudoViewCoef* pseudo, cudaStream_t s)
 {
     switch (bw) {
-    case 36: return launch_bw<36, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, s);
-    case 52: return launch_bw<52, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, s);
-    case 68: return launch_bw<68, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, s);
-    case 100: return launch_bw<100, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, s);
-    case 132: return launch_bw<132, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, s);
-    case 196: return launch_bw<196, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, s);
-    case 256: return launch_bw<256, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, s);
+    case 36: return launch_bw<36, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, s);
+    case 52: return launch_bw<52, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, s);
+    case 68: return launch_bw<68, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, s);
+    case 100: return launch_bw<100, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, s);
+    case 132: return launch_bw<132, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, s);
+    case 196: return launch_bw<196, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, s);
+    case 256: return launch_bw<256, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, s);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -635,7 +716,7 @@ bool fdk_tma_available() { return encode_fn() != nullptr; }
 cudaError_t launch_fdk_backproject_tma(const float* filtered, int layout, int ld,
     int rows_total_views, const FdkViewCoef* coef, int n_views, int nu, int nv,
     const VolumeGrid& g, bool axial, int bw, int bh, float* vol, int accumulate, int* err,
-    cudaStream_t s)
+    cudaStream_t s, const PseudoViewCoef* pseudo)
 {
     auto enc = encode_fn();
     if (!enc) return cudaErrorNotSupported;
@@ -660,9 +741,9 @@ cudaError_t launch_fdk_backproject_tma(const float* filtered, int layout, int ld
     const size_t ring = static_cast<size_t>(stage_stride_floats(bw, bh, pair)) * sizeof(float) * stages;
     const size_t smem = 128 + ring + 2 * stages * sizeof(uint64_t) + stages * sizeof(int4) + 16;
     return pair ? launch_layout<true>(map, coef, n_views, g, bw, bh, stages, smem, axial, vol,
-                      accumulate, err, s)
+                      accumulate, err, pseudo, s)
                 : launch_layout<false>(map, coef, n_views, g, bw, bh, stages, smem, axial, vol,
-                      accumulate, err, s);
+                      accumulate, err, pseudo, s);
 }
 
 // Scalar filtered rows [rows][ld_in] -> tap pairs [rows][ldp]: element

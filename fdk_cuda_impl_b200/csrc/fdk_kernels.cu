@@ -1,6 +1,7 @@
 // FDK kernels for sm_100a: cosine preweight, FP32 Toeplitz ramp filter and
 // voxel-driven weighted backprojection.
 #include "ykb_internal.hpp"
+#include "pseudo_weight.cuh"
 
 #include <cuda_bf16.h>
 
@@ -246,7 +247,77 @@ __global__ void __launch_bounds__(256) fdk_bp_kernel(const T* __restrict__ proj,
     }
 }
 
+// Pseudo-matched backprojection with bounds-checked loads: the non-axial
+// column walk of fdk_bp_kernel with the weight of pseudo_weight.cuh.
+template <int ZT>
+__global__ void __launch_bounds__(256) pseudo_bp_kernel(const float* __restrict__ proj,
+    const FdkViewCoef* __restrict__ coef, const PseudoViewCoef* __restrict__ pseudo, int n_views,
+    int nu, int nv, VolumeGrid g, float* __restrict__ vol, int accumulate)
+{
+    const int x = blockIdx.x * 32 + threadIdx.x;
+    const int y = blockIdx.y * 8 + threadIdx.y;
+    const int z0 = blockIdx.z * ZT;
+    if (x >= g.nx || y >= g.ny) return;
+    const double X = g.ox + x * g.vx;
+    const double Y = g.oy + y * g.vy;
+    const double Z0 = g.oz + z0 * g.vz;
+    float acc[ZT];
+#pragma unroll
+    for (int i = 0; i < ZT; ++i) acc[i] = 0.f;
+    const long view_elems = static_cast<long>(nu) * nv;
+    for (int k = 0; k < n_views; ++k) {
+        const FdkViewCoef& c = coef[k];
+        const PseudoViewCoef& p = pseudo[k];
+        const float* img = proj + k * view_elems;
+        const double den0 = fma(c.cd[2], Z0, fma(c.cd[1], Y, fma(c.cd[0], X, c.cd[3])));
+        const double un0 = fma(c.cu[2], Z0, fma(c.cu[1], Y, fma(c.cu[0], X, c.cu[3])));
+        const double vn0 = fma(c.cv[2], Z0, fma(c.cv[1], Y, fma(c.cv[0], X, c.cv[3])));
+        const float dn = static_cast<float>(den0), ddn = static_cast<float>(c.cd[2] * g.vz);
+        const float uu = static_cast<float>(un0), dun = static_cast<float>(c.cu[2] * g.vz);
+        const float vv = static_cast<float>(vn0), dvn = static_cast<float>(c.cv[2] * g.vz);
+        const PseudoColumn col = pseudo_column(p, X, Y, Z0, g.vz);
+#pragma unroll
+        for (int i = 0; i < ZT; ++i) {
+            const float fi = static_cast<float>(i);
+            const float den = fmaf(fi, ddn, dn);
+            if (!(den > 1e-8f)) continue;  // the voxel is not in front of the source
+            const float rden = 1.f / den;
+            const float u = fmaf(fi, dun, uu) * rden;
+            const float v = fmaf(fi, dvn, vv) * rden;
+            if (!(fabsf(u) < 1e7f && fabsf(v) < 1e7f)) continue;
+            const float w = pseudo_weight(p, col, fi, u, v);
+            const float fu = floorf(u), fv = floorf(v);
+            const int iu = static_cast<int>(fu), iv = static_cast<int>(fv);
+            const float au = u - fu, av = v - fv;
+            const float p00 = tap(img, nu, nv, nu, iu, iv), p10 = tap(img, nu, nv, nu, iu + 1, iv);
+            const float p01 = tap(img, nu, nv, nu, iu, iv + 1), p11 = tap(img, nu, nv, nu, iu + 1, iv + 1);
+            const float r0 = fmaf(au, p10 - p00, p00);
+            const float r1 = fmaf(au, p11 - p01, p01);
+            acc[i] = fmaf(w, fmaf(av, r1 - r0, r0), acc[i]);
+        }
+    }
+    const long plane = static_cast<long>(g.nx) * g.ny;
+#pragma unroll
+    for (int i = 0; i < ZT; ++i) {
+        const int z = z0 + i;
+        if (z >= g.nz) break;
+        float* dst = vol + z * plane + static_cast<long>(y) * g.nx + x;
+        *dst = accumulate ? *dst + acc[i] : acc[i];
+    }
+}
+
 } // namespace
+
+cudaError_t launch_pseudo_backproject(const float* proj, const FdkViewCoef* coef,
+    const PseudoViewCoef* pseudo, int n_views, int nu, int nv, const VolumeGrid& grid,
+    float* vol, int accumulate, cudaStream_t s)
+{
+    constexpr int ZT = 8;
+    const dim3 blocks((grid.nx + 31) / 32, (grid.ny + 7) / 8, (grid.nz + ZT - 1) / ZT);
+    pseudo_bp_kernel<ZT><<<blocks, dim3(32, 8), 0, s>>>(proj, coef, pseudo, n_views, nu, nv,
+        grid, vol, accumulate);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_fdk_preweight(const void* proj, int proj_dtype,
     const FdkPreweightView* pw, const float* parker, int n_views, int nu, int nv, float* out,

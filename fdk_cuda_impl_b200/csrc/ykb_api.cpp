@@ -505,6 +505,7 @@ YKB_API ykb_status ykb_joseph_plan_create(const ykb_cone_view* views, int n_view
     if (!p) return fail(YKB_ERR_OUT_OF_MEMORY, "host allocation failed");
     p->device = device; p->n_views = n_views; p->nu = nu; p->nv = nv; p->volume = *volume;
     std::string why;
+    p->cone_views.assign(views, views + n_views);
     if (!build_joseph_views(views, n_views, nu, nv, *volume, p->host_views, why)) {
         delete p;
         return fail(YKB_ERR_INVALID_GEOMETRY, why);
@@ -596,7 +597,8 @@ YKB_API size_t ykb_joseph_workspace_bytes(const ykb_joseph_plan* p)
 {
     if (!p) return 0;
     return p->views.bytes + p->view_proj.bytes + p->rays.bytes + p->lens.bytes +
-        p->weighted.bytes + p->slab_x.bytes + p->slab_y.bytes;
+        p->weighted.bytes + p->slab_x.bytes + p->slab_y.bytes + p->fdk_coef.bytes +
+        p->pseudo_coef.bytes + p->pairs.bytes + p->err_flag.bytes;
 }
 
 YKB_API ykb_status ykb_joseph_fp(ykb_joseph_plan* p, const float* d_volume, float* d_proj,
@@ -614,6 +616,124 @@ YKB_API ykb_status ykb_joseph_fp(ykb_joseph_plan* p, const float* d_volume, floa
     YKB_TRY_CUDA(launch_joseph_fp(slabs, p->views.as<JosephView>(), p->axes.data(), p->n_views,
         p->nu, p->nv, d_proj, accumulate ? 1 : 0, s));
     return YKB_OK;
+}
+
+} // extern "C"
+
+namespace {
+
+// Per-view tables of the pseudo-matched backprojection, built on first use:
+// the FDK projection coefficients of the views (the reference derives them
+// with the same GeoDerivedManagerVec for its operator, YkProjectionOperators.hpp:
+// 249-251), the weight coefficients, and the TMA projection box.
+ykb_status prepare_pseudo(ykb_joseph_plan* p, cudaStream_t s)
+{
+    if (p->pseudo_ready) return YKB_OK;
+    std::vector<FdkDerived> g;
+    std::string why;
+    // the scan range only scales the FDK view weight, which this weight does not use
+    if (!derive_fdk_geometry(p->cone_views.data(), p->n_views, p->nu, p->nv,
+            6.28318530717958647692f, g, why))
+        return fail(YKB_ERR_INVALID_GEOMETRY, why);
+    std::vector<FdkViewCoef> coef;
+    std::vector<FdkPreweightView> pw;
+    bool axial = false;
+    build_fdk_coefficients(g, p->nu, coef, pw, axial);
+    p->pseudo_axial = axial;
+    std::vector<PseudoViewCoef> pc;
+    build_pseudo_coefficients(g, p->volume, pc);
+    cudaError_t e;
+    if ((e = p->fdk_coef.alloc(sizeof(FdkViewCoef) * coef.size())) != cudaSuccess ||
+        (e = p->pseudo_coef.alloc(sizeof(PseudoViewCoef) * pc.size())) != cudaSuccess ||
+        (e = p->err_flag.alloc(4 * sizeof(int))) != cudaSuccess)
+        return cuda_status(e, "cudaMalloc (pseudo-matched tables)");
+    YKB_TRY_CUDA(cudaMemcpyAsync(p->fdk_coef.ptr, coef.data(), p->fdk_coef.bytes,
+        cudaMemcpyHostToDevice, s));
+    YKB_TRY_CUDA(cudaMemcpyAsync(p->pseudo_coef.ptr, pc.data(), p->pseudo_coef.bytes,
+        cudaMemcpyHostToDevice, s));
+    YKB_TRY_CUDA(cudaMemsetAsync(p->err_flag.ptr, 0, p->err_flag.bytes, s));
+    p->pseudo_bw = p->pseudo_bh = 0;
+    if (fdk_tma_available() && !std::getenv("YKB_PSEUDO_BP_GLOBAL")) {
+        int bw = 0, bh = 0;
+        YKB_TRY_CUDA(fdk_tma_box(p->fdk_coef.as<FdkViewCoef>(), p->n_views,
+            make_grid(p->volume), p->err_flag.as<int>() + 2, &bw, &bh, s));
+        if (bw > 0 && fdk_tma_stages(bw, bh, kFilteredPairs) > 0) {
+            const int ld = (p->nu + kPairLead + 1) / 2 * 2;
+            if (p->pairs.alloc(static_cast<size_t>(p->n_views) * p->nv * ld * 8) == cudaSuccess) {
+                p->pseudo_bw = bw;
+                p->pseudo_bh = bh;
+                p->pseudo_ld = ld;
+            } else {
+                // without room for the staged pairs the bounds-checked kernel runs
+                cudaGetLastError();
+            }
+        }
+    }
+    YKB_TRY_CUDA(cudaStreamSynchronize(s));
+    p->pseudo_ready = true;
+    return YKB_OK;
+}
+
+ykb_status pseudo_bp(ykb_joseph_plan* p, const float* d_proj, float* d_volume, int accumulate,
+    cudaStream_t s)
+{
+    if (const ykb_status st = prepare_pseudo(p, s)) return st;
+    const VolumeGrid g = make_grid(p->volume);
+    if (p->pseudo_bw > 0) {
+        YKB_TRY_CUDA(launch_fdk_pairify(d_proj, p->nu, static_cast<long>(p->n_views) * p->nv,
+            p->nu, p->pairs.as<float>(), p->pseudo_ld, s));
+        YKB_TRY_CUDA(launch_fdk_backproject_tma(p->pairs.as<float>(), kFilteredPairs,
+            p->pseudo_ld, p->n_views, p->fdk_coef.as<FdkViewCoef>(), p->n_views, p->nu, p->nv, g,
+            p->pseudo_axial, p->pseudo_bw, p->pseudo_bh, d_volume, accumulate,
+            p->err_flag.as<int>(), s,
+            p->pseudo_coef.as<PseudoViewCoef>()));
+        return YKB_OK;
+    }
+    YKB_TRY_CUDA(launch_pseudo_backproject(d_proj, p->fdk_coef.as<FdkViewCoef>(),
+        p->pseudo_coef.as<PseudoViewCoef>(), p->n_views, p->nu, p->nv, g, d_volume, accumulate, s));
+    return YKB_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+YKB_API ykb_status ykb_operator_apply(ykb_joseph_plan* p, int task, const float* d_in,
+    float* d_out, int accumulate, ykb_stream stream)
+{
+    clear_error();
+    if (!p) return fail(YKB_ERR_INVALID_CONFIG, "null plan");
+    switch (task) {
+    case YKB_TASK_FP_JOSEPH: return ykb_joseph_fp(p, d_in, d_out, accumulate, stream);
+    case YKB_TASK_BP_JOSEPH: return ykb_joseph_bp(p, d_in, d_out, accumulate, stream);
+    case YKB_TASK_BP_FDK_PSEUDO_MATCHED: {
+        if (!d_in || !d_out) return fail(YKB_ERR_INVALID_BUFFER, "null volume or projection buffer");
+        DeviceGuard guard(p->device);
+        return pseudo_bp(p, d_in, d_out, accumulate ? 1 : 0, reinterpret_cast<cudaStream_t>(stream));
+    }
+    default:
+        return fail(YKB_ERR_UNSUPPORTED, "operator task " + std::to_string(task) + " is not implemented");
+    }
+}
+
+YKB_API ykb_status ykb_joseph_check(ykb_joseph_plan* p, ykb_stream stream)
+{
+    clear_error();
+    if (!p) return fail(YKB_ERR_INVALID_CONFIG, "null plan");
+    if (!p->err_flag.ptr) return YKB_OK;
+    DeviceGuard guard(p->device);
+    const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    int word = 0;
+    YKB_TRY_CUDA(cudaMemcpyAsync(&word, p->err_flag.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));
+    YKB_TRY_CUDA(cudaStreamSynchronize(s));
+    if (word == 0) return YKB_OK;
+    YKB_TRY_CUDA(cudaMemsetAsync(p->err_flag.ptr, 0, sizeof(int), s));
+    YKB_TRY_CUDA(cudaStreamSynchronize(s));
+    std::string msg = "device-side failure in the pseudo-matched backprojection:";
+    if (word & 1) msg += " a pipeline wait timed out;";
+    if (word & 2) msg += " a voxel column left its projection box;";
+    if (word & 4) msg += " a staged copy was not 128-byte aligned (skipped);";
+    return fail(YKB_ERR_CUDA, msg);
 }
 
 YKB_API ykb_status ykb_joseph_bp(ykb_joseph_plan* p, const float* d_proj, float* d_volume,

@@ -346,6 +346,30 @@ void build_fdk_coefficients(const std::vector<FdkDerived>& g, int nu,
     }
 }
 
+// YkFDKBpPrecompute.cu:104-122 (L^2 expansion, 1/|SDD_plane|) and
+// YkBpFdkKernel.cu:363 (voxel volume over the pixel area of the first view)
+void build_pseudo_coefficients(const std::vector<FdkDerived>& g, const ykb_volume& vol,
+    std::vector<PseudoViewCoef>& out)
+{
+    out.assign(g.size(), PseudoViewCoef{});
+    if (g.empty()) return;
+    const double cell = static_cast<double>(vol.vox_x) * vol.vox_y * vol.vox_z / (g[0].du * g[0].dv);
+    for (size_t i = 0; i < g.size(); ++i) {
+        const FdkDerived& d = g[i];
+        const dvec3 r0 = dsub(d.detS, d.src);
+        PseudoViewCoef& c = out[i];
+        c.src[0] = d.src.x; c.src[1] = d.src.y; c.src[2] = d.src.z;
+        c.l2[0] = static_cast<float>(ddot(r0, r0));
+        c.l2[1] = static_cast<float>(2.0 * ddot(r0, d.detU));
+        c.l2[2] = static_cast<float>(2.0 * ddot(r0, d.detV));
+        c.l2[3] = static_cast<float>(ddot(d.detU, d.detU));
+        c.l2[4] = static_cast<float>(2.0 * ddot(d.detU, d.detV));
+        c.l2[5] = static_cast<float>(ddot(d.detV, d.detV));
+        c.k = std::fabs(d.plane) > 1e-12 ? static_cast<float>(cell / std::fabs(d.plane)) : 0.f;
+        c.ks = static_cast<float>(cell * std::fabs(d.plane));
+    }
+}
+
 namespace {
 double bessel_i0(double x)
 {

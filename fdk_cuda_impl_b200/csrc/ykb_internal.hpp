@@ -127,6 +127,27 @@ void build_fdk_coefficients(const std::vector<FdkDerived>& g, int nu,
 void build_ramp_kernel(int nu, double du, const ykb_filter& f,
     std::vector<double>& h);
 
+// Per-view data of the pseudo-matched backprojection (BP_FDK_PseudoMatched,
+// src/FlatFpBp/BP/kernels/YkBpFdkKernel.cu:356-450).  A voxel P projecting to
+// detector pixel coordinates (u, v) receives k L^3 / |P - S|^2 times the
+// bilinear sample, where L^2 = |detS + u detU + v detV - S|^2 is expanded
+// once per view as a quadratic in (u, v) and k = voxel volume /
+// (du dv |SDD_plane|) (src/Reconstruction/Analytic/Circular/Flat/FDK/kernels/
+// YkFDKBpPrecompute.cu:104-122).
+// Since |P - S| = L den / SDD_plane for the detector point of P (den =
+// (P - S).n, n the unit detector normal), the weight equals
+// ks L / den^2 with ks = voxel volume |SDD_plane| / (du dv); the TMA
+// kernel uses that form, in which only L varies along an axial z-column.
+struct alignas(16) PseudoViewCoef {
+    double src[4];
+    float l2[6];  // l2[0] + u l2[1] + v l2[2] + u^2 l2[3] + u v l2[4] + v^2 l2[5]
+    float k;
+    float ks;
+};
+
+void build_pseudo_coefficients(const std::vector<FdkDerived>& g, const ykb_volume& vol,
+    std::vector<PseudoViewCoef>& out);
+
 // Joseph per-view data (FP64), volume-centred voxel units.
 struct alignas(16) JosephView {
     double src[4];
@@ -190,10 +211,17 @@ bool fdk_tma_available();
 int fdk_tma_stages(int bw, int bh, int layout);
 cudaError_t fdk_tma_box(const FdkViewCoef* coef, int n_views, const VolumeGrid& g,
     int* scratch2, int* bw, int* bh, cudaStream_t s);
+// pseudo != nullptr: the pseudo-matched weight of PseudoViewCoef replaces the
+// FDK depth weight (tap-pair layout only)
 cudaError_t launch_fdk_backproject_tma(const float* filtered, int layout, int ld,
     int views_in_buffer, const FdkViewCoef* coef, int n_views, int nu, int nv,
     const VolumeGrid& g, bool axial, int bw, int bh, float* vol, int accumulate, int* err,
-    cudaStream_t s);
+    cudaStream_t s, const PseudoViewCoef* pseudo = nullptr);
+// Pseudo-matched backprojection straight from projections [n][nv][nu] with
+// bounds-checked loads (used when the TMA box does not fit)
+cudaError_t launch_pseudo_backproject(const float* proj, const FdkViewCoef* coef,
+    const PseudoViewCoef* pseudo, int n_views, int nu, int nv, const VolumeGrid& grid,
+    float* vol, int accumulate, cudaStream_t s);
 cudaError_t launch_fdk_pairify(const float* in, int ld_in, long rows, int nu, float* out,
     int ldp, cudaStream_t s);
 
@@ -255,6 +283,7 @@ struct ykb_joseph_plan {
     int n_views = 0, nu = 0, nv = 0;
     ykb_volume volume{};
     std::vector<ykb::JosephView> host_views;
+    std::vector<ykb_cone_view> cone_views;
     std::vector<int> axes;
     ykb::DeviceBuffer views;     // JosephView[n]
     ykb::DeviceBuffer view_proj; // float[n][12]: voxel-space 3x4 projection
@@ -262,4 +291,13 @@ struct ykb_joseph_plan {
     ykb::DeviceBuffer lens;      // float[n*nv*nu]: chord length per step
     ykb::DeviceBuffer weighted;  // float[n*nv*nu]: backprojector input x chord length
     ykb::DeviceBuffer slab_y, slab_x;  // transposed volume copies
+    // pseudo-matched backprojection, set up on first use
+    bool pseudo_ready = false;
+    bool pseudo_axial = false;         // untilted detector: the axial column walk
+    int pseudo_bw = 0, pseudo_bh = 0;  // TMA projection box (0: bounds-checked loads)
+    int pseudo_ld = 0;                 // tap-pair row pitch
+    ykb::DeviceBuffer fdk_coef;        // FdkViewCoef[n]
+    ykb::DeviceBuffer pseudo_coef;     // PseudoViewCoef[n]
+    ykb::DeviceBuffer pairs;           // projections as tap pairs [n][nv][pseudo_ld]
+    ykb::DeviceBuffer err_flag;        // int[4]: device error word, box pre-pass scratch
 };

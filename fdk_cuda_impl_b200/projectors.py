@@ -198,6 +198,34 @@ class JosephPlan:
                                        _stream_handle(self.device)))
         return out
 
+    def backproject_pseudo(self, proj: torch.Tensor, out: torch.Tensor | None = None,
+                           accumulate: bool = False) -> torch.Tensor:
+        """BP_FDK_PseudoMatched: voxel-driven bilinear backprojection with the
+        weight L^3 / (|P - S|^2 SDD_plane) x voxel volume / pixel area, an
+        approximate transpose of the forward projector
+        (src/FlatFpBp/BP/kernels/YkBpFdkKernel.cu:356-450)."""
+        return self.apply(L.TASK_BP_FDK_PSEUDO_MATCHED, proj, out, accumulate)
+
+    def apply(self, task: int, x: torch.Tensor, out: torch.Tensor | None = None,
+              accumulate: bool = False) -> torch.Tensor:
+        """One operator task (ykb_operator_apply; task values of YK::ETask)."""
+        forward = task == L.TASK_FP_JOSEPH
+        in_shape, out_shape = ((self.grid.shape, self.proj_shape) if forward
+                               else (self.proj_shape, self.grid.shape))
+        _check_tensor(x, in_shape, (torch.float32,), self.device, "input")
+        if out is None:
+            out = torch.empty(out_shape, dtype=torch.float32, device=x.device)
+            accumulate = False
+        _check_tensor(out, out_shape, (torch.float32,), self.device, "output")
+        L.check(self.lib.ykb_operator_apply(self._h, task, C.c_void_p(x.data_ptr()),
+                                            C.c_void_p(out.data_ptr()), 1 if accumulate else 0,
+                                            _stream_handle(self.device)))
+        return out
+
+    def check(self) -> None:
+        """Raises when the device error word of the plan is set."""
+        L.check(self.lib.ykb_joseph_check(self._h, _stream_handle(self.device)))
+
     def close(self) -> None:
         if getattr(self, "_h", None):
             self.lib.ykb_joseph_plan_destroy(self._h)

@@ -256,6 +256,36 @@ YKB_API ykb_status ykb_joseph_fp(ykb_joseph_plan* plan, const float* d_volume,
 YKB_API ykb_status ykb_joseph_bp(ykb_joseph_plan* plan, const float* d_proj,
     float* d_volume, int accumulate, ykb_stream stream);
 
+/* Operator tasks of a projector plan: the values of YK::ETask
+ * (src/common/YkOperatorTypes.hpp:5-22) that this library implements. */
+typedef enum ykb_task {
+    YKB_TASK_FP_JOSEPH = 1,
+    YKB_TASK_BP_FDK_PSEUDO_MATCHED = 7,
+    YKB_TASK_BP_JOSEPH = 8
+} ykb_task;
+
+/* Applies one operator of the plan's view sequence.  Forward tasks read a
+ * volume [nz][ny][nx] from d_in and write projections [n][nv][nu] to d_out,
+ * back tasks the reverse; d_out = (accumulate ? d_out : 0) + op(d_in).
+ * Replaces IForwardOperator/IBackOperator::apply for the task
+ * (src/common/YkProjectionOperators.hpp:138-180,242-340).
+ *   YKB_TASK_FP_JOSEPH, YKB_TASK_BP_JOSEPH: ykb_joseph_fp, ykb_joseph_bp.
+ *   YKB_TASK_BP_FDK_PSEUDO_MATCHED: voxel-driven bilinear backprojection
+ *     with the weight L^3 / (|P - S|^2 SDD_plane) x voxel volume / pixel
+ *     area (fdk_pseudo_matched_bp_launch, src/FlatFpBp/BP/kernels/
+ *     YkBpFdkKernel.cu:356-450,532-548), an approximate transpose of the
+ *     forward projector.  Its first call builds the plan's tables for it
+ *     (synchronising the stream) and a tap-pair copy of the projections
+ *     (8 bytes per pixel).
+ * Other task values return YKB_ERR_UNSUPPORTED. */
+YKB_API ykb_status ykb_operator_apply(ykb_joseph_plan* plan, int task,
+    const float* d_in, float* d_out, int accumulate, ykb_stream stream);
+
+/* Reads and clears the plan's device error word (pseudo-matched
+ * backprojection); synchronises the stream.  YKB_ERR_CUDA with the reasons
+ * when it was set. */
+YKB_API ykb_status ykb_joseph_check(ykb_joseph_plan* plan, ykb_stream stream);
+
 /* Bytes of device workspace the plan holds (introspection). */
 YKB_API size_t ykb_joseph_workspace_bytes(const ykb_joseph_plan* plan);
 

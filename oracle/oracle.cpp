@@ -726,6 +726,51 @@ int orc_fdk_backproject(const orc_view* views, int n, int nu, int nv,
     return 0;
 }
 
+// BP_FDK_PseudoMatched: fdk_bp_kernel_matched_weight,
+// src/FlatFpBp/BP/kernels/YkBpFdkKernel.cu:356-450, launched by
+// fdk_pseudo_matched_bp_launch (:532-548) through BackOperator::apply
+// (src/common/YkProjectionOperators.hpp:324-333).  Each voxel P takes the
+// bilinear sample (zero outside the detector) at its projection (u, v) times
+//     vox_x vox_y vox_z / (du dv) / |SDD_plane| * L^3 / |P - S|^2,
+// L = |detS + u detU + v detV - S| the distance from the source to the
+// detector point (YkFDKBpPrecompute.cu:104-122), du/dv of the first view.
+// Voxels whose plane depth is not positive are skipped, as the reference
+// skips den < 1e-8.
+int orc_pseudo_bp(const orc_view* views, int n, int nu, int nv, const orc_volume* vol,
+    const float* proj, double* volume, int flags)
+{
+    if (!valid_volume(vol) || !proj || !volume) return -1;
+    std::vector<Derived> g;
+    if (!derive(views, n, nu, nv, 6.28318530717958647692f, g)) return -2;
+    const bool tex = (flags & 1) != 0;
+    const orc_volume V = *vol;
+    const double cell = static_cast<double>(V.vox_x) * V.vox_y * V.vox_z / (g[0].du * g[0].dv);
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int z = 0; z < V.nz; ++z)
+        for (int y = 0; y < V.ny; ++y)
+            for (int x = 0; x < V.nx; ++x) {
+                const d3 P = md(vox_centre(x, V.nx, V.vox_x, V.center_x),
+                    vox_centre(y, V.ny, V.vox_y, V.center_y),
+                    vox_centre(z, V.nz, V.vox_z, V.center_z));
+                double acc = 0.0;
+                for (int i = 0; i < n; ++i) {
+                    const Derived& d = g[i];
+                    const d3 dir = subd(P, d.src);
+                    const double dn = dotd(dir, d.n);
+                    if (!(dn > 0.0)) continue;
+                    double u, v, depth;
+                    project_point(d, P, u, v, depth);
+                    const d3 hit = addd(d.detS, addd(scaled(d.detU, u), scaled(d.detV, v)));
+                    const d3 L = subd(hit, d.src);
+                    const double L2 = dotd(L, L), lsq = dotd(dir, dir);
+                    const double w = cell / std::fabs(d.plane) * L2 * std::sqrt(L2) / lsq;
+                    acc += w * bilerp_zero(proj + static_cast<size_t>(i) * nu * nv, nu, nv, u, v, tex);
+                }
+                volume[(static_cast<size_t>(z) * V.ny + y) * V.nx + x] = acc;
+            }
+    return 0;
+}
+
 int orc_fdk(const orc_view* views, int n, int nu, int nv, float range,
     const orc_volume* vol, const orc_filter* filter, const float* proj,
     double* volume_out, int flags)

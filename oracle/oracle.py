@@ -81,6 +81,7 @@ def lib():
             "orc_joseph_fp": [P, C.c_int, C.c_int, C.c_int, C.POINTER(Volume), P, P, C.c_int],
             "orc_joseph_bp": [P, C.c_int, C.c_int, C.c_int, C.POINTER(Volume), P, P],
             "orc_joseph_bp_refweight": [P, C.c_int, C.c_int, C.c_int, C.POINTER(Volume), P, P],
+            "orc_pseudo_bp": [P, C.c_int, C.c_int, C.c_int, C.POINTER(Volume), P, P, C.c_int],
             "orc_random_ellipsoids": [C.c_uint64, C.c_int, C.c_double, C.c_double, C.c_double,
                                       C.c_double, C.c_double, P],
             "orc_random_spheres": [C.c_uint64, C.c_int, C.c_double, C.c_double, C.c_double,
@@ -238,6 +239,15 @@ def joseph_bp(views, nu, nv, vol: Volume, proj, reference_weight=False) -> np.nd
     out = np.zeros((vol.nz, vol.ny, vol.nx), dtype=np.float64)
     fn = lib().orc_joseph_bp_refweight if reference_weight else lib().orc_joseph_bp
     _check(fn(_ptr(views), len(views), nu, nv, C.byref(vol), _ptr(proj), _ptr(out)), "joseph_bp")
+    return out
+
+
+def pseudo_bp(views, nu, nv, vol: Volume, proj, tex=False) -> np.ndarray:
+    """BP_FDK_PseudoMatched in FP64 (tex: 8-bit texture interpolation weights)."""
+    proj = np.ascontiguousarray(proj, dtype=np.float32)
+    out = np.zeros((vol.nz, vol.ny, vol.nx), dtype=np.float64)
+    _check(lib().orc_pseudo_bp(_ptr(views), len(views), nu, nv, C.byref(vol), _ptr(proj),
+                               _ptr(out), 1 if tex else 0), "pseudo_bp")
     return out
 
 

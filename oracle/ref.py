@@ -25,7 +25,7 @@ def _load():
     lib = C.CDLL(LIB)
     lib.ykref_last_error.restype = C.c_char_p
     for name in ("ykref_fdk", "ykref_fdk_stages", "ykref_fdk_time", "ykref_joseph_fp",
-                 "ykref_joseph_bp", "ykref_cgls"):
+                 "ykref_joseph_bp", "ykref_bp_pseudo", "ykref_cgls"):
         getattr(lib, name).restype = C.c_int
     return lib
 
@@ -81,7 +81,8 @@ def _child(op, scan_kw, grid_kw, filt_kw, paths, opts, q):
             x = np.ascontiguousarray(arrays[0], dtype=np.float32)
             out = np.zeros(nproj if op == "fp" else grid.shape, dtype=np.float32)
             ms = C.c_float(0.0)
-            fn = lib.ykref_joseph_fp if op == "fp" else lib.ykref_joseph_bp
+            fn = {"fp": lib.ykref_joseph_fp, "bp": lib.ykref_joseph_bp,
+                  "bp_pseudo": lib.ykref_bp_pseudo}[op]
             rc = fn(C.byref(s), C.byref(v), _fp(x), _fp(out), C.c_int(opts.get("warmup", 0)),
                     C.c_int(opts.get("reps", 0)), C.byref(ms), dev)
             res = (out, ms.value)
@@ -149,6 +150,11 @@ def cgls(scan, grid, proj, n_iter, matched=True, timeout=900):
 def joseph_fp(scan, grid, volume, warmup=0, reps=0):
     """Reference FP_Joseph: (projections, ms per call when reps > 0)."""
     return _run("fp", scan, grid, None, [volume], warmup=warmup, reps=reps)
+
+
+def bp_pseudo(scan, grid, proj, warmup=0, reps=0):
+    """Reference BP_FDK_PseudoMatched (clear volume): (volume, ms per call when reps > 0)."""
+    return _run("bp_pseudo", scan, grid, None, [proj], warmup=warmup, reps=reps)
 
 
 def joseph_bp(scan, grid, proj, warmup=0, reps=0):

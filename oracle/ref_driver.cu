@@ -271,7 +271,7 @@ int joseph(int mode, const ykb_circular_flat* scan, const ykb_volume* volume, co
         fp = YK::makeForwardOperator(YK::ETask::FP_Joseph);
         if (!fp->prepare(geometry, resources)) return fail("ForwardOperator::prepare");
     } else {
-        bp = YK::makeBackOperator(YK::ETask::BP_Joseph);
+        bp = YK::makeBackOperator(mode == 2 ? YK::ETask::BP_FDK_PseudoMatched : YK::ETask::BP_Joseph);
         if (!bp->prepare(geometry, resources)) return fail("BackOperator::prepare");
     }
     auto apply = [&]() {
@@ -363,6 +363,15 @@ __attribute__((visibility("default"))) int ykref_joseph_bp(const ykb_circular_fl
     int device)
 {
     return joseph(1, scan, volume, h_proj, h_vol, warmup, reps, ms, device);
+}
+
+// BackOperator with BP_FDK_PseudoMatched (src/common/YkProjectionOperators.hpp:
+// 324-333), clear volume; arguments as ykref_joseph_bp.
+__attribute__((visibility("default"))) int ykref_bp_pseudo(const ykb_circular_flat* scan,
+    const ykb_volume* volume, const float* h_proj, float* h_vol, int warmup, int reps, float* ms,
+    int device)
+{
+    return joseph(2, scan, volume, h_proj, h_vol, warmup, reps, ms, device);
 }
 
 } // extern "C"

@@ -178,3 +178,43 @@ def test_write_modes(cuda_device):
     v3 = torch.full_like(v1, 7.0)
     plan.adjoint(y, out=v3, accumulate=False)
     assert torch.equal(v3, v1)
+
+
+@pytest.mark.parametrize("path", ["tma", "global"])
+@pytest.mark.parametrize("case_fn", [K.c1_small, K.odd_case])
+def test_pseudo_bp_matches_oracle(oracle, cuda_device, monkeypatch, case_fn, path):
+    # BP_FDK_PseudoMatched through ykb_operator_apply: the TMA-staged tap-pair
+    # kernel and the bounds-checked fallback against the FP64 restatement
+    import torch
+    from fdk_cuda_impl_b200 import _lib as L
+    if path == "global":
+        monkeypatch.setenv("YKB_PSEUDO_BP_GLOBAL", "1")
+    case = case_fn()
+    views, plan = _plan(case)
+    y = oracle.normal(plan.proj_shape, 13)
+    yd = torch.from_numpy(y).cuda()
+    got = plan.backproject_pseudo(yd)
+    plan.check()
+    ref = oracle.pseudo_bp(views, case.scan.channels, case.scan.rows,
+                           K.oracle_volume(oracle, case.grid), y)
+    assert K.rel_rmse(got.cpu().numpy(), ref) <= 2e-5
+    # accumulate, and the task value of YK::ETask
+    acc = plan.apply(L.TASK_BP_FDK_PSEUDO_MATCHED, yd, got.clone(), accumulate=True)
+    assert K.rel_rmse(acc.cpu().numpy(), 2 * ref) <= 2e-5
+    plan.close()
+
+
+def test_operator_apply_tasks(oracle, cuda_device):
+    import torch
+    from fdk_cuda_impl_b200 import _lib as L
+    case = K.c1_small()
+    views, plan = _plan(case)
+    x = torch.from_numpy(K.phantom(oracle, case)).cuda()
+    assert torch.equal(plan.apply(L.TASK_FP_JOSEPH, x), plan.forward(x))
+    y = plan.forward(x)
+    assert torch.equal(plan.apply(L.TASK_BP_JOSEPH, y), plan.adjoint(y))
+    for task in (0, 2, 4, 6, 99):
+        with pytest.raises(L.YkbError) as e:
+            plan.apply(task, y)
+        assert e.value.code == L.ERR_UNSUPPORTED
+    plan.close()

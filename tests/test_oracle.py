@@ -254,3 +254,28 @@ def test_short_scan_fdk_matches_full_scan(oracle):
     # without the weights the short scan is visibly wrong
     plain = oracle.fdk(sv, 96, 64, short.scan.scan_range, vol, filt, ps)
     assert K.rel_rmse(plain, ref) > 2 * K.rel_rmse(rec, ref)
+
+
+@pytest.mark.parametrize("smooth", [False, True])
+def test_pseudo_bp_transposes_the_projector_on_smooth_data(oracle, smooth):
+    # BP_FDK_PseudoMatched weights each voxel by the ray density of the
+    # line-integral projector (voxel volume x L^3 / (|P-S|^2 SDD_plane du dv)),
+    # so it is the transpose of the Joseph projector up to the interpolation
+    # kernel: on slowly varying data <A x, y> = <x, B y> to a few 1e-4.
+    from tests import cases as K
+    case = K.c1_small()
+    views = case.scan.views()
+    nu, nv = case.scan.channels, case.scan.rows
+    vol = K.oracle_volume(oracle, case.grid)
+    x = oracle.uniform(case.grid.shape, 0.0, 1.0, 5)
+    if smooth:
+        u = np.arange(nu)[None, None, :] / nu
+        v = np.arange(nv)[None, :, None] / nv
+        k = np.arange(len(views))[:, None, None] / len(views)
+        y = (1.0 + 0.3 * np.cos(np.pi * u) * np.sin(np.pi * v) + 0.2 * np.cos(2 * np.pi * k))
+        y = np.ascontiguousarray(np.broadcast_to(y, (len(views), nv, nu)), dtype=np.float32)
+    else:
+        y = np.ones((len(views), nv, nu), dtype=np.float32)
+    lhs = float((oracle.joseph_fp(views, nu, nv, vol, x) * y).sum())
+    rhs = float((x * oracle.pseudo_bp(views, nu, nv, vol, y)).sum())
+    assert abs(lhs - rhs) / abs(lhs) < 2e-3
