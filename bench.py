@@ -221,7 +221,11 @@ def joseph_step(local: int, steps: int, warmup: int, timed_fn):
     pseudo = plan.backproject_pseudo(b)
     pseudo_ms = timed_fn(lambda: plan.backproject_pseudo(b, pseudo), steps)
     plan.check()
-    del pseudo
+    # the Siddon pair (FP_Siddon, BP_Siddon_RayDriven)
+    sfp = plan.forward_siddon(x.detach())
+    siddon_fp_ms = timed_fn(lambda: plan.forward_siddon(x.detach(), sfp), steps)
+    siddon_bp_ms = timed_fn(lambda: plan.backproject_siddon(b, pseudo), steps)
+    del pseudo, sfp
     with torch.no_grad():
         ax = plan.forward(x.detach())
         aty = plan.adjoint(b)
@@ -234,7 +238,8 @@ def joseph_step(local: int, steps: int, warmup: int, timed_fn):
             "samples_per_op": samples, "fp_gsamples": samples / (fp_ms * 1e-3) / 1e9,
             "bp_gsamples": samples / (bp_ms * 1e-3) / 1e9,
             "bp_pseudo_matched_ms": pseudo_ms,
-            "bp_pseudo_matched_gups": J_VOX ** 3 * J_VIEWS / (pseudo_ms * 1e-3) / 1e9}
+            "bp_pseudo_matched_gups": J_VOX ** 3 * J_VIEWS / (pseudo_ms * 1e-3) / 1e9,
+            "siddon_fp_ms": siddon_fp_ms, "siddon_bp_ms": siddon_bp_ms}
 
 
 def make_workload(rank: int, local: int):
@@ -315,13 +320,16 @@ def run_reference(args):
         _, fp_ms = R.joseph_fp(jscan, jgrid, jx, warmup=args.warmup, reps=args.steps)
         _, bp_ms = R.joseph_bp(jscan, jgrid, jy, warmup=args.warmup, reps=args.steps)
         _, pseudo_ms = R.bp_pseudo(jscan, jgrid, jy, warmup=args.warmup, reps=args.steps)
+        _, siddon_fp_ms = R.siddon_fp(jscan, jgrid, jx, warmup=args.warmup, reps=args.steps)
+        _, siddon_bp_ms = R.siddon_bp(jscan, jgrid, jy, warmup=args.warmup, reps=args.steps)
         samples = J_VIEWS * J_DET * J_DET * J_VOX
         joseph = {"workload": f"joseph-{J_VOX}^3-{J_VIEWS}v-{J_DET}^2", "fp_ms": fp_ms,
                   "bp_ms": bp_ms, "grad_step_ms": fp_ms + bp_ms,
                   "fp_gsamples": samples / (fp_ms * 1e-3) / 1e9,
                   "bp_gsamples": samples / (bp_ms * 1e-3) / 1e9,
                   "bp_pseudo_matched_ms": pseudo_ms,
-                  "bp_pseudo_matched_gups": J_VOX ** 3 * J_VIEWS / (pseudo_ms * 1e-3) / 1e9}
+                  "bp_pseudo_matched_gups": J_VOX ** 3 * J_VIEWS / (pseudo_ms * 1e-3) / 1e9,
+                  "siddon_fp_ms": siddon_fp_ms, "siddon_bp_ms": siddon_bp_ms}
         line.update({
             "value": value, "ms_per_step": ms_dev, "dtype": "f32",
             "config": dict(cfg, implementation="reference CUDA build (YKCBCT FdkPipeline, "

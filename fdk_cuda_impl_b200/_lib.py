@@ -97,6 +97,8 @@ SIGNATURES = {
 
 # ykb_task == YK::ETask values
 TASK_FP_JOSEPH = 1
+TASK_FP_SIDDON = 2
+TASK_BP_SIDDON_RAY_DRIVEN = 4
 TASK_BP_FDK_PSEUDO_MATCHED = 7
 TASK_BP_JOSEPH = 8
 

@@ -597,7 +597,8 @@ YKB_API size_t ykb_joseph_workspace_bytes(const ykb_joseph_plan* p)
 {
     if (!p) return 0;
     return p->views.bytes + p->view_proj.bytes + p->rays.bytes + p->lens.bytes +
-        p->weighted.bytes + p->slab_x.bytes + p->slab_y.bytes + p->fdk_coef.bytes +
+        p->weighted.bytes + p->slab_x.bytes + p->slab_y.bytes + p->world_views.bytes +
+        p->fdk_coef.bytes +
         p->pseudo_coef.bytes + p->pairs.bytes + p->err_flag.bytes;
 }
 
@@ -694,6 +695,29 @@ ykb_status pseudo_bp(ykb_joseph_plan* p, const float* d_proj, float* d_volume, i
     return YKB_OK;
 }
 
+ykb_status siddon(ykb_joseph_plan* p, bool forward, const float* d_in, float* d_out,
+    int accumulate, cudaStream_t s)
+{
+    if (!p->world_views.ptr) {
+        const size_t bytes = sizeof(ykb_cone_view) * p->cone_views.size();
+        cudaError_t e = p->world_views.alloc(bytes);
+        if (e != cudaSuccess) return cuda_status(e, "cudaMalloc (Siddon views)");
+        e = cudaMemcpyAsync(p->world_views.ptr, p->cone_views.data(), bytes, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) {
+            p->world_views.reset();
+            return cuda_status(e, "cudaMemcpy (Siddon views)");
+        }
+    }
+    const VolumeGrid g = make_grid(p->volume);
+    const ykb_cone_view* v = p->world_views.as<ykb_cone_view>();
+    if (forward)
+        YKB_TRY_CUDA(launch_siddon_fp(d_in, v, p->n_views, p->nu, p->nv, g, d_out, accumulate, s));
+    else
+        YKB_TRY_CUDA(launch_siddon_bp(d_in, v, p->n_views, p->nu, p->nv, g, d_out, accumulate, s));
+    return YKB_OK;
+}
+
 } // namespace
 
 extern "C" {
@@ -706,6 +730,13 @@ YKB_API ykb_status ykb_operator_apply(ykb_joseph_plan* p, int task, const float*
     switch (task) {
     case YKB_TASK_FP_JOSEPH: return ykb_joseph_fp(p, d_in, d_out, accumulate, stream);
     case YKB_TASK_BP_JOSEPH: return ykb_joseph_bp(p, d_in, d_out, accumulate, stream);
+    case YKB_TASK_FP_SIDDON:
+    case YKB_TASK_BP_SIDDON_RAY_DRIVEN: {
+        if (!d_in || !d_out) return fail(YKB_ERR_INVALID_BUFFER, "null volume or projection buffer");
+        DeviceGuard guard(p->device);
+        return siddon(p, task == YKB_TASK_FP_SIDDON, d_in, d_out, accumulate ? 1 : 0,
+            reinterpret_cast<cudaStream_t>(stream));
+    }
     case YKB_TASK_BP_FDK_PSEUDO_MATCHED: {
         if (!d_in || !d_out) return fail(YKB_ERR_INVALID_BUFFER, "null volume or projection buffer");
         DeviceGuard guard(p->device);

@@ -233,6 +233,11 @@ cudaError_t launch_joseph_fp(const float* slabs[3], const JosephView* views,
     int accumulate, cudaStream_t s);
 cudaError_t launch_joseph_ray_table(const JosephView* views, int n_views,
     int nu, int nv, float4* rays, float* lens, cudaStream_t s);
+// Siddon (siddon_kernels.cu); views in world coordinates
+cudaError_t launch_siddon_fp(const float* vol, const ykb_cone_view* views, int n_views, int nu,
+    int nv, const VolumeGrid& g, float* proj, int accumulate, cudaStream_t s);
+cudaError_t launch_siddon_bp(const float* proj, const ykb_cone_view* views, int n_views, int nu,
+    int nv, const VolumeGrid& g, float* vol, int accumulate, cudaStream_t s);
 cudaError_t launch_joseph_bp(const float* proj, const float4* rays, const float* lens,
     const float* view_proj, const JosephView* views, int n_views, int nu, int nv,
     const ykb_volume& vol, float* weighted, float* out, int accumulate, cudaStream_t s);
@@ -291,6 +296,7 @@ struct ykb_joseph_plan {
     ykb::DeviceBuffer lens;      // float[n*nv*nu]: chord length per step
     ykb::DeviceBuffer weighted;  // float[n*nv*nu]: backprojector input x chord length
     ykb::DeviceBuffer slab_y, slab_x;  // transposed volume copies
+    ykb::DeviceBuffer world_views;     // ykb_cone_view[n] (Siddon), uploaded on first use
     // pseudo-matched backprojection, set up on first use
     bool pseudo_ready = false;
     bool pseudo_axial = false;         // untilted detector: the axial column walk

@@ -206,10 +206,23 @@ class JosephPlan:
         (src/FlatFpBp/BP/kernels/YkBpFdkKernel.cu:356-450)."""
         return self.apply(L.TASK_BP_FDK_PSEUDO_MATCHED, proj, out, accumulate)
 
+    def forward_siddon(self, volume: torch.Tensor, out: torch.Tensor | None = None,
+                       accumulate: bool = False) -> torch.Tensor:
+        """FP_Siddon: exact voxel intersection lengths of each source-to-pixel
+        ray (src/FlatFpBp/FP/kernels/YkFPSiddonKernel.cu:19-129)."""
+        return self.apply(L.TASK_FP_SIDDON, volume, out, accumulate)
+
+    def backproject_siddon(self, proj: torch.Tensor, out: torch.Tensor | None = None,
+                           accumulate: bool = False) -> torch.Tensor:
+        """BP_Siddon_RayDriven: the exact transpose of forward_siddon
+        (src/FlatFpBp/BP/kernels/YkBPSiddonKernel.cu:31-127), summed with
+        atomics (last bits vary between runs)."""
+        return self.apply(L.TASK_BP_SIDDON_RAY_DRIVEN, proj, out, accumulate)
+
     def apply(self, task: int, x: torch.Tensor, out: torch.Tensor | None = None,
               accumulate: bool = False) -> torch.Tensor:
         """One operator task (ykb_operator_apply; task values of YK::ETask)."""
-        forward = task == L.TASK_FP_JOSEPH
+        forward = task in (L.TASK_FP_JOSEPH, L.TASK_FP_SIDDON)
         in_shape, out_shape = ((self.grid.shape, self.proj_shape) if forward
                                else (self.proj_shape, self.grid.shape))
         _check_tensor(x, in_shape, (torch.float32,), self.device, "input")

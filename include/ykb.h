@@ -260,6 +260,8 @@ YKB_API ykb_status ykb_joseph_bp(ykb_joseph_plan* plan, const float* d_proj,
  * (src/common/YkOperatorTypes.hpp:5-22) that this library implements. */
 typedef enum ykb_task {
     YKB_TASK_FP_JOSEPH = 1,
+    YKB_TASK_FP_SIDDON = 2,
+    YKB_TASK_BP_SIDDON_RAY_DRIVEN = 4,
     YKB_TASK_BP_FDK_PSEUDO_MATCHED = 7,
     YKB_TASK_BP_JOSEPH = 8
 } ykb_task;
@@ -270,6 +272,13 @@ typedef enum ykb_task {
  * Replaces IForwardOperator/IBackOperator::apply for the task
  * (src/common/YkProjectionOperators.hpp:138-180,242-340).
  *   YKB_TASK_FP_JOSEPH, YKB_TASK_BP_JOSEPH: ykb_joseph_fp, ykb_joseph_bp.
+ *   YKB_TASK_FP_SIDDON, YKB_TASK_BP_SIDDON_RAY_DRIVEN: the Siddon pair,
+ *     exact intersection lengths of the source-to-pixel-centre ray with each
+ *     voxel (fp_siddon_launch, src/FlatFpBp/FP/kernels/YkFPSiddonKernel.cu:
+ *     19-129,283-316; bp_siddon_launch, src/FlatFpBp/BP/kernels/
+ *     YkBPSiddonKernel.cu:31-160).  The backprojector is the exact transpose
+ *     of the projector; it sums with global atomics, so its last bits vary
+ *     between runs.
  *   YKB_TASK_BP_FDK_PSEUDO_MATCHED: voxel-driven bilinear backprojection
  *     with the weight L^3 / (|P - S|^2 SDD_plane) x voxel volume / pixel
  *     area (fdk_pseudo_matched_bp_launch, src/FlatFpBp/BP/kernels/

@@ -461,6 +461,59 @@ long poisson(std::mt19937_64& g, double mu)
 
 } // namespace
 
+namespace {
+template <typename F>
+void siddon_ray(const orc_view& vw, int iu, int iv, const orc_volume& V, F&& f)
+{
+    const double S[3] = {vw.src[0], vw.src[1], vw.src[2]};
+    double r[3], lo[3], vox[3];
+    const int N[3] = {V.nx, V.ny, V.nz};
+    const double c[3] = {V.center_x, V.center_y, V.center_z};
+    vox[0] = V.vox_x; vox[1] = V.vox_y; vox[2] = V.vox_z;
+    for (int a = 0; a < 3; ++a) {
+        const double D = static_cast<double>(vw.detS[a]) + iu * static_cast<double>(vw.detU[a]) +
+            iv * static_cast<double>(vw.detV[a]);
+        r[a] = D - S[a];
+        lo[a] = c[a] - 0.5 * (N[a] - 1) * vox[a] - 0.5 * vox[a];
+    }
+    const double len = std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+    double tmin = 0.0, tmax = 1.0;
+    for (int a = 0; a < 3; ++a) {
+        const double hi = lo[a] + N[a] * vox[a];
+        if (std::fabs(r[a]) > 1e-8) {
+            double ta = (lo[a] - S[a]) / r[a], tb = (hi - S[a]) / r[a];
+            if (ta > tb) std::swap(ta, tb);
+            tmin = std::max(tmin, ta);
+            tmax = std::min(tmax, tb);
+        } else if (S[a] < lo[a] || S[a] > hi) {
+            return;
+        }
+    }
+    if (!(tmin < tmax)) return;
+    std::vector<double> ts{tmin, tmax};
+    for (int a = 0; a < 3; ++a) {
+        if (!(std::fabs(r[a]) > 1e-8)) continue;
+        for (int k = 0; k <= N[a]; ++k) {
+            const double t = (lo[a] + k * vox[a] - S[a]) / r[a];
+            if (t > tmin && t < tmax) ts.push_back(t);
+        }
+    }
+    std::sort(ts.begin(), ts.end());
+    for (size_t q = 0; q + 1 < ts.size(); ++q) {
+        const double t0 = ts[q], t1 = ts[q + 1];
+        if (!(t1 > t0)) continue;
+        const double tm = 0.5 * (t0 + t1);
+        long idx[3];
+        bool in = true;
+        for (int a = 0; a < 3; ++a) {
+            idx[a] = static_cast<long>(std::floor((S[a] + tm * r[a] - lo[a]) / vox[a]));
+            in = in && idx[a] >= 0 && idx[a] < N[a];
+        }
+        if (in) f((idx[2] * V.ny + idx[1]) * V.nx + idx[0], (t1 - t0) * len);
+    }
+}
+} // namespace
+
 extern "C" {
 
 int orc_num_threads(void)
@@ -723,6 +776,56 @@ int orc_fdk_backproject(const orc_view* views, int n, int nu, int nv,
                 }
                 volume[(static_cast<size_t>(z) * V.ny + y) * V.nx + x] += acc;
             }
+    return 0;
+}
+
+// Siddon pair: FP_Siddon (siddon_fp_tex_kernel with a Point/Border texture,
+// src/FlatFpBp/FP/kernels/YkFPSiddonKernel.cu:129-234,283-316, applied by
+// ForwardOperator::apply, src/common/YkProjectionOperators.hpp:159-171) and
+// BP_Siddon_RayDriven (siddon_bp_kernel, src/FlatFpBp/BP/kernels/
+// YkBPSiddonKernel.cu:31-127).  The ray S + t (D - S) from the source to the
+// pixel centre D, t in [0, 1] clipped to the outer voxel faces, contributes
+// vol[voxel] x (length of the ray inside the voxel) -- here computed by
+// Siddon's original parametric method: every face crossing in the clipped
+// range, sorted, each interval assigned to the voxel holding its midpoint.
+
+int orc_siddon_fp(const orc_view* views, int n, int nu, int nv, const orc_volume* vol,
+    const float* volume, double* proj)
+{
+    if (!valid_volume(vol) || !views || !volume || !proj) return -1;
+    const orc_volume V = *vol;
+#pragma omp parallel for collapse(2) schedule(dynamic, 4)
+    for (int k = 0; k < n; ++k)
+        for (int iv = 0; iv < nv; ++iv)
+            for (int iu = 0; iu < nu; ++iu) {
+                double acc = 0.0;
+                siddon_ray(views[k], iu, iv, V, [&](long i, double l) { acc += volume[i] * l; });
+                proj[(static_cast<size_t>(k) * nv + iv) * nu + iu] = acc;
+            }
+    return 0;
+}
+
+int orc_siddon_bp(const orc_view* views, int n, int nu, int nv, const orc_volume* vol,
+    const float* proj, double* volume)
+{
+    if (!valid_volume(vol) || !views || !volume || !proj) return -1;
+    const orc_volume V = *vol;
+    const size_t nvox = static_cast<size_t>(V.nx) * V.ny * V.nz;
+    std::fill(volume, volume + nvox, 0.0);
+    // per-thread partial volumes keep the sum deterministic
+#pragma omp parallel
+    {
+        std::vector<double> part(nvox, 0.0);
+#pragma omp for collapse(2) schedule(static)
+        for (int k = 0; k < n; ++k)
+            for (int iv = 0; iv < nv; ++iv)
+                for (int iu = 0; iu < nu; ++iu) {
+                    const double p = proj[(static_cast<size_t>(k) * nv + iv) * nu + iu];
+                    siddon_ray(views[k], iu, iv, V, [&](long i, double l) { part[i] += p * l; });
+                }
+#pragma omp critical
+        for (size_t i = 0; i < nvox; ++i) volume[i] += part[i];
+    }
     return 0;
 }
 

@@ -82,6 +82,8 @@ def lib():
             "orc_joseph_bp": [P, C.c_int, C.c_int, C.c_int, C.POINTER(Volume), P, P],
             "orc_joseph_bp_refweight": [P, C.c_int, C.c_int, C.c_int, C.POINTER(Volume), P, P],
             "orc_pseudo_bp": [P, C.c_int, C.c_int, C.c_int, C.POINTER(Volume), P, P, C.c_int],
+            "orc_siddon_fp": [P, C.c_int, C.c_int, C.c_int, C.POINTER(Volume), P, P],
+            "orc_siddon_bp": [P, C.c_int, C.c_int, C.c_int, C.POINTER(Volume), P, P],
             "orc_random_ellipsoids": [C.c_uint64, C.c_int, C.c_double, C.c_double, C.c_double,
                                       C.c_double, C.c_double, P],
             "orc_random_spheres": [C.c_uint64, C.c_int, C.c_double, C.c_double, C.c_double,
@@ -239,6 +241,22 @@ def joseph_bp(views, nu, nv, vol: Volume, proj, reference_weight=False) -> np.nd
     out = np.zeros((vol.nz, vol.ny, vol.nx), dtype=np.float64)
     fn = lib().orc_joseph_bp_refweight if reference_weight else lib().orc_joseph_bp
     _check(fn(_ptr(views), len(views), nu, nv, C.byref(vol), _ptr(proj), _ptr(out)), "joseph_bp")
+    return out
+
+
+def siddon_fp(views, nu, nv, vol: Volume, volume) -> np.ndarray:
+    volume = np.ascontiguousarray(volume, dtype=np.float32)
+    out = np.zeros((len(views), nv, nu), dtype=np.float64)
+    _check(lib().orc_siddon_fp(_ptr(views), len(views), nu, nv, C.byref(vol), _ptr(volume),
+                               _ptr(out)), "siddon_fp")
+    return out
+
+
+def siddon_bp(views, nu, nv, vol: Volume, proj) -> np.ndarray:
+    proj = np.ascontiguousarray(proj, dtype=np.float32)
+    out = np.zeros((vol.nz, vol.ny, vol.nx), dtype=np.float64)
+    _check(lib().orc_siddon_bp(_ptr(views), len(views), nu, nv, C.byref(vol), _ptr(proj),
+                               _ptr(out)), "siddon_bp")
     return out
 
 

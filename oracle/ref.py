@@ -25,7 +25,8 @@ def _load():
     lib = C.CDLL(LIB)
     lib.ykref_last_error.restype = C.c_char_p
     for name in ("ykref_fdk", "ykref_fdk_stages", "ykref_fdk_time", "ykref_joseph_fp",
-                 "ykref_joseph_bp", "ykref_bp_pseudo", "ykref_cgls"):
+                 "ykref_joseph_bp", "ykref_bp_pseudo", "ykref_siddon_fp", "ykref_siddon_bp",
+                 "ykref_cgls"):
         getattr(lib, name).restype = C.c_int
     return lib
 
@@ -79,10 +80,11 @@ def _child(op, scan_kw, grid_kw, filt_kw, paths, opts, q):
             res = (ms[0], ms[1])
         else:
             x = np.ascontiguousarray(arrays[0], dtype=np.float32)
-            out = np.zeros(nproj if op == "fp" else grid.shape, dtype=np.float32)
+            out = np.zeros(nproj if op in ("fp", "siddon_fp") else grid.shape, dtype=np.float32)
             ms = C.c_float(0.0)
             fn = {"fp": lib.ykref_joseph_fp, "bp": lib.ykref_joseph_bp,
-                  "bp_pseudo": lib.ykref_bp_pseudo}[op]
+                  "bp_pseudo": lib.ykref_bp_pseudo, "siddon_fp": lib.ykref_siddon_fp,
+                  "siddon_bp": lib.ykref_siddon_bp}[op]
             rc = fn(C.byref(s), C.byref(v), _fp(x), _fp(out), C.c_int(opts.get("warmup", 0)),
                     C.c_int(opts.get("reps", 0)), C.byref(ms), dev)
             res = (out, ms.value)
@@ -150,6 +152,16 @@ def cgls(scan, grid, proj, n_iter, matched=True, timeout=900):
 def joseph_fp(scan, grid, volume, warmup=0, reps=0):
     """Reference FP_Joseph: (projections, ms per call when reps > 0)."""
     return _run("fp", scan, grid, None, [volume], warmup=warmup, reps=reps)
+
+
+def siddon_fp(scan, grid, volume, warmup=0, reps=0):
+    """Reference FP_Siddon: (projections, ms per call when reps > 0)."""
+    return _run("siddon_fp", scan, grid, None, [volume], warmup=warmup, reps=reps)
+
+
+def siddon_bp(scan, grid, proj, warmup=0, reps=0):
+    """Reference BP_Siddon_RayDriven (clear volume): (volume, ms per call when reps > 0)."""
+    return _run("siddon_bp", scan, grid, None, [proj], warmup=warmup, reps=reps)
 
 
 def bp_pseudo(scan, grid, proj, warmup=0, reps=0):

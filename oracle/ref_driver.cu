@@ -260,23 +260,27 @@ int joseph(int mode, const ykb_circular_flat* scan, const ykb_volume* volume, co
     resources.attach(stream.s, device);
     const size_t nvox = size_t(volume->nx) * volume->ny * volume->nz;
     const size_t nproj = size_t(scan->channels) * scan->rows * scan->total_views;
-    const size_t n_in = mode == 0 ? nvox : nproj, n_out = mode == 0 ? nproj : nvox;
+    // mode: 0 FP_Joseph, 1 BP_Joseph, 2 BP_FDK_PseudoMatched, 3 FP_Siddon,
+    // 4 BP_Siddon_RayDriven
+    const bool forward = mode == 0 || mode == 3;
+    const size_t n_in = forward ? nvox : nproj, n_out = forward ? nproj : nvox;
     Dev<float> d_in(n_in), d_out(n_out);
     if (!d_in.p || !d_out.p) return fail("cudaMalloc");
     if (cudaMemcpy(d_in.p, h_in, n_in * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess)
         return fail("cudaMemcpy input");
     std::unique_ptr<YK::IForwardOperator> fp;
     std::unique_ptr<YK::IBackOperator> bp;
-    if (mode == 0) {
-        fp = YK::makeForwardOperator(YK::ETask::FP_Joseph);
+    if (forward) {
+        fp = YK::makeForwardOperator(mode == 3 ? YK::ETask::FP_Siddon : YK::ETask::FP_Joseph);
         if (!fp->prepare(geometry, resources)) return fail("ForwardOperator::prepare");
     } else {
-        bp = YK::makeBackOperator(mode == 2 ? YK::ETask::BP_FDK_PseudoMatched : YK::ETask::BP_Joseph);
+        bp = YK::makeBackOperator(mode == 2 ? YK::ETask::BP_FDK_PseudoMatched
+            : mode == 4 ? YK::ETask::BP_Siddon_RayDriven : YK::ETask::BP_Joseph);
         if (!bp->prepare(geometry, resources)) return fail("BackOperator::prepare");
     }
     auto apply = [&]() {
-        return mode == 0 ? fp->apply(d_in.p, geometry.base(), d_out.p, resources)
-                         : bp->apply(d_in.p, geometry.base(), d_out.p, true, resources);
+        return forward ? fp->apply(d_in.p, geometry.base(), d_out.p, resources)
+                       : bp->apply(d_in.p, geometry.base(), d_out.p, true, resources);
     };
     if (!apply()) return fail("operator apply");
     if (cudaStreamSynchronize(stream.s) != cudaSuccess) return fail("operator execution");
@@ -363,6 +367,23 @@ __attribute__((visibility("default"))) int ykref_joseph_bp(const ykb_circular_fl
     int device)
 {
     return joseph(1, scan, volume, h_proj, h_vol, warmup, reps, ms, device);
+}
+
+// ForwardOperator with FP_Siddon and BackOperator with BP_Siddon_RayDriven
+// (src/common/YkProjectionOperators.hpp:159-171,262-270); arguments as
+// ykref_joseph_fp / ykref_joseph_bp.
+__attribute__((visibility("default"))) int ykref_siddon_fp(const ykb_circular_flat* scan,
+    const ykb_volume* volume, const float* h_vol, float* h_proj, int warmup, int reps, float* ms,
+    int device)
+{
+    return joseph(3, scan, volume, h_vol, h_proj, warmup, reps, ms, device);
+}
+
+__attribute__((visibility("default"))) int ykref_siddon_bp(const ykb_circular_flat* scan,
+    const ykb_volume* volume, const float* h_proj, float* h_vol, int warmup, int reps, float* ms,
+    int device)
+{
+    return joseph(4, scan, volume, h_proj, h_vol, warmup, reps, ms, device);
 }
 
 // BackOperator with BP_FDK_PseudoMatched (src/common/YkProjectionOperators.hpp:

@@ -213,8 +213,36 @@ def test_operator_apply_tasks(oracle, cuda_device):
     assert torch.equal(plan.apply(L.TASK_FP_JOSEPH, x), plan.forward(x))
     y = plan.forward(x)
     assert torch.equal(plan.apply(L.TASK_BP_JOSEPH, y), plan.adjoint(y))
-    for task in (0, 2, 4, 6, 99):
+    for task in (0, 3, 5, 6, 99):
         with pytest.raises(L.YkbError) as e:
             plan.apply(task, y)
         assert e.value.code == L.ERR_UNSUPPORTED
+    plan.close()
+
+
+@pytest.mark.parametrize("case_fn", [K.c1_small, K.odd_case])
+def test_siddon_pair_matches_oracle(oracle, cuda_device, case_fn):
+    # FP_Siddon / BP_Siddon_RayDriven against the FP64 parametric Siddon, the
+    # FP64 dot-product test, and accumulate
+    import torch
+    case = case_fn()
+    views, plan = _plan(case)
+    nu, nv = case.scan.channels, case.scan.rows
+    vol = K.oracle_volume(oracle, case.grid)
+    x = K.phantom(oracle, case)
+    xd = torch.from_numpy(x).cuda()
+    fp = plan.forward_siddon(xd)
+    assert K.rel_rmse(fp.cpu().numpy(), oracle.siddon_fp(views, nu, nv, vol, x)) <= FP32_TOL
+    y = oracle.normal(plan.proj_shape, 17)
+    yd = torch.from_numpy(y).cuda()
+    bp = plan.backproject_siddon(yd)
+    assert K.rel_rmse(bp.cpu().numpy(), oracle.siddon_bp(views, nu, nv, vol, y)) <= FP32_TOL
+    r = torch.from_numpy(oracle.uniform(case.grid.shape, 0.0, 1.0, 3)).cuda()
+    lhs = float((plan.forward_siddon(r).double() * yd.double()).sum())
+    rhs = float((r.double() * bp.double()).sum())
+    assert abs(lhs - rhs) / abs(lhs) <= ADJ_TOL
+    two = plan.forward_siddon(xd, fp.clone(), accumulate=True)
+    assert torch.allclose(two, 2 * fp, rtol=1e-6, atol=1e-6)
+    bp2 = plan.backproject_siddon(yd, bp.clone(), accumulate=True)
+    assert K.rel_rmse(bp2.cpu().numpy(), 2 * bp.cpu().numpy()) <= 1e-6
     plan.close()

@@ -279,3 +279,41 @@ def test_pseudo_bp_transposes_the_projector_on_smooth_data(oracle, smooth):
     lhs = float((oracle.joseph_fp(views, nu, nv, vol, x) * y).sum())
     rhs = float((x * oracle.pseudo_bp(views, nu, nv, vol, y)).sum())
     assert abs(lhs - rhs) / abs(lhs) < 2e-3
+
+
+@pytest.mark.parametrize("case_fn", [K.c1_small, K.odd_case])
+def test_siddon_oracle_pins(oracle, case_fn):
+    # FP of a constant volume is the chord of the ray through the volume box
+    # (slab clipping in numpy, independent of the oracle's voxel walk); the
+    # backprojector is the exact transpose (the reference's Siddon adjoint
+    # error bound is 1e-4, unit_test/test_operator_benchmarks.cpp:978)
+    case = case_fn()
+    views = case.scan.views()
+    nu, nv = case.scan.channels, case.scan.rows
+    g = case.grid
+    vol = K.oracle_volume(oracle, g)
+    ones = np.ones(g.shape, dtype=np.float32)
+    got = oracle.siddon_fp(views, nu, nv, vol, ones)
+    n = np.array([g.nx, g.ny, g.nz], dtype=np.float64)
+    # the grid as the volume struct holds it (float members)
+    vox = np.array(g.voxel_mm, dtype=np.float32).astype(np.float64)
+    lo = np.array(g.center_mm, dtype=np.float32).astype(np.float64) - 0.5 * n * vox
+    hi = lo + n * vox
+    iu, iv = np.meshgrid(np.arange(nu), np.arange(nv))
+    chord = np.zeros((len(views), nv, nu))
+    for k, vw in enumerate(views):
+        s = vw["src"][:3].astype(np.float64)
+        d = (vw["detS"][:3].astype(np.float64) + iu[..., None] * vw["detU"][:3].astype(np.float64)
+             + iv[..., None] * vw["detV"][:3].astype(np.float64))
+        r = d - s
+        with np.errstate(divide="ignore", invalid="ignore"):
+            ta, tb = (lo - s) / r, (hi - s) / r
+        tmin = np.clip(np.max(np.minimum(ta, tb), axis=-1), 0.0, None)
+        tmax = np.clip(np.min(np.maximum(ta, tb), axis=-1), None, 1.0)
+        chord[k] = np.clip(tmax - tmin, 0.0, None) * np.linalg.norm(r, axis=-1)
+    assert np.abs(got - chord).max() <= 1e-9 * chord.max()
+    x = oracle.uniform(g.shape, 0.0, 1.0, 5)
+    y = oracle.normal((len(views), nv, nu), 6)
+    lhs = float((oracle.siddon_fp(views, nu, nv, vol, x) * y).sum())
+    rhs = float((x * oracle.siddon_bp(views, nu, nv, vol, y)).sum())
+    assert abs(lhs - rhs) <= 1e-12 * abs(lhs)

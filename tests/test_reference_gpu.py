@@ -282,3 +282,34 @@ def test_pseudo_bp_matches_reference(oracle, name):
         assert K.rel_rmse(r, o) <= tol_ref, (name, kind, "ref vs oracle")
         assert K.rel_rmse(ours, r) <= tol_ours, (name, kind, "ours vs ref")
     plan.close()
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_siddon_pair_matches_reference(oracle, name):
+    # FP_Siddon and BP_Siddon_RayDriven of the reference build against the FP64
+    # oracle and this build, on a constant volume, a phantom and a random
+    # sinogram.  The reference walks in FP32 with face crossings accumulated
+    # along the ray; the residuals are that drift.
+    import torch
+    case = CASES[name]()
+    sc = case.scan
+    views = sc.views()
+    vol = K.oracle_volume(oracle, case.grid)
+    plan = JosephPlan(views, sc.channels, sc.rows, case.grid)
+    for kind, x in (("ones", np.ones(case.grid.shape, dtype=np.float32)),
+                    ("phantom", K.phantom(oracle, case))):
+        r, _ = ref.siddon_fp(sc, case.grid, x)
+        o = oracle.siddon_fp(views, sc.channels, sc.rows, vol, x)
+        ours = plan.forward_siddon(torch.from_numpy(x).cuda()).cpu().numpy()
+        assert K.rel_rmse(r, o) <= SIDDON_REF_TOL, (name, kind, "ref vs oracle")
+        assert K.rel_rmse(ours, r) <= SIDDON_REF_TOL, (name, kind, "ours vs ref")
+    y = oracle.normal((sc.total_views, sc.rows, sc.channels), 23)
+    r, _ = ref.siddon_bp(sc, case.grid, y)
+    o = oracle.siddon_bp(views, sc.channels, sc.rows, vol, y)
+    ours = plan.backproject_siddon(torch.from_numpy(y).cuda()).cpu().numpy()
+    assert K.rel_rmse(r, o) <= SIDDON_REF_TOL, (name, "bp", "ref vs oracle")
+    assert K.rel_rmse(ours, r) <= SIDDON_REF_TOL, (name, "bp", "ours vs ref")
+    plan.close()
+
+
+SIDDON_REF_TOL = 1e-3
