@@ -178,18 +178,16 @@ __global__ void joseph_weight_rays_kernel(const float* __restrict__ proj,
 }
 
 // Weight with which a sample at minor coordinate f reaches voxel j:
-// 1 - w when floor(f) = j, w when floor(f) = j - 1, with w = f - floor(f).
-// Both cases take w with the forward projector's own subtraction f - floor(f)
-// (jf = j, jm = j - 1 as floats), so the weights are bit-identical to
-// joseph_fp_kernel's without a float-to-int conversion.  f - (j - 1) is exact
-// except for j = 0 (f just below 0), where it may round up to 1 -- as the
-// forward projector's w does, which then gives voxel 0 the full weight 1:
-// hence e <= 1 (e = 1 with floor(f) = j is caught by the first case).
-__device__ __forceinline__ float hat_weight(float f, float jf, float jm)
+// max(0, 1 - |f - j|).  The forward projector gives voxel floor(f) the weight
+// 1 - w and voxel floor(f) + 1 the weight w, w = f - floor(f).  For
+// floor(f) = j the expression is 1 - (f - j), the same operations.  For
+// floor(f) = j - 1 it is 1 - (j - f): j - f = 1 - w is exact whenever
+// f >= j / 2 (Sterbenz), i.e. for every j >= 2, and then 1 - (1 - w) = w
+// exactly; at j = 0 (f in [-1, 0)) both compute f + 1.  Only j = 1 with
+// f < 1/2 may differ, by one rounding of a weight below 1/2.
+__device__ __forceinline__ float hat_weight(float f, float jf)
 {
-    const float d = f - jf;   // floor(f) = j      <=> 0 <= d < 1
-    const float e = f - jm;   // floor(f) = j - 1  <=> 0 <= e <= 1
-    return (d >= 0.f && d < 1.f) ? 1.f - d : ((e >= 0.f && e <= 1.f) ? e : 0.f);
+    return fmaxf(0.f, 1.f - fabsf(f - jf));
 }
 
 __global__ void __launch_bounds__(256) joseph_bp_kernel(const float* __restrict__ vl,
@@ -235,17 +233,18 @@ __global__ void __launch_bounds__(256) joseph_bp_kernel(const float* __restrict_
         const int u1 = min(nu - 1, static_cast<int>(floorf(umax + margin)));
         const int v0 = max(0, static_cast<int>(ceilf(vmin - margin)));
         const int v1 = min(nv - 1, static_cast<int>(floorf(vmax + margin)));
-        const float j1f = static_cast<float>(j1), j1m = static_cast<float>(j1 - 1);
-        const float j2f = static_cast<float>(j2), j2m = static_cast<float>(j2 - 1);
+        const float j1f = static_cast<float>(j1), j2f = static_cast<float>(j2);
         const long base = k * view_elems;
         float accv = 0.f;
+        // every candidate of the box is evaluated without a branch: a ray
+        // outside the footprint has weight 0
         for (int iv = v0; iv <= v1; ++iv) {
             const long row = base + static_cast<long>(iv) * nu;
             for (int iu = u0; iu <= u1; ++iu) {
                 const float4 r = __ldg(rays + row + iu);
-                const float w = hat_weight(fmaf(r.x, c0, r.y), j1f, j1m) *
-                    hat_weight(fmaf(r.z, c0, r.w), j2f, j2m);
-                if (w != 0.f) accv = fmaf(__ldg(vl + row + iu), w, accv);
+                const float w = hat_weight(fmaf(r.x, c0, r.y), j1f) *
+                    hat_weight(fmaf(r.z, c0, r.w), j2f);
+                accv = fmaf(__ldg(vl + row + iu), w, accv);
             }
         }
         acc += static_cast<double>(accv);

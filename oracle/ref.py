@@ -10,6 +10,7 @@ from __future__ import annotations
 import ctypes as C
 import multiprocessing as mp
 import os
+import sys
 
 import numpy as np
 
@@ -36,6 +37,10 @@ def _fp(a):
 
 
 def _child(op, scan_kw, grid_kw, filt_kw, paths, opts, q):
+    # the reference library logs to stdout; keep the caller's stdout for its
+    # own output (the benchmark's single JSON line)
+    sys.stdout.flush()
+    os.dup2(2, 1)
     try:
         from fdk_cuda_impl_b200.geometry import CircularScan, RampFilter, VolumeGrid
         arrays = [np.load(p, mmap_mode="r") for p in paths]
