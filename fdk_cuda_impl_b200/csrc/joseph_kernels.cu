@@ -190,6 +190,43 @@ __device__ __forceinline__ float hat_weight(float f, float jf)
     return fmaxf(0.f, 1.f - fabsf(f - jf));
 }
 
+// Detector box of the slice rectangle [j1 - 1, j1 + 1] x [j2lo - 1, j2hi + 1]
+// (voxel-index coordinates on the minor axes of slice c0), from its four
+// projected corners, clipped to the detector; empty when u0 > u1 or v0 > v1.
+__device__ __forceinline__ void footprint_box(const ViewProj& m, const JosephView& j, float c0,
+    int j1, int j2lo, int j2hi, int nu, int nv, int& u0, int& u1, int& v0, int& v1)
+{
+    float umin = 1e30f, umax = -1e30f, vmin = 1e30f, vmax = -1e30f;
+#pragma unroll
+    for (int corner = 0; corner < 4; ++corner) {
+        const float q1 = static_cast<float>(j1 + ((corner & 1) ? 1 : -1)) - 0.5f * (j.n1 - 1);
+        const float q2 = static_cast<float>((corner & 2) ? j2hi + 1 : j2lo - 1) - 0.5f * (j.n2 - 1);
+        float px, py, pz;
+        if (j.axis == 0) { px = c0; py = q1; pz = q2; }
+        else if (j.axis == 1) { px = q1; py = c0; pz = q2; }
+        else { px = q1; py = q2; pz = c0; }
+        const float w = fmaf(m.m[8], px, fmaf(m.m[9], py, fmaf(m.m[10], pz, m.m[11])));
+        // the box only needs a few 1e-6 px: correctly rounded reciprocal
+        const float rw = __frcp_rn(w);
+        const float u = fmaf(m.m[0], px, fmaf(m.m[1], py, fmaf(m.m[2], pz, m.m[3]))) * rw;
+        const float v = fmaf(m.m[4], px, fmaf(m.m[5], py, fmaf(m.m[6], pz, m.m[7]))) * rw;
+        umin = fminf(umin, u); umax = fmaxf(umax, u);
+        vmin = fminf(vmin, v); vmax = fmaxf(vmax, v);
+    }
+    constexpr float margin = 0.05f;
+    u0 = max(0, static_cast<int>(ceilf(umin - margin)));
+    u1 = min(nu - 1, static_cast<int>(floorf(umax + margin)));
+    v0 = max(0, static_cast<int>(ceilf(vmin - margin)));
+    v1 = min(nv - 1, static_cast<int>(floorf(vmax + margin)));
+}
+
+// One thread gathers ZV voxels stacked along z.  When z is a minor axis of
+// the view (main axis x or y, every view of a circular orbit) the stack lies
+// in one slice with a common minor-1 index: each candidate ray of the stack's
+// detector box is loaded once, its minor-1 weight computed once, and only the
+// minor-2 weight is evaluated per voxel.  Views whose main axis is z take
+// the voxels one at a time.
+template <int ZV>
 __global__ void __launch_bounds__(256) joseph_bp_kernel(const float* __restrict__ vl,
     const float4* __restrict__ rays, const ViewProj* __restrict__ vp,
     const JosephView* __restrict__ views, int n_views, int nu, int nv, int nx, int ny, int nz,
@@ -197,60 +234,67 @@ __global__ void __launch_bounds__(256) joseph_bp_kernel(const float* __restrict_
 {
     const int x = blockIdx.x * 32 + threadIdx.x;
     const int y = blockIdx.y * 8 + threadIdx.y;
-    const int z = blockIdx.z;
+    const int z0 = blockIdx.z * ZV;
     if (x >= nx || y >= ny) return;
-    const long view_elems = static_cast<long>(nu) * nv;
-    double acc = 0.0;  // FP64 over views; each view's few hits summed in FP32
+    const int view_elems = nu * nv;
+    double acc[ZV];  // FP64 over views; each view's few hits summed in FP32
+#pragma unroll
+    for (int q = 0; q < ZV; ++q) acc[q] = 0.0;
     for (int k = 0; k < n_views; ++k) {
         const JosephView& j = views[k];
-        int s, j1, j2;
-        if (j.axis == 0) { s = x; j1 = y; j2 = z; }
-        else if (j.axis == 1) { s = y; j1 = x; j2 = z; }
-        else { s = z; j1 = x; j2 = y; }
-        const float c0 = static_cast<float>(s) - 0.5f * (j.n0 - 1);
-        // detector bounding box of the slice square [j1-1,j1+1]x[j2-1,j2+1]
         const ViewProj& m = vp[k];
-        float umin = 1e30f, umax = -1e30f, vmin = 1e30f, vmax = -1e30f;
+        const float4* rk = rays + static_cast<long>(k) * view_elems;
+        const float* vk = vl + static_cast<long>(k) * view_elems;
+        if (j.axis != 2) {
+            const int s = j.axis == 0 ? x : y, j1 = j.axis == 0 ? y : x;
+            const float c0 = static_cast<float>(s) - 0.5f * (j.n0 - 1);
+            int u0, u1, v0, v1;
+            footprint_box(m, j, c0, j1, z0, z0 + ZV - 1, nu, nv, u0, u1, v0, v1);
+            const float j1f = static_cast<float>(j1);
+            float jq[ZV], accv[ZV];
 #pragma unroll
-        for (int corner = 0; corner < 4; ++corner) {
-            const float d1 = (corner & 1) ? 1.f : -1.f, d2 = (corner & 2) ? 1.f : -1.f;
-            const float q1 = static_cast<float>(j1) + d1 - 0.5f * (j.n1 - 1);
-            const float q2 = static_cast<float>(j2) + d2 - 0.5f * (j.n2 - 1);
-            float px, py, pz;
-            if (j.axis == 0) { px = c0; py = q1; pz = q2; }
-            else if (j.axis == 1) { px = q1; py = c0; pz = q2; }
-            else { px = q1; py = q2; pz = c0; }
-            const float w = fmaf(m.m[8], px, fmaf(m.m[9], py, fmaf(m.m[10], pz, m.m[11])));
-            // the box only needs a few 1e-6 px: correctly rounded reciprocal
-            const float rw = __frcp_rn(w);
-            const float u = fmaf(m.m[0], px, fmaf(m.m[1], py, fmaf(m.m[2], pz, m.m[3]))) * rw;
-            const float v = fmaf(m.m[4], px, fmaf(m.m[5], py, fmaf(m.m[6], pz, m.m[7]))) * rw;
-            umin = fminf(umin, u); umax = fmaxf(umax, u);
-            vmin = fminf(vmin, v); vmax = fmaxf(vmax, v);
-        }
-        constexpr float margin = 0.05f;
-        const int u0 = max(0, static_cast<int>(ceilf(umin - margin)));
-        const int u1 = min(nu - 1, static_cast<int>(floorf(umax + margin)));
-        const int v0 = max(0, static_cast<int>(ceilf(vmin - margin)));
-        const int v1 = min(nv - 1, static_cast<int>(floorf(vmax + margin)));
-        const float j1f = static_cast<float>(j1), j2f = static_cast<float>(j2);
-        const long base = k * view_elems;
-        float accv = 0.f;
-        // every candidate of the box is evaluated without a branch: a ray
-        // outside the footprint has weight 0
-        for (int iv = v0; iv <= v1; ++iv) {
-            const long row = base + static_cast<long>(iv) * nu;
-            for (int iu = u0; iu <= u1; ++iu) {
-                const float4 r = __ldg(rays + row + iu);
-                const float w = hat_weight(fmaf(r.x, c0, r.y), j1f) *
-                    hat_weight(fmaf(r.z, c0, r.w), j2f);
-                accv = fmaf(__ldg(vl + row + iu), w, accv);
+            for (int q = 0; q < ZV; ++q) { jq[q] = static_cast<float>(z0 + q); accv[q] = 0.f; }
+            for (int iv = v0; iv <= v1; ++iv) {
+                const int row = iv * nu;
+                for (int iu = u0; iu <= u1; ++iu) {
+                    const float4 r = __ldg(rk + row + iu);
+                    const float t = __ldg(vk + row + iu) * hat_weight(fmaf(r.x, c0, r.y), j1f);
+                    const float f2 = fmaf(r.z, c0, r.w);
+#pragma unroll
+                    for (int q = 0; q < ZV; ++q) accv[q] = fmaf(t, hat_weight(f2, jq[q]), accv[q]);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < ZV; ++q) acc[q] += static_cast<double>(accv[q]);
+        } else {
+            // main axis z: each voxel of the stack is its own slice
+            const float j1f = static_cast<float>(x), j2f = static_cast<float>(y);
+#pragma unroll
+            for (int q = 0; q < ZV; ++q) {
+                const float c0 = static_cast<float>(z0 + q) - 0.5f * (j.n0 - 1);
+                int u0, u1, v0, v1;
+                footprint_box(m, j, c0, x, y, y, nu, nv, u0, u1, v0, v1);
+                float accv = 0.f;
+                for (int iv = v0; iv <= v1; ++iv) {
+                    const int row = iv * nu;
+                    for (int iu = u0; iu <= u1; ++iu) {
+                        const float4 r = __ldg(rk + row + iu);
+                        const float w = hat_weight(fmaf(r.x, c0, r.y), j1f) *
+                            hat_weight(fmaf(r.z, c0, r.w), j2f);
+                        accv = fmaf(__ldg(vk + row + iu), w, accv);
+                    }
+                }
+                acc[q] += static_cast<double>(accv);
             }
         }
-        acc += static_cast<double>(accv);
     }
-    float* dst = vol + (static_cast<long>(z) * ny + y) * nx + x;
-    *dst = accumulate ? static_cast<float>(*dst + acc) : static_cast<float>(acc);
+    const long plane = static_cast<long>(nx) * ny;
+#pragma unroll
+    for (int q = 0; q < ZV; ++q) {
+        if (z0 + q >= nz) break;
+        float* dst = vol + (z0 + q) * plane + static_cast<long>(y) * nx + x;
+        *dst = accumulate ? static_cast<float>(*dst + acc[q]) : static_cast<float>(acc[q]);
+    }
 }
 
 } // namespace
@@ -319,8 +363,9 @@ cudaError_t launch_joseph_bp(const float* proj, const float4* rays, const float*
     joseph_weight_rays_kernel<<<148 * 8, 256, 0, s>>>(proj, lens, n, weighted);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    const dim3 grid((vol.nx + 31) / 32, (vol.ny + 7) / 8, vol.nz);
-    joseph_bp_kernel<<<grid, dim3(32, 8), 0, s>>>(weighted, rays,
+    constexpr int ZV = 4;
+    const dim3 grid((vol.nx + 31) / 32, (vol.ny + 7) / 8, (vol.nz + ZV - 1) / ZV);
+    joseph_bp_kernel<ZV><<<grid, dim3(32, 8), 0, s>>>(weighted, rays,
         reinterpret_cast<const ViewProj*>(view_proj), views, n_views, nu, nv, vol.nx, vol.ny,
         vol.nz, out, accumulate);
     return cudaGetLastError();
