@@ -4,10 +4,13 @@
 // (.../FDK/kernels/YkFDKFilterKernels.cu:32-140).  With N >= 2 Nu that is the
 // linear product C = A T, A = preweighted rows [rows][Nu], T[k][j] = h(j-k)
 // (Toeplitz and, h being even, symmetric).  Here it runs as one BF16 GEMM with
-// FP32 accumulation in TMEM and a split hi/lo correction:
-//     A T ~= A_hi T_hi + A_hi T_lo + A_lo T_hi,
-// folded into a single GEMM over K' = 3 Nu ([A_hi | A_hi | A_lo] x
-// [T_hi; T_lo; T_hi]) so one accumulator carries all three products.
+// FP32 accumulation in TMEM and split-precision operands.  Each operand is a
+// sum of BF16 parts, X = X0 + X1 (+ X2), each part the BF16 rounding of what
+// the previous parts leave; the products are summed over K' = NSEG Nu into
+// one accumulator:
+//   NSEG 3 (BF16 plans): A0 T0 + A0 T1 + A1 T0, about 16 significant bits;
+//   NSEG 6 (FP32 plans): A0 T0 + A0 T1 + A1 T0 + A0 T2 + A1 T1 + A2 T0, the
+//     24 bits of FP32 (the dropped products are below 2^-24 of the result).
 //
 // CTA = 128 output rows x TN output columns, 4 warps:
 //   warp 0 lane 0 : TMA producer (A and T tiles, 128-byte swizzle, this
@@ -107,10 +110,19 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar)
                  ::"r"(smem_u32(bar)) : "memory");
 }
 
-template <int TN, bool PAIR>
+// (A part, T part) of segment `seg` of the split product
+__device__ __forceinline__ void segment_parts(int seg, int& a, int& t)
+{
+    // segments 0..5 = (0,0) (0,1) (1,0) (0,2) (1,1) (2,0), one nibble each
+    a = (0x210100 >> (4 * seg)) & 0xF;
+    t = (0x012010 >> (4 * seg)) & 0xF;
+}
+
+template <int TN, bool PAIR, int NSEG>
 __global__ void __launch_bounds__(128, 1) ramp_tc_kernel(
-    const __grid_constant__ CUtensorMap map_a_hi, const __grid_constant__ CUtensorMap map_a_lo,
-    const __grid_constant__ CUtensorMap map_t_hi, const __grid_constant__ CUtensorMap map_t_lo,
+    const __grid_constant__ CUtensorMap map_a0, const __grid_constant__ CUtensorMap map_a1,
+    const __grid_constant__ CUtensorMap map_a2, const __grid_constant__ CUtensorMap map_t0,
+    const __grid_constant__ CUtensorMap map_t1, const __grid_constant__ CUtensorMap map_t2,
     long rows, int nu, int nv, int kchunks, const FdkPreweightView* __restrict__ pwv,
     float* __restrict__ C, int ldc, int* __restrict__ err)
 {
@@ -130,7 +142,7 @@ __global__ void __launch_bounds__(128, 1) ramp_tc_kernel(
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const long m0 = static_cast<long>(blockIdx.y) * TM;
     const int n0 = blockIdx.x * TN;
-    const int total = 3 * kchunks;
+    const int total = NSEG * kchunks;
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
@@ -159,9 +171,11 @@ __global__ void __launch_bounds__(128, 1) ramp_tc_kernel(
                 break;
             }
             if (*(volatile int*)abort_flag) break;
-            const int seg = i / kchunks, kc = i % kchunks;
-            const CUtensorMap* ma = seg == 2 ? &map_a_lo : &map_a_hi;
-            const CUtensorMap* mt = seg == 1 ? &map_t_lo : &map_t_hi;
+            const int seg = i / kchunks, kc = i - seg * kchunks;
+            int pa, pt;
+            segment_parts(seg, pa, pt);
+            const CUtensorMap* ma = pa == 0 ? &map_a0 : pa == 1 ? &map_a1 : &map_a2;
+            const CUtensorMap* mt = pt == 0 ? &map_t0 : pt == 1 ? &map_t1 : &map_t2;
             bar_expect_tx(&full[s], kAStageBytes + kBStageBytes);
             tma_2d(a_ring + s * kAStageBytes, ma, &full[s], kc * TK, static_cast<int>(m0));
             tma_2d(b_ring + s * kBStageBytes, mt, &full[s], kc * TK, n0);
@@ -246,10 +260,12 @@ __global__ void __launch_bounds__(128, 1) ramp_tc_kernel(
                      ::"r"(tmem), "r"(kTmemCols) : "memory");
 }
 
-// preweighted rows split into bf16 hi and lo parts, rows padded to lda
+// preweighted rows split into BF16 parts (two, or three when part2 is
+// given), rows padded to lda
 __global__ void __launch_bounds__(128) preweight_split_kernel(const void* __restrict__ in, int in_bf16,
     const FdkPreweightView* __restrict__ pw, const float* __restrict__ parker, int nu, int nv,
-    int lda, __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo)
+    int lda, __nv_bfloat16* __restrict__ part0, __nv_bfloat16* __restrict__ part1,
+    __nv_bfloat16* __restrict__ part2)
 {
     const long row = blockIdx.x;
     const int view = static_cast<int>(row / nv);
@@ -276,8 +292,11 @@ __global__ void __launch_bounds__(128) preweight_split_kernel(const void* __rest
             x = v * wt;
         }
         const __nv_bfloat16 h = __float2bfloat16_rn(x);
-        hi[row * lda + iu] = h;
-        lo[row * lda + iu] = __float2bfloat16_rn(x - __bfloat162float(h));
+        const float r1 = x - __bfloat162float(h);  // exact
+        const __nv_bfloat16 m = __float2bfloat16_rn(r1);
+        part0[row * lda + iu] = h;
+        part1[row * lda + iu] = m;
+        if (part2) part2[row * lda + iu] = __float2bfloat16_rn(r1 - __bfloat162float(m));
     }
 }
 
@@ -309,19 +328,27 @@ bool make_map(CUtensorMap* map, const void* base, long inner, long outer, long l
                CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-template <int TN, bool PAIR>
-cudaError_t launch_tn(const CUtensorMap& ah, const CUtensorMap& al, const CUtensorMap& th,
-    const CUtensorMap& tl, long rows, int nu, int nv, int kchunks, const FdkPreweightView* pwv,
-    float* C, int ldc, int* err, cudaStream_t s)
+template <int TN, bool PAIR, int NSEG>
+cudaError_t launch_tn3(const CUtensorMap* a, const CUtensorMap* t, long rows, int nu, int nv,
+    int kchunks, const FdkPreweightView* pwv, float* C, int ldc, int* err, cudaStream_t s)
 {
     const size_t smem = 1024 + STAGES * (kAStageBytes + TN * TK * 2) + (2 * STAGES + 1) * 8 + 16;
-    auto k = ramp_tc_kernel<TN, PAIR>;
+    auto k = ramp_tc_kernel<TN, PAIR, NSEG>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
         static_cast<int>(smem));
     if (e != cudaSuccess) return e;
     const dim3 grid((nu + TN - 1) / TN, static_cast<unsigned>((rows + TM - 1) / TM));
-    k<<<grid, 128, smem, s>>>(ah, al, th, tl, rows, nu, nv, kchunks, pwv, C, ldc, err);
+    k<<<grid, 128, smem, s>>>(a[0], a[1], a[2], t[0], t[1], t[2], rows, nu, nv, kchunks, pwv, C,
+        ldc, err);
     return cudaGetLastError();
+}
+
+template <int TN, bool PAIR>
+cudaError_t launch_tn(const CUtensorMap* a, const CUtensorMap* t, int nseg, long rows, int nu,
+    int nv, int kchunks, const FdkPreweightView* pwv, float* C, int ldc, int* err, cudaStream_t s)
+{
+    return nseg == 6 ? launch_tn3<TN, PAIR, 6>(a, t, rows, nu, nv, kchunks, pwv, C, ldc, err, s)
+                     : launch_tn3<TN, PAIR, 3>(a, t, rows, nu, nv, kchunks, pwv, C, ldc, err, s);
 }
 
 } // namespace
@@ -344,37 +371,42 @@ int tc_filter_lda(int nu) { return (nu + TK - 1) / TK * TK; }
 
 cudaError_t launch_fdk_preweight_split_bf16(const void* proj, int proj_dtype,
     const FdkPreweightView* pw, const float* parker, int n_views, int nu, int nv, int ld,
-    __nv_bfloat16* hi, __nv_bfloat16* lo, cudaStream_t s)
+    __nv_bfloat16* const parts[3], cudaStream_t s)
 {
     const long rows = static_cast<long>(n_views) * nv;
     if (rows <= 0) return cudaSuccess;
     preweight_split_kernel<<<static_cast<unsigned>(rows), 128, 0, s>>>(proj,
-        proj_dtype == YKB_DTYPE_BF16 ? 1 : 0, pw, parker, nu, nv, ld, hi, lo);
+        proj_dtype == YKB_DTYPE_BF16 ? 1 : 0, pw, parker, nu, nv, ld, parts[0], parts[1], parts[2]);
     return cudaGetLastError();
 }
 
-cudaError_t launch_fdk_ramp_tcgen05(const __nv_bfloat16* a_hi, const __nv_bfloat16* a_lo,
-    const __nv_bfloat16* t_hi, const __nv_bfloat16* t_lo, int rows, int nu, int ld,
-    const FdkPreweightView* pwv, int nv, float* out, int layout, int ldc, int* err, cudaStream_t s)
+cudaError_t launch_fdk_ramp_tcgen05(const __nv_bfloat16* const a_parts[3],
+    const __nv_bfloat16* const t_parts[3], int rows, int nu, int ld, const FdkPreweightView* pwv,
+    int nv, float* out, int layout, int ldc, int* err, cudaStream_t s)
 {
     if (rows <= 0) return cudaSuccess;
     const int tn = tc_filter_tile_n(nu);
-    CUtensorMap ah, al, th, tl;
+    const int nparts = a_parts[2] && t_parts[2] ? 3 : 2;
+    CUtensorMap a[3], t[3];
     // A: [rows][ld] K-major, box 64 x 128; T: [nu][ld] K-major, box 64 x TN
-    if (!make_map(&ah, a_hi, nu, rows, ld, TK, TM) || !make_map(&al, a_lo, nu, rows, ld, TK, TM) ||
-        !make_map(&th, t_hi, nu, nu, ld, TK, tn) || !make_map(&tl, t_lo, nu, nu, ld, TK, tn))
-        return cudaErrorInvalidValue;
+    for (int q = 0; q < 3; ++q) {
+        const int src = q < nparts ? q : 0;  // an unused slot repeats part 0
+        if (!make_map(&a[q], a_parts[src], nu, rows, ld, TK, TM) ||
+            !make_map(&t[q], t_parts[src], nu, nu, ld, TK, tn))
+            return cudaErrorInvalidValue;
+    }
+    const int nseg = nparts == 3 ? 6 : 3;
     const int kchunks = (nu + TK - 1) / TK;
     const bool pair = layout == kFilteredPairs;
     switch (tn) {
-    case 256: return pair ? launch_tn<256, true>(ah, al, th, tl, rows, nu, nv, kchunks, pwv, out, ldc, err, s)
-                          : launch_tn<256, false>(ah, al, th, tl, rows, nu, nv, kchunks, pwv, out, ldc, err, s);
-    case 192: return pair ? launch_tn<192, true>(ah, al, th, tl, rows, nu, nv, kchunks, pwv, out, ldc, err, s)
-                          : launch_tn<192, false>(ah, al, th, tl, rows, nu, nv, kchunks, pwv, out, ldc, err, s);
-    case 128: return pair ? launch_tn<128, true>(ah, al, th, tl, rows, nu, nv, kchunks, pwv, out, ldc, err, s)
-                          : launch_tn<128, false>(ah, al, th, tl, rows, nu, nv, kchunks, pwv, out, ldc, err, s);
-    default: return pair ? launch_tn<64, true>(ah, al, th, tl, rows, nu, nv, kchunks, pwv, out, ldc, err, s)
-                         : launch_tn<64, false>(ah, al, th, tl, rows, nu, nv, kchunks, pwv, out, ldc, err, s);
+    case 256: return pair ? launch_tn<256, true>(a, t, nseg, rows, nu, nv, kchunks, pwv, out, ldc, err, s)
+                          : launch_tn<256, false>(a, t, nseg, rows, nu, nv, kchunks, pwv, out, ldc, err, s);
+    case 192: return pair ? launch_tn<192, true>(a, t, nseg, rows, nu, nv, kchunks, pwv, out, ldc, err, s)
+                          : launch_tn<192, false>(a, t, nseg, rows, nu, nv, kchunks, pwv, out, ldc, err, s);
+    case 128: return pair ? launch_tn<128, true>(a, t, nseg, rows, nu, nv, kchunks, pwv, out, ldc, err, s)
+                          : launch_tn<128, false>(a, t, nseg, rows, nu, nv, kchunks, pwv, out, ldc, err, s);
+    default: return pair ? launch_tn<64, true>(a, t, nseg, rows, nu, nv, kchunks, pwv, out, ldc, err, s)
+                         : launch_tn<64, false>(a, t, nseg, rows, nu, nv, kchunks, pwv, out, ldc, err, s);
     }
 }
 

@@ -70,11 +70,12 @@ size_t volume_elems(const ykb_volume& v)
 }
 
 // Views per workspace chunk: bounded so the filter workspace stays below
-// about 4 GiB whatever the scan length.
-int chunk_capacity(int n_views, int nu, int nv)
+// about 8 GiB whatever the scan length.  a_bytes: bytes per pixel of the
+// preweighted rows (4 as float or as two BF16 parts, 6 as three).
+int chunk_capacity(int n_views, int nu, int nv, int a_bytes)
 {
-    // preweighted rows (4 B) + filtered tap pairs (8 B) per detector pixel
-    const size_t per_view = static_cast<size_t>(nu) * nv * 12;
+    // preweighted rows + filtered tap pairs (8 B) per detector pixel
+    const size_t per_view = static_cast<size_t>(nu) * nv * (a_bytes + 8);
     const size_t budget = size_t(8) << 30;
     const size_t cap = std::max<size_t>(1, budget / std::max<size_t>(per_view, 1));
     return static_cast<int>(std::min<size_t>(n_views, cap));
@@ -169,17 +170,26 @@ YKB_API ykb_status ykb_fdk_plan_create_ex(const ykb_cone_view* views, int n_view
     build_ramp_kernel(nu, p->derived[0].du, *filter, h);
     std::vector<float> hf(h.begin(), h.end());
 
-    p->batch_capacity = chunk_capacity(n_views, nu, nv);
-    p->tc_filter = precision == YKB_PRECISION_BF16 && tcgen05_filter_supported(nu);
+    // the ramp filter runs on the tensor cores: BF16 plans with two BF16
+    // parts per operand, FP32 plans with three (FP32 accuracy); the FP32
+    // Toeplitz product on the CUDA cores when tcgen05 is unavailable, or
+    // when YKB_FDK_FILTER=simt asks for it (tests compare the two)
+    const char* filter_path = std::getenv("YKB_FDK_FILTER");
+    const bool force_simt = filter_path && std::strcmp(filter_path, "simt") == 0;
+    p->tc_filter = tcgen05_filter_supported(nu) &&
+        (precision == YKB_PRECISION_BF16 || !force_simt);
+    p->tc_parts = p->tc_filter ? (precision == YKB_PRECISION_BF16 ? 2 : 3) : 0;
     p->lda = p->tc_filter ? tc_filter_lda(nu) : nu;
-    // work_a holds the preweighted rows: float, or bf16 hi + bf16 lo
+    const int a_bytes = p->tc_parts == 3 ? 6 : 4;
+    p->batch_capacity = chunk_capacity(n_views, nu, nv, a_bytes);
+    // work_a holds the preweighted rows: float, or the bf16 parts in turn
     const size_t chunk_elems = static_cast<size_t>(p->batch_capacity) * p->lda * nv;
     cudaError_t e;
     if ((e = p->coef.alloc(sizeof(FdkViewCoef) * n_views)) != cudaSuccess ||
         (e = p->pwv.alloc(sizeof(FdkPreweightView) * n_views)) != cudaSuccess ||
         (e = p->ramp.alloc(sizeof(float) * hf.size())) != cudaSuccess ||
         (e = p->err_flag.alloc(4 * sizeof(int))) != cudaSuccess ||
-        (e = p->work_a.alloc(chunk_elems * sizeof(float))) != cudaSuccess) {
+        (e = p->work_a.alloc(chunk_elems * a_bytes)) != cudaSuccess) {
         delete p;
         return cuda_status(e, "cudaMalloc (FDK plan workspace)");
     }
@@ -201,21 +211,30 @@ YKB_API ykb_status ykb_fdk_plan_create_ex(const ykb_cone_view* views, int n_view
         return cuda_status(e, "Parker weight table");
     }
     if (p->tc_filter) {
-        // Toeplitz operand T[j][k] = h(j-k) split into bf16 hi and lo parts
+        // Toeplitz operand T[j][k] = h(j-k) split into BF16 parts, each the
+        // rounding of what the previous parts leave of h (FP64)
         const size_t tn = static_cast<size_t>(nu) * p->lda;
-        std::vector<__nv_bfloat16> thi(tn, __float2bfloat16_rn(0.f)), tlo(tn, __float2bfloat16_rn(0.f));
+        const __nv_bfloat16 zero = __float2bfloat16_rn(0.f);
+        std::vector<__nv_bfloat16> t0(tn, zero), t1(tn, zero), t2(p->tc_parts == 3 ? tn : 0, zero);
         for (int j = 0; j < nu; ++j)
             for (int k = 0; k < nu; ++k) {
-                const double v = h[static_cast<size_t>(j - k + nu - 1)];
-                const __nv_bfloat16 hb = __float2bfloat16_rn(static_cast<float>(v));
-                thi[static_cast<size_t>(j) * p->lda + k] = hb;
-                tlo[static_cast<size_t>(j) * p->lda + k] =
-                    __float2bfloat16_rn(static_cast<float>(v - static_cast<double>(__bfloat162float(hb))));
+                const size_t at = static_cast<size_t>(j) * p->lda + k;
+                double v = h[static_cast<size_t>(j - k + nu - 1)];
+                const __nv_bfloat16 b0 = __float2bfloat16_rn(static_cast<float>(v));
+                v -= static_cast<double>(__bfloat162float(b0));
+                const __nv_bfloat16 b1 = __float2bfloat16_rn(static_cast<float>(v));
+                t0[at] = b0;
+                t1[at] = b1;
+                if (p->tc_parts == 3)
+                    t2[at] = __float2bfloat16_rn(static_cast<float>(v - static_cast<double>(__bfloat162float(b1))));
             }
         if ((e = p->toeplitz_hi.alloc(tn * 2)) != cudaSuccess ||
             (e = p->toeplitz_lo.alloc(tn * 2)) != cudaSuccess ||
-            (e = cudaMemcpy(p->toeplitz_hi.ptr, thi.data(), tn * 2, cudaMemcpyHostToDevice)) != cudaSuccess ||
-            (e = cudaMemcpy(p->toeplitz_lo.ptr, tlo.data(), tn * 2, cudaMemcpyHostToDevice)) != cudaSuccess) {
+            (p->tc_parts == 3 && (e = p->toeplitz_lo2.alloc(tn * 2)) != cudaSuccess) ||
+            (e = cudaMemcpy(p->toeplitz_hi.ptr, t0.data(), tn * 2, cudaMemcpyHostToDevice)) != cudaSuccess ||
+            (e = cudaMemcpy(p->toeplitz_lo.ptr, t1.data(), tn * 2, cudaMemcpyHostToDevice)) != cudaSuccess ||
+            (p->tc_parts == 3 &&
+             (e = cudaMemcpy(p->toeplitz_lo2.ptr, t2.data(), tn * 2, cudaMemcpyHostToDevice)) != cudaSuccess)) {
             delete p;
             return cuda_status(e, "Toeplitz operand");
         }
@@ -270,7 +289,8 @@ YKB_API size_t ykb_fdk_workspace_bytes(const ykb_fdk_plan* p)
 {
     if (!p) return 0;
     return p->coef.bytes + p->pwv.bytes + p->ramp.bytes + p->toeplitz_hi.bytes +
-        p->toeplitz_lo.bytes + p->work_a.bytes + p->work_filtered.bytes + p->err_flag.bytes +
+        p->toeplitz_lo.bytes + p->toeplitz_lo2.bytes + p->work_a.bytes + p->work_filtered.bytes +
+        p->err_flag.bytes +
         p->parker.bytes + p->stage_in.bytes;
 }
 
@@ -299,13 +319,16 @@ ykb_status filter_chunk(ykb_fdk_plan* p, const void* proj, int proj_dtype, int f
     const float* parker = p->parker.ptr ? p->parker.as<float>() + static_cast<size_t>(first) * p->nu
                                         : nullptr;
     if (p->tc_filter) {
-        const size_t half = static_cast<size_t>(p->batch_capacity) * p->nv * p->lda;
-        __nv_bfloat16* a_hi = p->work_a.as<__nv_bfloat16>();
-        __nv_bfloat16* a_lo = a_hi + half;
+        const size_t part = static_cast<size_t>(p->batch_capacity) * p->nv * p->lda;
+        __nv_bfloat16* a0 = p->work_a.as<__nv_bfloat16>();
+        __nv_bfloat16* const a[3] = {a0, a0 + part, p->tc_parts == 3 ? a0 + 2 * part : nullptr};
         YKB_TRY_CUDA(launch_fdk_preweight_split_bf16(proj, proj_dtype, pwv, parker, count, p->nu, p->nv,
-            p->lda, a_hi, a_lo, s));
-        YKB_TRY_CUDA(launch_fdk_ramp_tcgen05(a_hi, a_lo, p->toeplitz_hi.as<__nv_bfloat16>(),
-            p->toeplitz_lo.as<__nv_bfloat16>(), count * p->nv, p->nu, p->lda, pwv, p->nv,
+            p->lda, a, s));
+        const __nv_bfloat16* const ac[3] = {a[0], a[1], a[2]};
+        const __nv_bfloat16* const t[3] = {p->toeplitz_hi.as<__nv_bfloat16>(),
+            p->toeplitz_lo.as<__nv_bfloat16>(),
+            p->tc_parts == 3 ? p->toeplitz_lo2.as<__nv_bfloat16>() : nullptr};
+        YKB_TRY_CUDA(launch_fdk_ramp_tcgen05(ac, t, count * p->nv, p->nu, p->lda, pwv, p->nv,
             dst, layout, ldc, p->err_flag.as<int>(), s));
         return YKB_OK;
     }

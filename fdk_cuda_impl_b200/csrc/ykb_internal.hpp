@@ -192,12 +192,16 @@ cudaError_t launch_fdk_preweight(const void* proj, int proj_dtype,
 cudaError_t launch_fdk_ramp_fp32(const float* pw_rows, const float* h_dev,
     const FdkPreweightView* pwv, int n_views, int nu, int nv, float* out,
     int layout, int ldc, cudaStream_t s);
+// BF16 split parts of the preweighted rows: parts[0], parts[1] and, when
+// parts[2] is not null, a third part (FP32-equivalent split)
 cudaError_t launch_fdk_preweight_split_bf16(const void* proj, int proj_dtype,
     const FdkPreweightView* pw, const float* parker, int n_views, int nu, int nv, int ld,
-    __nv_bfloat16* hi, __nv_bfloat16* lo, cudaStream_t s);
-cudaError_t launch_fdk_ramp_tcgen05(const __nv_bfloat16* a_hi,
-    const __nv_bfloat16* a_lo, const __nv_bfloat16* t_hi,
-    const __nv_bfloat16* t_lo, int rows, int nu, int ld,
+    __nv_bfloat16* const parts[3], cudaStream_t s);
+// tcgen05 Toeplitz filter over split operands: two parts each (3 products,
+// BF16 plans) or three (6 products, FP32 accuracy) when a_parts[2] and
+// t_parts[2] are given
+cudaError_t launch_fdk_ramp_tcgen05(const __nv_bfloat16* const a_parts[3],
+    const __nv_bfloat16* const t_parts[3], int rows, int nu, int ld,
     const FdkPreweightView* pwv, int nv, float* out, int layout, int ldc, int* err_flag,
     cudaStream_t s);
 bool tcgen05_filter_supported(int nu);
@@ -254,6 +258,7 @@ struct ykb_fdk_plan {
     int precision = YKB_PRECISION_FP32;
     bool axial = false;
     bool tc_filter = false;
+    int tc_parts = 0;            // BF16 parts per operand of the tensor-core filter (2 or 3)
     int batch_capacity = 0;      // views the workspace holds
     int ld = 0;                  // row pitch (elements) of the filtered workspace
     int layout = 0;              // FilteredLayout of the filtered workspace
@@ -265,8 +270,8 @@ struct ykb_fdk_plan {
     ykb::DeviceBuffer pwv;       // FdkPreweightView[n_views]
     ykb::DeviceBuffer ramp;      // float[2*nu-1]
     ykb::DeviceBuffer parker;    // float[n_views][nu] short-scan weights, or empty
-    ykb::DeviceBuffer toeplitz_hi, toeplitz_lo;  // bf16 [nu][ld] (BF16 plans)
-    ykb::DeviceBuffer work_a;    // preweighted rows: float, or bf16 hi then lo
+    ykb::DeviceBuffer toeplitz_hi, toeplitz_lo, toeplitz_lo2;  // bf16 [nu][lda] split parts
+    ykb::DeviceBuffer work_a;    // preweighted rows: float, or the bf16 split parts in turn
     ykb::DeviceBuffer work_filtered;  // filtered projections (layout, pitch ld)
     ykb::DeviceBuffer err_flag;  // int[4]: device error word, box pre-pass scratch
     // host-input streaming (ykb_fdk_execute_host), created on first use
