@@ -108,11 +108,14 @@ public:
             return fail_(EApiErrorCode::InvalidGeometry,
                 "Forward-projection volume rotation must contain finite radians");
         if (r.pipeline == EPipeline::ForwardProjection &&
-            r.forward_projector != EForwardProjector::Joseph)
-            // resolveForwardProjector maps Automatic to Siddon for flat
-            // detectors (src/interface/YkProjectorSelection.hpp:11-24)
+            r.forward_projector == EForwardProjector::SeparableFootprint)
             return fail_(EApiErrorCode::UnsupportedCombination,
-                "forward projection here is Joseph: request EForwardProjector::Joseph");
+                "forward projection here is Joseph or Siddon (EForwardProjector::SeparableFootprint "
+                "is not implemented)");
+        // resolveForwardProjector maps Automatic to Siddon for flat detectors
+        // (src/interface/YkProjectorSelection.hpp:11-24)
+        fp_task_ = r.forward_projector == EForwardProjector::Joseph ? YKB_TASK_FP_JOSEPH
+                                                                    : YKB_TASK_FP_SIDDON;
         if (g.volume.nx <= 0 || g.volume.ny <= 0 || g.volume.nz <= 0 ||
             !(g.volume.voxel_x_mm > 0.f) || !(g.volume.voxel_y_mm > 0.f) ||
             !(g.volume.voxel_z_mm > 0.f) || !std::isfinite(g.volume.center_mm.x) ||
@@ -327,7 +330,7 @@ private:
                 return fail_(EApiErrorCode::CudaError, "device projection scratch allocation failed");
             d_proj = static_cast<float*>(proj_scratch_.ptr);
         }
-        if (ykb_joseph_fp(joseph_, d_vol, d_proj, 0, stream_) != YKB_OK)
+        if (ykb_operator_apply(joseph_, fp_task_, d_vol, d_proj, 0, stream_) != YKB_OK)
             return fail_(EApiErrorCode::CudaError, ykb_last_error());
         if (r.projection.location == EMemoryLocation::Host) {
             const cudaError_t e = cudaMemcpyAsync(r.projection.data, d_proj, proj_bytes,
@@ -359,6 +362,7 @@ private:
     bool initialized_ = false;
     ykb_fdk_plan* fdk_ = nullptr;
     ykb_joseph_plan* joseph_ = nullptr;
+    int fp_task_ = YKB_TASK_FP_JOSEPH;  // FP_Joseph or FP_Siddon
     cudaStream_t stream_ = nullptr;
     DeviceScratch proj_scratch_, vol_scratch_;
     EApiErrorCode code_ = EApiErrorCode::None;

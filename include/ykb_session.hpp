@@ -3,11 +3,12 @@
 // API (include/YKCBCT/interface/YkReconstructionApi.hpp:18-98,
 // YkReconstructionTypes.hpp, YkSystemReconstruction.hpp, and the geometry
 // specs of include/YKCBCT/geometry/YkGeometryBuilderTypes.hpp), so code
-// written against that API for FDK and Joseph forward projection compiles
-// and runs unchanged on this library.
+// written against that API for FDK and forward projection compiles and runs
+// unchanged on this library.
 //
 // Scope: flat detector, circular trajectory, EPipeline::FDK and
-// EPipeline::ForwardProjection with EForwardProjector::Joseph.  Other
+// EPipeline::ForwardProjection with EForwardProjector::Joseph, ::Siddon or
+// ::Automatic (Siddon for a flat detector, as the reference resolves it).  Other
 // pipelines, detectors and trajectories are outside this library and are
 // rejected with EApiErrorCode::UnsupportedCombination at initialize().
 // Members the reference carries only for those other algorithms (helical and

@@ -122,8 +122,8 @@ int mode_validate()
     }
     {
         SSystemSpec spec = small_system(EPipeline::ForwardProjection);
-        spec.reconstruction.forward_projector = EForwardProjector::Automatic;
-        expect_code("fp_automatic", s->initialize(spec), *s, EApiErrorCode::UnsupportedCombination, failures);
+        spec.reconstruction.forward_projector = EForwardProjector::SeparableFootprint;
+        expect_code("fp_footprint", s->initialize(spec), *s, EApiErrorCode::UnsupportedCombination, failures);
     }
     {
         SSystemSpec spec = small_system(EPipeline::ForwardProjection);
@@ -273,7 +273,7 @@ void write_f32(const char* path, const std::vector<float>& v)
 }
 
 // fdk|fp <in> <out> views per_turn sid sdd nu nv du dv nx ny nz vox filter
-int mode_file(bool fdk, int argc, char** argv)
+int mode_file(bool fdk, int argc, char** argv, bool siddon = false)
 {
     if (argc < 17) return 4;
     SSystemSpec spec{};
@@ -289,7 +289,9 @@ int mode_file(bool fdk, int argc, char** argv)
     spec.geometry.volume = {std::atoi(argv[12]), std::atoi(argv[13]), std::atoi(argv[14]), vox, vox, vox,
         {0.f, 0.f, 0.f}};
     spec.reconstruction.pipeline = fdk ? EPipeline::FDK : EPipeline::ForwardProjection;
-    spec.reconstruction.forward_projector = EForwardProjector::Joseph;
+    // the FP modes pick the projector: "fp" Joseph, "fp_auto" Automatic (Siddon)
+    spec.reconstruction.forward_projector = siddon ? EForwardProjector::Automatic
+                                                   : EForwardProjector::Joseph;
     spec.reconstruction.fdk.filter.type = static_cast<EFdkFilter>(std::atoi(argv[16]));
     const size_t pn = size_t(spec.geometry.circular.total_views) * spec.geometry.flat_detector.channels *
         spec.geometry.flat_detector.rows;
@@ -317,6 +319,7 @@ int main(int argc, char** argv)
     if (mode == "streaming") return mode_streaming();
     if (mode == "fdk") return mode_file(true, argc, argv);
     if (mode == "fp") return mode_file(false, argc, argv);
-    std::fprintf(stderr, "usage: session_test validate|roundtrip|streaming|fdk|fp ...\n");
+    if (mode == "fp_auto") return mode_file(false, argc, argv, true);
+    std::fprintf(stderr, "usage: session_test validate|roundtrip|streaming|fdk|fp|fp_auto ...\n");
     return 4;
 }

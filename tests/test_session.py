@@ -71,6 +71,12 @@ def test_session_fdk_and_fp_match_oracle(session_bin, cuda_device, oracle, tmp_p
     proj = np.fromfile(pout, dtype=np.float32).reshape(len(views), sc.rows, sc.channels)
     ref_p = oracle.joseph_fp(views, sc.channels, sc.rows, K.oracle_volume(oracle, case.grid), ph)
     assert K.rel_rmse(proj, ref_p) <= 1e-5
+    # EForwardProjector::Automatic resolves to Siddon for a flat detector
+    rc, _, err = _run(session_bin, "fp_auto", vin, pout, *geo, *grid, 1)
+    assert rc == 0, err
+    proj_s = np.fromfile(pout, dtype=np.float32).reshape(len(views), sc.rows, sc.channels)
+    ref_s = oracle.siddon_fp(views, sc.channels, sc.rows, K.oracle_volume(oracle, case.grid), ph)
+    assert K.rel_rmse(proj_s, ref_s) <= 1e-5
     # FDK through the Session vs the oracle
     pin, vout = tmp_path / "p.f32", tmp_path / "v.f32"
     p32 = ref_p.astype(np.float32)
