@@ -79,6 +79,8 @@ SIGNATURES = {
     "ykb_fdk_plan_destroy": (C.c_int, [_P]),
     "ykb_fdk_execute": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_int, _P, C.c_int, _P]),
     "ykb_fdk_execute_host": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_int, _P, C.c_int, _P]),
+    "ykb_fdk_execute_host_out": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_int, _P, _P, C.c_int,
+                                           _P]),
     "ykb_fdk_filter": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_int, _P, _P]),
     "ykb_fdk_backproject": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_int, _P, C.c_int, _P]),
     "ykb_fdk_workspace_bytes": (C.c_size_t, [_P]),

@@ -341,10 +341,18 @@ ykb_status filter_chunk(ykb_fdk_plan* p, const void* proj, int proj_dtype, int f
 
 // weighted backprojection of `count` filtered views (FilteredLayout
 // `layout`, row pitch ld elements) starting at plan view `first`
+// z_begin/z_count restrict the work to volume slices [z_begin, z_begin +
+// z_count) (z_count < 0: all); z_begin must be a multiple of 32, the z tile
+// of the TMA backprojection, so that its tiles are those of the box pre-pass
 ykb_status backproject_chunk(ykb_fdk_plan* p, const void* filtered, int layout, int ld, int first,
-    int count, float* vol, int accumulate, cudaStream_t s)
+    int count, float* vol, int accumulate, cudaStream_t s, int z_begin = 0, int z_count = -1)
 {
-    const VolumeGrid grid = make_grid(p->volume);
+    VolumeGrid grid = make_grid(p->volume);
+    if (z_count >= 0) {
+        vol += static_cast<size_t>(z_begin) * grid.nx * grid.ny;
+        grid.oz += z_begin * grid.vz;
+        grid.nz = z_count;
+    }
     const FdkViewCoef* coef = p->coef.as<FdkViewCoef>() + first;
     const bool aligned = (reinterpret_cast<uintptr_t>(filtered) & 15) == 0;
     if (layout == kFilteredPairs) {
@@ -488,6 +496,83 @@ YKB_API ykb_status ykb_fdk_execute_host(ykb_fdk_plan* p, const void* h_proj, int
         if (const ykb_status st = backproject_chunk(p, p->work_filtered.ptr, p->layout, p->ld,
                 view_offset + c, cnt, d_volume, accumulate, s))
             return st;
+    }
+    return YKB_OK;
+}
+
+YKB_API ykb_status ykb_fdk_execute_host_out(ykb_fdk_plan* p, const void* h_proj, int proj_dtype,
+    int view_offset, int n_views, float* d_volume, float* h_volume, int clear_output,
+    ykb_stream stream)
+{
+    clear_error();
+    if (const ykb_status st = check_range(p, h_proj, proj_dtype, view_offset, n_views)) return st;
+    if (!d_volume || !h_volume) return fail(YKB_ERR_INVALID_BUFFER, "null volume buffer");
+    DeviceGuard guard(p->device);
+    const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const size_t view_bytes = static_cast<size_t>(p->nu) * p->nv * dtype_bytes(proj_dtype);
+    const int batch = std::min(p->batch_capacity, std::max(16, (p->n_views + 7) / 8));
+    if (p->stage_views < batch || p->stage_in.bytes < 2 * batch * static_cast<size_t>(p->nu) * p->nv * 4) {
+        if (p->copy_stream) YKB_TRY_CUDA(cudaStreamSynchronize(p->copy_stream));
+        YKB_TRY_CUDA(cudaStreamSynchronize(s));
+        YKB_TRY_CUDA(p->stage_in.alloc(2 * static_cast<size_t>(batch) * p->nu * p->nv * 4));
+        p->stage_views = batch;
+    }
+    if (!p->copy_stream) {
+        YKB_TRY_CUDA(cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking));
+        for (int i = 0; i < 2; ++i) {
+            YKB_TRY_CUDA(cudaEventCreateWithFlags(&p->copied[i], cudaEventDisableTiming));
+            YKB_TRY_CUDA(cudaEventCreateWithFlags(&p->consumed[i], cudaEventDisableTiming));
+        }
+    }
+    YKB_TRY_CUDA(cudaEventRecord(p->consumed[0], s));
+    YKB_TRY_CUDA(cudaEventRecord(p->consumed[1], s));
+    const size_t slot_bytes = static_cast<size_t>(p->stage_views) * view_bytes;
+    // a short first batch: its copy is the one the kernels wait for
+    const int first_batch = std::min(batch, std::max(8, batch / 4));
+    // the last batch is backprojected in z slabs of whole 32-slice tiles, and
+    // each finished slab is copied to the host while the next is computed
+    const int nz = p->volume.nz;
+    const int slab = std::max(32, (nz / 4 + 31) / 32 * 32);
+    const size_t plane = static_cast<size_t>(p->volume.nx) * p->volume.ny;
+    for (int c = 0, b = 0; c < n_views; ++b) {
+        const int cnt = std::min(b == 0 ? first_batch : batch, n_views - c);
+        const int slot = b & 1;
+        char* dst = static_cast<char*>(p->stage_in.ptr) + slot * slot_bytes;
+        YKB_TRY_CUDA(cudaStreamWaitEvent(p->copy_stream, p->consumed[slot], 0));
+        YKB_TRY_CUDA(cudaMemcpyAsync(dst, static_cast<const char*>(h_proj) + c * view_bytes,
+            cnt * view_bytes, cudaMemcpyHostToDevice, p->copy_stream));
+        YKB_TRY_CUDA(cudaEventRecord(p->copied[slot], p->copy_stream));
+        YKB_TRY_CUDA(cudaStreamWaitEvent(s, p->copied[slot], 0));
+        if (const ykb_status st = filter_chunk(p, dst, proj_dtype, view_offset + c, cnt,
+                p->work_filtered.as<float>(), p->layout, p->ld, s))
+            return st;
+        YKB_TRY_CUDA(cudaEventRecord(p->consumed[slot], s));
+        const int accumulate = (c == 0 && clear_output) ? 0 : 1;
+        const bool last = c + cnt >= n_views;
+        if (!last) {
+            if (const ykb_status st = backproject_chunk(p, p->work_filtered.ptr, p->layout, p->ld,
+                    view_offset + c, cnt, d_volume, accumulate, s))
+                return st;
+        } else {
+            for (int z0 = 0, k = 0; z0 < nz; z0 += slab, ++k) {
+                const int zc = std::min(slab, nz - z0);
+                if (const ykb_status st = backproject_chunk(p, p->work_filtered.ptr, p->layout,
+                        p->ld, view_offset + c, cnt, d_volume, accumulate, s, z0, zc))
+                    return st;
+                // slab k is final: the copy stream downloads it behind the
+                // next slab's kernel (the event slots alternate, and a slot is
+                // reused only after the copy stream has waited on it)
+                cudaEvent_t done = p->copied[k & 1];
+                YKB_TRY_CUDA(cudaEventRecord(done, s));
+                YKB_TRY_CUDA(cudaStreamWaitEvent(p->copy_stream, done, 0));
+                YKB_TRY_CUDA(cudaMemcpyAsync(h_volume + z0 * plane, d_volume + z0 * plane,
+                    zc * plane * sizeof(float), cudaMemcpyDeviceToHost, p->copy_stream));
+            }
+            // the caller's stream completes when the host volume is complete
+            YKB_TRY_CUDA(cudaEventRecord(p->consumed[0], p->copy_stream));
+            YKB_TRY_CUDA(cudaStreamWaitEvent(s, p->consumed[0], 0));
+        }
+        c += cnt;
     }
     return YKB_OK;
 }

@@ -295,13 +295,22 @@ private:
         // host projections stream in batches, their copies overlapping the
         // kernels of earlier batches (the reference copies each 32-view chunk
         // synchronously: YkFdkPipeline.hpp:454-457)
-        const ykb_status st = r.projection.location == EMemoryLocation::Host
-            ? ykb_fdk_execute_host(fdk_, r.projection.data, YKB_DTYPE_F32, offset, count, d_vol,
-                  r.clear_output ? 1 : 0, stream_)
-            : ykb_fdk_execute(fdk_, r.projection.data, YKB_DTYPE_F32, offset, count, d_vol,
-                  r.clear_output ? 1 : 0, stream_);
+        const bool last = received_ + count == view_count_;
+        const bool host_vol = r.volume.location == EMemoryLocation::Host;
+        ykb_status st;
+        if (r.projection.location == EMemoryLocation::Host && host_vol && last)
+            // the final batch also returns the volume, its download
+            // overlapping the last backprojection slab by slab
+            st = ykb_fdk_execute_host_out(fdk_, r.projection.data, YKB_DTYPE_F32, offset, count,
+                d_vol, r.volume.data, r.clear_output ? 1 : 0, stream_);
+        else if (r.projection.location == EMemoryLocation::Host)
+            st = ykb_fdk_execute_host(fdk_, r.projection.data, YKB_DTYPE_F32, offset, count, d_vol,
+                r.clear_output ? 1 : 0, stream_);
+        else
+            st = ykb_fdk_execute(fdk_, r.projection.data, YKB_DTYPE_F32, offset, count, d_vol,
+                r.clear_output ? 1 : 0, stream_);
         if (st != YKB_OK) return fail_(EApiErrorCode::CudaError, ykb_last_error());
-        if (r.volume.location == EMemoryLocation::Host && received_ + count == view_count_) {
+        if (host_vol && last && r.projection.location != EMemoryLocation::Host) {
             const cudaError_t e = cudaMemcpyAsync(r.volume.data, d_vol, vol_bytes,
                 cudaMemcpyDeviceToHost, stream_);
             if (e != cudaSuccess) return cuda_fail_(e, "volume download");

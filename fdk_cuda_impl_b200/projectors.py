@@ -102,11 +102,15 @@ class FdkPlan:
         return volume
 
     def execute_host(self, proj: torch.Tensor, volume: torch.Tensor | None = None,
-                     view_offset: int = 0, clear: bool = True) -> torch.Tensor:
+                     view_offset: int = 0, clear: bool = True,
+                     host_out: torch.Tensor | None = None) -> torch.Tensor:
         """FDK of projections held in host memory (pin them for copy/compute
         overlap): batches stream to the device while earlier ones are filtered
-        and backprojected.  Asynchronous on the current stream; `proj` must
-        stay alive and unchanged until that stream has run the work."""
+        and backprojected.  With host_out (a contiguous float32 host tensor,
+        pinned for overlap) the volume is also copied there, slab by slab
+        behind the last batch's kernels (ykb_fdk_execute_host_out).
+        Asynchronous on the current stream; `proj` and `host_out` must stay
+        alive until that stream has run the work."""
         n = proj.shape[0]
         if proj.device.type != "cpu" or not proj.is_contiguous():
             raise ValueError("projections must be a contiguous host tensor")
@@ -114,10 +118,20 @@ class FdkPlan:
                                                                               torch.bfloat16):
             raise ValueError(f"projections must be float32/bfloat16 [n][{self.nv}][{self.nu}]")
         volume = self._vol_out(volume)
-        L.check(self.lib.ykb_fdk_execute_host(self._h, C.c_void_p(proj.data_ptr()),
-                                              _dtype_code(proj), view_offset, n,
-                                              C.c_void_p(volume.data_ptr()), 1 if clear else 0,
-                                              _stream_handle(self.device)))
+        if host_out is None:
+            L.check(self.lib.ykb_fdk_execute_host(self._h, C.c_void_p(proj.data_ptr()),
+                                                  _dtype_code(proj), view_offset, n,
+                                                  C.c_void_p(volume.data_ptr()), 1 if clear else 0,
+                                                  _stream_handle(self.device)))
+            return volume
+        if (host_out.device.type != "cpu" or not host_out.is_contiguous() or
+                host_out.dtype != torch.float32 or tuple(host_out.shape) != tuple(self.grid.shape)):
+            raise ValueError(f"host_out must be a contiguous float32 host tensor {self.grid.shape}")
+        L.check(self.lib.ykb_fdk_execute_host_out(self._h, C.c_void_p(proj.data_ptr()),
+                                                  _dtype_code(proj), view_offset, n,
+                                                  C.c_void_p(volume.data_ptr()),
+                                                  C.c_void_p(host_out.data_ptr()),
+                                                  1 if clear else 0, _stream_handle(self.device)))
         return volume
 
     def filter(self, proj: torch.Tensor, view_offset: int = 0) -> torch.Tensor:

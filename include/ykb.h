@@ -188,6 +188,19 @@ YKB_API ykb_status ykb_fdk_execute_host(ykb_fdk_plan* plan, const void* h_proj,
     int proj_dtype, int view_offset, int n_views, float* d_volume,
     int clear_output, ykb_stream stream);
 
+/* ykb_fdk_execute_host with the volume returned to host memory as well:
+ * the reconstruction accumulates in d_volume (device, [nz][ny][nx]) and is
+ * copied to h_volume (host; pin it for the copies to overlap).  The last
+ * projection batch is backprojected in z slabs and each finished slab is
+ * copied behind the next slab's kernel, so most of the volume download
+ * overlaps the GPU work.  Asynchronous on `stream`: the host volume is
+ * complete when the stream's work up to this call has run.  Replaces the
+ * Session's host-buffer FDK path (projection upload, FdkPipeline batches,
+ * volume download; src/interface/YkSession.cpp:693-728). */
+YKB_API ykb_status ykb_fdk_execute_host_out(ykb_fdk_plan* plan, const void* h_proj,
+    int proj_dtype, int view_offset, int n_views, float* d_volume, float* h_volume,
+    int clear_output, ykb_stream stream);
+
 /* Stage entry: preweight + ramp filter only; d_filtered receives
  * [n_views][nv][nu] float.  Replaces PreweightProcessor::apply +
  * FilterProcessor::apply (.../FDK/YkFDKPreWeightProcessor.hpp,

@@ -287,6 +287,32 @@ def test_fdk_execute_host_matches_device(oracle, cuda_device, pinned, precision)
     plan.close()
 
 
+@pytest.mark.parametrize("nz", [48, 100])
+def test_fdk_execute_host_out(oracle, cuda_device, nz):
+    # host projections in, host volume out: the last batch runs in z slabs of
+    # 32 slices whose downloads overlap the next slab (nz = 100: slabs of 32,
+    # 32, 32 and 4 slices)
+    import torch
+    from fdk_cuda_impl_b200.geometry import VolumeGrid
+    from fdk_cuda_impl_b200.projectors import FdkPlan
+    case = K.c1_small()
+    case.grid = VolumeGrid(64, 64, nz, (1.0, 1.0, 48.0 / nz))
+    views = case.scan.views()
+    p = torch.from_numpy(K.projections(oracle, case, views))
+    plan = FdkPlan(views, 96, 64, case.scan.scan_range, case.grid, case.filt)
+    dev = plan.execute(p.cuda()).cpu().numpy()
+    host = p.pin_memory()
+    out = torch.empty(case.grid.shape, dtype=torch.float32).pin_memory()
+    out.fill_(float("nan"))
+    for _ in range(2):  # a second call reuses the staging and events
+        vol = plan.execute_host(host, host_out=out)
+        torch.cuda.current_stream().synchronize()
+        plan.check()
+        assert K.rel_rmse(out.numpy(), dev) < 1e-6
+        assert torch.equal(out, vol.cpu())
+    plan.close()
+
+
 def _short_scan_case(start=0.3, direction=-1):
     from fdk_cuda_impl_b200.geometry import CircularScan
     case = K.c1_small()
