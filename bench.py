@@ -79,6 +79,30 @@ def chunk_views() -> int:
     return max(1, min(N_VIEWS, (8 << 30) // (12 * N_DET * N_DET)))
 
 
+def object_seed(rank: int) -> int:
+    """Seed of rank's phantom: each rank reconstructs its own object (weak
+    scaling, no data exchanged between ranks)."""
+    return 1000 + rank
+
+
+def max_over_ranks(x: float, world: int, device: str) -> float:
+    """The slowest rank's time: all ranks take part (same collective on every
+    rank), each gets the maximum."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.item()
+
+
+def job_gups(world: int, updates: int, ms: float) -> float:
+    """Whole-job throughput: every rank processes `updates` in the slowest
+    rank's time."""
+    return world * updates / (ms * 1e-3) / 1e9
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -253,9 +277,10 @@ def make_workload(rank: int, local: int):
     scan = CircularScan(N_VIEWS, N_VIEWS, SID, SDD, N_DET, N_DET, PIX_MM, PIX_MM)
     grid = VolumeGrid.cube(N_VOX, VOX_MM)
     views = scan.views()
-    ell = PH.random_ellipsoids(1000 + rank, N_ELL)
+    seed = object_seed(rank)
+    ell = PH.random_ellipsoids(seed, N_ELL)
     if N_SPH:
-        ell = np.concatenate([ell, PH.random_spheres(1000 + rank, N_SPH)])
+        ell = np.concatenate([ell, PH.random_spheres(seed, N_SPH)])
     phantom = PH.voxelize(grid, ell, device=f"cuda:{local}")
     dtype = torch.bfloat16 if PRECISION == "bf16" else torch.float32
     proj = torch.empty((N_VIEWS, N_DET, N_DET), dtype=dtype, device=f"cuda:{local}")
@@ -393,13 +418,6 @@ def main():
         if world > 1:
             dist.barrier()
 
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return t.item()
-
     def timed(fn, k):
         barrier()
         torch.cuda.synchronize()
@@ -410,7 +428,7 @@ def main():
         e1.record(stream)
         torch.cuda.synchronize()
         barrier()
-        return max_over_ranks(e0.elapsed_time(e1) / k)
+        return max_over_ranks(e0.elapsed_time(e1) / k, world, f"cuda:{local}")
 
     # full FDK steps, device resident
     for _ in range(args.warmup):
@@ -418,7 +436,7 @@ def main():
     with ClockSampler(local) as clocks:
         ms = timed(lambda: plan.execute(proj, vol), args.steps)
     clock_info = clocks.summary()
-    value = world * UPDATES / (ms * 1e-3) / 1e9
+    value = job_gups(world, UPDATES, ms)
 
     # stage timings for the roofline (same stream, CUDA events)
     filtered = plan.filter(proj)
@@ -443,7 +461,7 @@ def main():
     for _ in range(max(1, args.warmup - 1)):
         e2e_step()
     ms_e2e = timed(e2e_step, args.steps)
-    e2e_value = world * UPDATES / (ms_e2e * 1e-3) / 1e9
+    e2e_value = job_gups(world, UPDATES, ms_e2e)
 
     # BF16 form on the same views: projections stored in BF16 (host and
     # device), Shepp-Logan window, tcgen05 split hi/lo Toeplitz filter, the
