@@ -55,6 +55,28 @@ def phantom(O, case: Case) -> np.ndarray:
     return O.voxelize(vol, ell)
 
 
+def aligned_tilted():
+    """odd_case's geometry with a detector the reference accepts (its row
+    pitch and view size meet the texture alignment,
+    src/Reconstruction/Analytic/Circular/Flat/FDK/YkFdkPipeline.hpp:283-301)."""
+    scan = CircularScan(37, 36, 300.0, 650.0, 64, 40, 1.1, 0.9, start_angle_rad=0.2,
+                        rotation_direction=-1, source_offset_mm=(0.7, -0.3, 0.4),
+                        offset_unv_mm=(2.1, 0.0, -1.3), tilt_rad=(0.01, -0.015, 0.02))
+    grid = VolumeGrid(29, 23, 19, (0.9, 1.1, 1.3), (1.5, -2.0, 0.75))
+    return Case("tilted-aligned", scan, grid, RampFilter.named("hann", cutoff=0.4),
+                n_ellipsoids=5, seed=7, center_range=8.0, axis_min=2.0, axis_max=8.0)
+
+
+def smooth_projections(scan) -> np.ndarray:
+    """Constant 1 plus a slow cosine: no texture weight quantisation effect
+    at the 1e-6 level."""
+    v = np.arange(scan.rows)[:, None] / scan.rows
+    u = np.arange(scan.channels)[None, :] / scan.channels
+    img = 1.0 + 0.05 * np.cos(np.pi * u) * np.cos(np.pi * v)
+    return np.ascontiguousarray(np.broadcast_to(img, (scan.total_views, scan.rows, scan.channels)),
+                                dtype=np.float32)
+
+
 def oracle_volume(O, grid: VolumeGrid):
     return O.volume_struct(grid.shape, grid.voxel_mm, grid.center_mm)
 

@@ -33,27 +33,10 @@ pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not ref.available(), reason="oracle/_ref/libykref.so not built")]
 
 
-def _aligned_tilted():
-    # odd_case geometry with a detector the reference accepts (row pitch and
-    # view size must meet the texture alignment, YkFdkPipeline.hpp:283-301)
-    scan = CircularScan(37, 36, 300.0, 650.0, 64, 40, 1.1, 0.9, start_angle_rad=0.2,
-                        rotation_direction=-1, source_offset_mm=(0.7, -0.3, 0.4),
-                        offset_unv_mm=(2.1, 0.0, -1.3), tilt_rad=(0.01, -0.015, 0.02))
-    grid = VolumeGrid(29, 23, 19, (0.9, 1.1, 1.3), (1.5, -2.0, 0.75))
-    return K.Case("tilted-aligned", scan, grid, RampFilter.named("hann", cutoff=0.4),
-                  n_ellipsoids=5, seed=7, center_range=8.0, axis_min=2.0, axis_max=8.0)
+CASES = {"c1-small": K.c1_small, "tilted": K.aligned_tilted}
 
 
-CASES = {"c1-small": K.c1_small, "tilted": _aligned_tilted}
-
-
-def _smooth_proj(scan):
-    # constant 1 plus a slow cosine: no weight quantisation effect at 1e-6
-    v = np.arange(scan.rows)[:, None] / scan.rows
-    u = np.arange(scan.channels)[None, :] / scan.channels
-    img = 1.0 + 0.05 * np.cos(np.pi * u) * np.cos(np.pi * v)
-    return np.ascontiguousarray(np.broadcast_to(img, (scan.total_views, scan.rows, scan.channels)),
-                                dtype=np.float32)
+_smooth_proj = K.smooth_projections
 
 
 def _ykb_fdk(case, proj, filt=None):
