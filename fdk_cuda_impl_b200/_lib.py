@@ -95,6 +95,11 @@ SIGNATURES = {
     "ykb_joseph_workspace_bytes": (C.c_size_t, [_P]),
     "ykb_operator_apply": (C.c_int, [_P, C.c_int, _P, _P, C.c_int, _P]),
     "ykb_joseph_check": (C.c_int, [_P, _P]),
+    "ykb_iter_create": (C.c_int, [C.c_int, C.POINTER(_P)]),
+    "ykb_iter_destroy": (C.c_int, [_P]),
+    "ykb_dot_f64": (C.c_int, [_P, _P, _P, C.c_size_t, _P, _P]),
+    "ykb_cgls_update_xr": (C.c_int, [_P, _P, _P, _P, _P, C.c_size_t, _P, _P, C.c_size_t, _P]),
+    "ykb_cgls_update_p": (C.c_int, [_P, _P, _P, _P, _P, C.c_size_t, _P]),
 }
 
 # ykb_task == YK::ETask values

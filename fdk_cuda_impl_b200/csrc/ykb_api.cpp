@@ -875,6 +875,72 @@ YKB_API ykb_status ykb_joseph_check(ykb_joseph_plan* p, ykb_stream stream)
     return fail(YKB_ERR_CUDA, msg);
 }
 
+// ------------------------------------------------- iterative solvers ---
+YKB_API ykb_status ykb_iter_create(int device, ykb_iter** ctx)
+{
+    clear_error();
+    if (!ctx) return fail(YKB_ERR_INVALID_BUFFER, "null context output");
+    *ctx = nullptr;
+    if (const ykb_status st = check_device(device)) return st;
+    DeviceGuard guard(device);
+    ykb_iter* c = new (std::nothrow) ykb_iter();
+    if (!c) return fail(YKB_ERR_OUT_OF_MEMORY, "host allocation failed");
+    c->device = device;
+    const cudaError_t e = c->partials.alloc(sizeof(double) * dot_partial_count());
+    if (e != cudaSuccess) {
+        delete c;
+        return cuda_status(e, "cudaMalloc (reduction workspace)");
+    }
+    *ctx = c;
+    return YKB_OK;
+}
+
+YKB_API ykb_status ykb_iter_destroy(ykb_iter* ctx)
+{
+    clear_error();
+    if (!ctx) return YKB_OK;
+    DeviceGuard guard(ctx->device);
+    delete ctx;
+    return YKB_OK;
+}
+
+YKB_API ykb_status ykb_dot_f64(ykb_iter* ctx, const float* d_a, const float* d_b, size_t n,
+    double* d_result, ykb_stream stream)
+{
+    clear_error();
+    if (!ctx) return fail(YKB_ERR_INVALID_CONFIG, "null context");
+    if (!d_result || (n > 0 && (!d_a || !d_b))) return fail(YKB_ERR_INVALID_BUFFER, "null buffer");
+    DeviceGuard guard(ctx->device);
+    YKB_TRY_CUDA(launch_dot_f64(d_a, d_b, n, ctx->partials.as<double>(), d_result,
+        reinterpret_cast<cudaStream_t>(stream)));
+    return YKB_OK;
+}
+
+YKB_API ykb_status ykb_cgls_update_xr(ykb_iter* ctx, const double* d_gamma, const double* d_ww,
+    float* d_x, const float* d_p, size_t nx, float* d_r, const float* d_w, size_t nr,
+    ykb_stream stream)
+{
+    clear_error();
+    if (!ctx) return fail(YKB_ERR_INVALID_CONFIG, "null context");
+    if (!d_gamma || !d_ww || !d_x || !d_p || !d_r || !d_w) return fail(YKB_ERR_INVALID_BUFFER, "null buffer");
+    DeviceGuard guard(ctx->device);
+    YKB_TRY_CUDA(launch_cgls_xr(d_gamma, d_ww, d_x, d_p, nx, d_r, d_w, nr,
+        reinterpret_cast<cudaStream_t>(stream)));
+    return YKB_OK;
+}
+
+YKB_API ykb_status ykb_cgls_update_p(ykb_iter* ctx, const double* d_gamma_new,
+    const double* d_gamma_old, float* d_p, const float* d_z, size_t n, ykb_stream stream)
+{
+    clear_error();
+    if (!ctx) return fail(YKB_ERR_INVALID_CONFIG, "null context");
+    if (!d_gamma_new || !d_gamma_old || !d_p || !d_z) return fail(YKB_ERR_INVALID_BUFFER, "null buffer");
+    DeviceGuard guard(ctx->device);
+    YKB_TRY_CUDA(launch_cgls_p(d_gamma_new, d_gamma_old, d_p, d_z, n,
+        reinterpret_cast<cudaStream_t>(stream)));
+    return YKB_OK;
+}
+
 YKB_API ykb_status ykb_joseph_bp(ykb_joseph_plan* p, const float* d_proj, float* d_volume,
     int accumulate, ykb_stream stream)
 {

@@ -237,6 +237,15 @@ cudaError_t launch_joseph_fp(const float* slabs[3], const JosephView* views,
     int accumulate, cudaStream_t s);
 cudaError_t launch_joseph_ray_table(const JosephView* views, int n_views,
     int nu, int nv, float4* rays, float* lens, cudaStream_t s);
+// Iterative-solver vectors (iter_kernels.cu)
+int dot_partial_count();
+cudaError_t launch_dot_f64(const float* a, const float* b, size_t n, double* partials,
+    double* result, cudaStream_t s);
+cudaError_t launch_cgls_xr(const double* gamma, const double* ww, float* x, const float* p,
+    size_t nx, float* r, const float* w, size_t nr, cudaStream_t s);
+cudaError_t launch_cgls_p(const double* gamma_new, const double* gamma_old, float* p,
+    const float* z, size_t n, cudaStream_t s);
+
 // Siddon (siddon_kernels.cu); views in world coordinates
 cudaError_t launch_siddon_fp(const float* vol, const ykb_cone_view* views, int n_views, int nu,
     int nv, const VolumeGrid& g, float* proj, int accumulate, cudaStream_t s);
@@ -311,4 +320,9 @@ struct ykb_joseph_plan {
     ykb::DeviceBuffer pseudo_coef;     // PseudoViewCoef[n]
     ykb::DeviceBuffer pairs;           // projections as tap pairs [n][nv][pseudo_ld]
     ykb::DeviceBuffer err_flag;        // int[4]: device error word, box pre-pass scratch
+};
+
+struct ykb_iter {
+    int device = 0;
+    ykb::DeviceBuffer partials;  // double[dot_partial_count()]
 };

@@ -4,8 +4,10 @@ The consumers of the FP/BP operators that the reference drives from its
 iterative solvers (src/Reconstruction/Iterative/Flat/YkCglsBackends.hpp:22-196):
 
 * ``cgls``: CGLS with the Joseph pair and FP64 dot products, the algorithm of
-  the reference's ``CglsAstraBackend::run`` (:70-150).  The reference reduces
-  its dots in FP32 and synchronises the host on each one.
+  the reference's ``CglsAstraBackend::run`` (:70-150), on the library's
+  vector kernels (``IterVectors``).  The reference reduces its dots in FP32
+  and synchronises the host on each one; here the loop never waits on the
+  host.
 * ``unrolled_tv``: TV-regularised reconstruction by differentiating through
   unrolled iterations.  K gradient iterations
       x_{k+1} = x_k - alpha_k (A^T (A x_k - b) / m + lam grad TV(x_k))
@@ -23,11 +25,13 @@ explicitly, so each unrolled step is first-order in torch ops.
 """
 from __future__ import annotations
 
+import ctypes as C
 import math
 
 import torch
 from torch.utils.checkpoint import checkpoint
 
+from . import _lib as L
 from .autograd import JosephProjector
 from .projectors import JosephPlan
 
@@ -90,26 +94,86 @@ def power_norm(plan: JosephPlan, iters: int = 8, seed: int = 0) -> float:
     return lam
 
 
+class IterVectors:
+    """The library's vector kernels for iterative solvers (ykb_iter_*): FP64
+    dot products written on the device and CGLS updates whose step sizes
+    are read there, so a solver loop never waits on the host."""
+
+    def __init__(self, device: int = 0):
+        self.lib = L.load()
+        self.device = device
+        h = C.c_void_p()
+        L.check(self.lib.ykb_iter_create(device, C.byref(h)))
+        self._h = h
+
+    def dot(self, a: torch.Tensor, b: torch.Tensor, out: torch.Tensor) -> torch.Tensor:
+        """out (a float64 device scalar) = sum a * b in FP64."""
+        assert a.is_contiguous() and b.is_contiguous() and a.numel() == b.numel()
+        assert out.dtype == torch.float64 and out.numel() == 1
+        L.check(self.lib.ykb_dot_f64(self._h, C.c_void_p(a.data_ptr()), C.c_void_p(b.data_ptr()),
+                                     a.numel(), C.c_void_p(out.data_ptr()), _stream(self.device)))
+        return out
+
+    def update_xr(self, gamma, ww, x, p, r, w) -> None:
+        """x += (gamma / ww) p,  r -= (gamma / ww) w."""
+        L.check(self.lib.ykb_cgls_update_xr(self._h, C.c_void_p(gamma.data_ptr()),
+                                            C.c_void_p(ww.data_ptr()), C.c_void_p(x.data_ptr()),
+                                            C.c_void_p(p.data_ptr()), x.numel(),
+                                            C.c_void_p(r.data_ptr()), C.c_void_p(w.data_ptr()),
+                                            r.numel(), _stream(self.device)))
+
+    def update_p(self, gamma_new, gamma_old, p, z) -> None:
+        """p = z + (gamma_new / gamma_old) p."""
+        L.check(self.lib.ykb_cgls_update_p(self._h, C.c_void_p(gamma_new.data_ptr()),
+                                           C.c_void_p(gamma_old.data_ptr()),
+                                           C.c_void_p(p.data_ptr()), C.c_void_p(z.data_ptr()),
+                                           p.numel(), _stream(self.device)))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self.lib.ykb_iter_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _stream(device: int):
+    return C.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+
+
 def cgls(plan: JosephPlan, b: torch.Tensor, n_iter: int, x0: torch.Tensor | None = None):
-    """CGLS for min ||A x - b||^2 with FP64 dots.  Returns (x, residual norms)."""
-    x = torch.zeros(plan.grid.shape, device=b.device) if x0 is None else x0.clone()
+    """CGLS for min ||A x - b||^2 (the algorithm of the reference's
+    CglsAstraBackend::run) with FP64 dot products on the device.  The loop
+    enqueues work only: step sizes stay on the device (ykb_cgls_update_*),
+    and the residual norms are read once at the end.  Returns (x, residual
+    norms per iteration)."""
+    vec = IterVectors(plan.device)
+    dev = b.device
+    x = torch.zeros(plan.grid.shape, device=dev) if x0 is None else x0.clone()
     r = b - plan.forward(x)
     p = plan.adjoint(r)
-    gamma = float((p.double() * p.double()).sum())
-    norms = [float(torch.linalg.vector_norm(r.double()))]
-    for _ in range(n_iter):
-        w = plan.forward(p)
-        ww = float((w.double() * w.double()).sum())
-        if ww <= 1e-30:
-            break
-        alpha = gamma / ww
-        x.add_(p, alpha=alpha)
-        r.add_(w, alpha=-alpha)
-        z = plan.adjoint(r)
-        gamma1 = float((z.double() * z.double()).sum())
-        p.mul_(gamma1 / gamma).add_(z)
-        gamma = gamma1
-        norms.append(float(torch.linalg.vector_norm(r.double())))
+    w = torch.empty_like(r)
+    z = torch.empty_like(p)
+    # scalars: gamma for each iteration, |w|^2, |r|^2 per iteration
+    gamma = torch.zeros(n_iter + 1, dtype=torch.float64, device=dev)
+    ww = torch.zeros(1, dtype=torch.float64, device=dev)
+    rr = torch.zeros(n_iter + 1, dtype=torch.float64, device=dev)
+    vec.dot(p, p, gamma[0:1])
+    vec.dot(r, r, rr[0:1])
+    for k in range(n_iter):
+        plan.forward(p, w)
+        vec.dot(w, w, ww)
+        vec.update_xr(gamma[k:k + 1], ww, x, p, r, w)
+        plan.adjoint(r, z)
+        vec.dot(z, z, gamma[k + 1:k + 2])
+        vec.update_p(gamma[k + 1:k + 2], gamma[k:k + 1], p, z)
+        vec.dot(r, r, rr[k + 1:k + 2])
+    norms = [float(v) for v in torch.sqrt(rr).cpu()]
+    vec.close()
     return x, norms
 
 

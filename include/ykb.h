@@ -311,6 +311,33 @@ YKB_API ykb_status ykb_joseph_check(ykb_joseph_plan* plan, ykb_stream stream);
 /* Bytes of device workspace the plan holds (introspection). */
 YKB_API size_t ykb_joseph_workspace_bytes(const ykb_joseph_plan* plan);
 
+/* ------------------------------------------------- iterative solvers --- */
+
+/* Vector kernels for the solvers that drive the projector pair (CGLS,
+ * src/Reconstruction/Iterative/Flat/YkCglsBackends.hpp:70-150).  A context
+ * holds the reduction workspace of one device; calls on one context from
+ * streams without ordering between them race on it. */
+typedef struct ykb_iter ykb_iter;
+YKB_API ykb_status ykb_iter_create(int device, ykb_iter** ctx);
+YKB_API ykb_status ykb_iter_destroy(ykb_iter* ctx);
+
+/* *d_result = sum a[i] b[i] accumulated in FP64, deterministic, written on
+ * the device (no host synchronisation).  Replaces dot_launch
+ * (src/Reconstruction/Iterative/Common/kernels/YkIterKernels.cu:367-430),
+ * which reduces in FP32 and returns through the host. */
+YKB_API ykb_status ykb_dot_f64(ykb_iter* ctx, const float* d_a, const float* d_b, size_t n,
+    double* d_result, ykb_stream stream);
+
+/* CGLS updates with device-resident step sizes:
+ *   ykb_cgls_update_xr: x += a p, r -= a w with a = *d_gamma / *d_ww
+ *   ykb_cgls_update_p:  p = z + b p with b = *d_gamma_new / *d_gamma_old
+ * (a ratio with a zero denominator counts as 0). */
+YKB_API ykb_status ykb_cgls_update_xr(ykb_iter* ctx, const double* d_gamma, const double* d_ww,
+    float* d_x, const float* d_p, size_t nx, float* d_r, const float* d_w, size_t nr,
+    ykb_stream stream);
+YKB_API ykb_status ykb_cgls_update_p(ykb_iter* ctx, const double* d_gamma_new,
+    const double* d_gamma_old, float* d_p, const float* d_z, size_t n, ykb_stream stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -108,3 +108,42 @@ def test_tv_reconstruction_beats_reference_cgls_at_full_size():
         assert R.rel_rmse(xt, truth) < 0.95 * e_ref
     finally:
         plan.close()
+
+
+@pytest.mark.gpu
+def test_fp64_dot_and_cgls_updates():
+    # ykb_dot_f64 against an FP64 sum on the host, deterministic, on an
+    # unaligned length; the CGLS updates against the same torch expressions
+    if not torch.cuda.is_available():
+        pytest.skip("needs a GPU")
+    g = torch.Generator(device="cuda").manual_seed(5)
+    n = 10_000_003
+    a = torch.randn(n, device="cuda", generator=g)
+    b = torch.randn(n, device="cuda", generator=g)
+    vec = R.IterVectors(0)
+    out = torch.zeros(2, dtype=torch.float64, device="cuda")
+    vec.dot(a, b, out[0:1])
+    vec.dot(a, b, out[1:2])
+    ref = float((a.double() * b.double()).sum())
+    assert abs(float(out[0]) - ref) <= 1e-12 * abs(ref) + 1e-9
+    assert float(out[0]) == float(out[1])
+    # a misaligned view takes the scalar path
+    vec.dot(a[1:], b[1:], out[0:1])
+    ref1 = float((a[1:].double() * b[1:].double()).sum())
+    assert abs(float(out[0]) - ref1) <= 1e-12 * abs(ref1) + 1e-9
+    gam = torch.tensor([3.0], dtype=torch.float64, device="cuda")
+    ww = torch.tensor([2.0], dtype=torch.float64, device="cuda")
+    x, p, r, w = a[:1000].clone(), b[:1000].clone(), a[1000:3000].clone(), b[1000:3000].clone()
+    x0, r0 = x.clone(), r.clone()
+    vec.update_xr(gam, ww, x, p, r, w)
+    assert torch.allclose(x, x0 + 1.5 * p, rtol=1e-6, atol=1e-6)
+    assert torch.allclose(r, r0 - 1.5 * w, rtol=1e-6, atol=1e-6)
+    z = a[5000:6000].clone()
+    p0 = p.clone()
+    vec.update_p(gam, ww, p, z)
+    assert torch.allclose(p, z + 1.5 * p0, rtol=1e-6, atol=1e-6)
+    zero = torch.zeros(1, dtype=torch.float64, device="cuda")
+    x1 = x.clone()
+    vec.update_xr(gam, zero, x, p, r, w)  # a zero denominator leaves x, r as they were
+    assert torch.equal(x, x1)
+    vec.close()
