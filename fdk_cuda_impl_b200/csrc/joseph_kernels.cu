@@ -89,6 +89,8 @@ __global__ void __launch_bounds__(128) joseph_fp_kernel(const float* __restrict_
         slice_range(r.a2, r.e2, j.n2, j.n0, lo, hi);
         const long plane = static_cast<long>(j.n1) * j.n2;
         const float half = 0.5f * (j.n0 - 1);
+        // unrolled: the four gathers of several samples are in flight at once
+#pragma unroll 4
         for (int s = lo; s <= hi; ++s) {
             const float c0 = static_cast<float>(s) - half;
             const float f1 = fmaf(r.a1, c0, r.e1);
