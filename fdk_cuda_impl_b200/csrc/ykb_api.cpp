@@ -370,6 +370,82 @@ ykb_status backproject_chunk(ykb_fdk_plan* p, const void* filtered, int layout, 
     return YKB_OK;
 }
 
+// Host projections streamed through the plan: batches of about an eighth
+// of the views (at least 16; a short first batch, whose copy the kernels
+// wait for) are copied on the plan's copy stream into two staging slots,
+// double-buffered against the filter and backprojection on `s`.  With
+// h_volume, the last batch is backprojected in z slabs of whole 32-slice
+// tiles and each finished slab is copied to h_volume behind the next slab's
+// kernel; `s` then completes with the host volume.
+ykb_status stream_host(ykb_fdk_plan* p, const void* h_proj, int proj_dtype, int view_offset,
+    int n_views, float* d_volume, float* h_volume, int clear_output, cudaStream_t s)
+{
+    const size_t view_bytes = static_cast<size_t>(p->nu) * p->nv * dtype_bytes(proj_dtype);
+    const int batch = std::min(p->batch_capacity, std::max(16, (p->n_views + 7) / 8));
+    if (p->stage_views < batch || p->stage_in.bytes < 2 * batch * static_cast<size_t>(p->nu) * p->nv * 4) {
+        if (p->copy_stream) YKB_TRY_CUDA(cudaStreamSynchronize(p->copy_stream));
+        YKB_TRY_CUDA(cudaStreamSynchronize(s));
+        YKB_TRY_CUDA(p->stage_in.alloc(2 * static_cast<size_t>(batch) * p->nu * p->nv * 4));
+        p->stage_views = batch;
+    }
+    if (!p->copy_stream) {
+        YKB_TRY_CUDA(cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking));
+        for (int i = 0; i < 2; ++i) {
+            YKB_TRY_CUDA(cudaEventCreateWithFlags(&p->copied[i], cudaEventDisableTiming));
+            YKB_TRY_CUDA(cudaEventCreateWithFlags(&p->consumed[i], cudaEventDisableTiming));
+        }
+    }
+    // the copy stream starts after work already queued on `s` that may
+    // still read the staging slots (a previous call)
+    YKB_TRY_CUDA(cudaEventRecord(p->consumed[0], s));
+    YKB_TRY_CUDA(cudaEventRecord(p->consumed[1], s));
+    const size_t slot_bytes = static_cast<size_t>(p->stage_views) * view_bytes;
+    const int first_batch = std::min(batch, std::max(8, batch / 4));
+    const int nz = p->volume.nz;
+    const int slab = std::max(32, (nz / 4 + 31) / 32 * 32);
+    const size_t plane = static_cast<size_t>(p->volume.nx) * p->volume.ny;
+    for (int c = 0, b = 0; c < n_views; ++b) {
+        const int cnt = std::min(b == 0 ? first_batch : batch, n_views - c);
+        const int slot = b & 1;
+        char* dst = static_cast<char*>(p->stage_in.ptr) + slot * slot_bytes;
+        YKB_TRY_CUDA(cudaStreamWaitEvent(p->copy_stream, p->consumed[slot], 0));
+        YKB_TRY_CUDA(cudaMemcpyAsync(dst, static_cast<const char*>(h_proj) + c * view_bytes,
+            cnt * view_bytes, cudaMemcpyHostToDevice, p->copy_stream));
+        YKB_TRY_CUDA(cudaEventRecord(p->copied[slot], p->copy_stream));
+        YKB_TRY_CUDA(cudaStreamWaitEvent(s, p->copied[slot], 0));
+        if (const ykb_status st = filter_chunk(p, dst, proj_dtype, view_offset + c, cnt,
+                p->work_filtered.as<float>(), p->layout, p->ld, s))
+            return st;
+        YKB_TRY_CUDA(cudaEventRecord(p->consumed[slot], s));
+        const int accumulate = (c == 0 && clear_output) ? 0 : 1;
+        const bool last = c + cnt >= n_views;
+        if (!last || !h_volume) {
+            if (const ykb_status st = backproject_chunk(p, p->work_filtered.ptr, p->layout, p->ld,
+                    view_offset + c, cnt, d_volume, accumulate, s))
+                return st;
+        } else {
+            for (int z0 = 0, k = 0; z0 < nz; z0 += slab, ++k) {
+                const int zc = std::min(slab, nz - z0);
+                if (const ykb_status st = backproject_chunk(p, p->work_filtered.ptr, p->layout,
+                        p->ld, view_offset + c, cnt, d_volume, accumulate, s, z0, zc))
+                    return st;
+                // slab k is final: the copy stream downloads it behind the
+                // next slab's kernel (each wait binds to the record just made)
+                cudaEvent_t done = p->copied[k & 1];
+                YKB_TRY_CUDA(cudaEventRecord(done, s));
+                YKB_TRY_CUDA(cudaStreamWaitEvent(p->copy_stream, done, 0));
+                YKB_TRY_CUDA(cudaMemcpyAsync(h_volume + z0 * plane, d_volume + z0 * plane,
+                    zc * plane * sizeof(float), cudaMemcpyDeviceToHost, p->copy_stream));
+            }
+            // the caller's stream completes when the host volume is complete
+            YKB_TRY_CUDA(cudaEventRecord(p->consumed[0], p->copy_stream));
+            YKB_TRY_CUDA(cudaStreamWaitEvent(s, p->consumed[0], 0));
+        }
+        c += cnt;
+    }
+    return YKB_OK;
+}
+
 } // namespace
 
 YKB_API ykb_status ykb_fdk_filter(ykb_fdk_plan* p, const void* d_proj, int proj_dtype,
@@ -456,48 +532,8 @@ YKB_API ykb_status ykb_fdk_execute_host(ykb_fdk_plan* p, const void* h_proj, int
     if (const ykb_status st = check_range(p, h_proj, proj_dtype, view_offset, n_views)) return st;
     if (!d_volume) return fail(YKB_ERR_INVALID_BUFFER, "null volume buffer");
     DeviceGuard guard(p->device);
-    const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    const size_t view_bytes = static_cast<size_t>(p->nu) * p->nv * dtype_bytes(proj_dtype);
-    // batches of about an eighth of the views (at least 16): the first
-    // batch's copy is the only one left exposed
-    const int batch = std::min(p->batch_capacity, std::max(16, (p->n_views + 7) / 8));
-    if (p->stage_views < batch || p->stage_in.bytes < 2 * batch * static_cast<size_t>(p->nu) * p->nv * 4) {
-        if (p->copy_stream) YKB_TRY_CUDA(cudaStreamSynchronize(p->copy_stream));
-        YKB_TRY_CUDA(cudaStreamSynchronize(s));
-        YKB_TRY_CUDA(p->stage_in.alloc(2 * static_cast<size_t>(batch) * p->nu * p->nv * 4));
-        p->stage_views = batch;
-    }
-    if (!p->copy_stream) {
-        YKB_TRY_CUDA(cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking));
-        for (int i = 0; i < 2; ++i) {
-            YKB_TRY_CUDA(cudaEventCreateWithFlags(&p->copied[i], cudaEventDisableTiming));
-            YKB_TRY_CUDA(cudaEventCreateWithFlags(&p->consumed[i], cudaEventDisableTiming));
-        }
-    }
-    // the copy stream starts after work already queued on `stream` that may
-    // still read the staging slots (a previous call)
-    YKB_TRY_CUDA(cudaEventRecord(p->consumed[0], s));
-    YKB_TRY_CUDA(cudaEventRecord(p->consumed[1], s));
-    const size_t slot_bytes = static_cast<size_t>(p->stage_views) * view_bytes;
-    for (int c = 0, b = 0; c < n_views; c += batch, ++b) {
-        const int cnt = std::min(batch, n_views - c);
-        const int slot = b & 1;
-        char* dst = static_cast<char*>(p->stage_in.ptr) + slot * slot_bytes;
-        YKB_TRY_CUDA(cudaStreamWaitEvent(p->copy_stream, p->consumed[slot], 0));
-        YKB_TRY_CUDA(cudaMemcpyAsync(dst, static_cast<const char*>(h_proj) + c * view_bytes,
-            cnt * view_bytes, cudaMemcpyHostToDevice, p->copy_stream));
-        YKB_TRY_CUDA(cudaEventRecord(p->copied[slot], p->copy_stream));
-        YKB_TRY_CUDA(cudaStreamWaitEvent(s, p->copied[slot], 0));
-        if (const ykb_status st = filter_chunk(p, dst, proj_dtype, view_offset + c, cnt,
-                p->work_filtered.as<float>(), p->layout, p->ld, s))
-            return st;
-        YKB_TRY_CUDA(cudaEventRecord(p->consumed[slot], s));
-        const int accumulate = (c == 0 && clear_output) ? 0 : 1;
-        if (const ykb_status st = backproject_chunk(p, p->work_filtered.ptr, p->layout, p->ld,
-                view_offset + c, cnt, d_volume, accumulate, s))
-            return st;
-    }
-    return YKB_OK;
+    return stream_host(p, h_proj, proj_dtype, view_offset, n_views, d_volume, nullptr,
+        clear_output, reinterpret_cast<cudaStream_t>(stream));
 }
 
 YKB_API ykb_status ykb_fdk_execute_host_out(ykb_fdk_plan* p, const void* h_proj, int proj_dtype,
@@ -508,73 +544,8 @@ YKB_API ykb_status ykb_fdk_execute_host_out(ykb_fdk_plan* p, const void* h_proj,
     if (const ykb_status st = check_range(p, h_proj, proj_dtype, view_offset, n_views)) return st;
     if (!d_volume || !h_volume) return fail(YKB_ERR_INVALID_BUFFER, "null volume buffer");
     DeviceGuard guard(p->device);
-    const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    const size_t view_bytes = static_cast<size_t>(p->nu) * p->nv * dtype_bytes(proj_dtype);
-    const int batch = std::min(p->batch_capacity, std::max(16, (p->n_views + 7) / 8));
-    if (p->stage_views < batch || p->stage_in.bytes < 2 * batch * static_cast<size_t>(p->nu) * p->nv * 4) {
-        if (p->copy_stream) YKB_TRY_CUDA(cudaStreamSynchronize(p->copy_stream));
-        YKB_TRY_CUDA(cudaStreamSynchronize(s));
-        YKB_TRY_CUDA(p->stage_in.alloc(2 * static_cast<size_t>(batch) * p->nu * p->nv * 4));
-        p->stage_views = batch;
-    }
-    if (!p->copy_stream) {
-        YKB_TRY_CUDA(cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking));
-        for (int i = 0; i < 2; ++i) {
-            YKB_TRY_CUDA(cudaEventCreateWithFlags(&p->copied[i], cudaEventDisableTiming));
-            YKB_TRY_CUDA(cudaEventCreateWithFlags(&p->consumed[i], cudaEventDisableTiming));
-        }
-    }
-    YKB_TRY_CUDA(cudaEventRecord(p->consumed[0], s));
-    YKB_TRY_CUDA(cudaEventRecord(p->consumed[1], s));
-    const size_t slot_bytes = static_cast<size_t>(p->stage_views) * view_bytes;
-    // a short first batch: its copy is the one the kernels wait for
-    const int first_batch = std::min(batch, std::max(8, batch / 4));
-    // the last batch is backprojected in z slabs of whole 32-slice tiles, and
-    // each finished slab is copied to the host while the next is computed
-    const int nz = p->volume.nz;
-    const int slab = std::max(32, (nz / 4 + 31) / 32 * 32);
-    const size_t plane = static_cast<size_t>(p->volume.nx) * p->volume.ny;
-    for (int c = 0, b = 0; c < n_views; ++b) {
-        const int cnt = std::min(b == 0 ? first_batch : batch, n_views - c);
-        const int slot = b & 1;
-        char* dst = static_cast<char*>(p->stage_in.ptr) + slot * slot_bytes;
-        YKB_TRY_CUDA(cudaStreamWaitEvent(p->copy_stream, p->consumed[slot], 0));
-        YKB_TRY_CUDA(cudaMemcpyAsync(dst, static_cast<const char*>(h_proj) + c * view_bytes,
-            cnt * view_bytes, cudaMemcpyHostToDevice, p->copy_stream));
-        YKB_TRY_CUDA(cudaEventRecord(p->copied[slot], p->copy_stream));
-        YKB_TRY_CUDA(cudaStreamWaitEvent(s, p->copied[slot], 0));
-        if (const ykb_status st = filter_chunk(p, dst, proj_dtype, view_offset + c, cnt,
-                p->work_filtered.as<float>(), p->layout, p->ld, s))
-            return st;
-        YKB_TRY_CUDA(cudaEventRecord(p->consumed[slot], s));
-        const int accumulate = (c == 0 && clear_output) ? 0 : 1;
-        const bool last = c + cnt >= n_views;
-        if (!last) {
-            if (const ykb_status st = backproject_chunk(p, p->work_filtered.ptr, p->layout, p->ld,
-                    view_offset + c, cnt, d_volume, accumulate, s))
-                return st;
-        } else {
-            for (int z0 = 0, k = 0; z0 < nz; z0 += slab, ++k) {
-                const int zc = std::min(slab, nz - z0);
-                if (const ykb_status st = backproject_chunk(p, p->work_filtered.ptr, p->layout,
-                        p->ld, view_offset + c, cnt, d_volume, accumulate, s, z0, zc))
-                    return st;
-                // slab k is final: the copy stream downloads it behind the
-                // next slab's kernel (the event slots alternate, and a slot is
-                // reused only after the copy stream has waited on it)
-                cudaEvent_t done = p->copied[k & 1];
-                YKB_TRY_CUDA(cudaEventRecord(done, s));
-                YKB_TRY_CUDA(cudaStreamWaitEvent(p->copy_stream, done, 0));
-                YKB_TRY_CUDA(cudaMemcpyAsync(h_volume + z0 * plane, d_volume + z0 * plane,
-                    zc * plane * sizeof(float), cudaMemcpyDeviceToHost, p->copy_stream));
-            }
-            // the caller's stream completes when the host volume is complete
-            YKB_TRY_CUDA(cudaEventRecord(p->consumed[0], p->copy_stream));
-            YKB_TRY_CUDA(cudaStreamWaitEvent(s, p->consumed[0], 0));
-        }
-        c += cnt;
-    }
-    return YKB_OK;
+    return stream_host(p, h_proj, proj_dtype, view_offset, n_views, d_volume, h_volume,
+        clear_output, reinterpret_cast<cudaStream_t>(stream));
 }
 
 YKB_API ykb_status ykb_fdk_check(ykb_fdk_plan* p, ykb_stream stream)
