@@ -370,10 +370,12 @@ ykb_status backproject_chunk(ykb_fdk_plan* p, const void* filtered, int layout, 
     return YKB_OK;
 }
 
-// Host projections streamed through the plan: batches of about an eighth
-// of the views (at least 16; a short first batch, whose copy the kernels
-// wait for) are copied on the plan's copy stream into two staging slots,
-// double-buffered against the filter and backprojection on `s`.  With
+// Host projections streamed through the plan, copied on the plan's copy
+// stream into two staging slots double-buffered against the filter and
+// backprojection on `s`.  Batches grow geometrically from 16 views up to a
+// quarter of the views: the kernels wait only for the first, short copy,
+// and each later copy (a view copies in about a third of the time its
+// kernels take) completes while the previous batch is processed.  With
 // h_volume, the last batch is backprojected in z slabs of whole 32-slice
 // tiles and each finished slab is copied to h_volume behind the next slab's
 // kernel; `s` then completes with the host volume.
@@ -381,7 +383,7 @@ ykb_status stream_host(ykb_fdk_plan* p, const void* h_proj, int proj_dtype, int 
     int n_views, float* d_volume, float* h_volume, int clear_output, cudaStream_t s)
 {
     const size_t view_bytes = static_cast<size_t>(p->nu) * p->nv * dtype_bytes(proj_dtype);
-    const int batch = std::min(p->batch_capacity, std::max(16, (p->n_views + 7) / 8));
+    const int batch = std::min(p->batch_capacity, std::max(16, (p->n_views + 3) / 4));
     if (p->stage_views < batch || p->stage_in.bytes < 2 * batch * static_cast<size_t>(p->nu) * p->nv * 4) {
         if (p->copy_stream) YKB_TRY_CUDA(cudaStreamSynchronize(p->copy_stream));
         YKB_TRY_CUDA(cudaStreamSynchronize(s));
@@ -400,12 +402,14 @@ ykb_status stream_host(ykb_fdk_plan* p, const void* h_proj, int proj_dtype, int 
     YKB_TRY_CUDA(cudaEventRecord(p->consumed[0], s));
     YKB_TRY_CUDA(cudaEventRecord(p->consumed[1], s));
     const size_t slot_bytes = static_cast<size_t>(p->stage_views) * view_bytes;
-    const int first_batch = std::min(batch, std::max(8, batch / 4));
+    int next_batch = std::min(batch, 16);
     const int nz = p->volume.nz;
-    const int slab = std::max(32, (nz / 4 + 31) / 32 * 32);
+    // eighths of the volume: the download of the last slab is what stays exposed
+    const int slab = std::max(32, (nz / 8 + 31) / 32 * 32);
     const size_t plane = static_cast<size_t>(p->volume.nx) * p->volume.ny;
     for (int c = 0, b = 0; c < n_views; ++b) {
-        const int cnt = std::min(b == 0 ? first_batch : batch, n_views - c);
+        const int cnt = std::min(next_batch, n_views - c);
+        next_batch = std::min(batch, 2 * next_batch);
         const int slot = b & 1;
         char* dst = static_cast<char*>(p->stage_in.ptr) + slot * slot_bytes;
         YKB_TRY_CUDA(cudaStreamWaitEvent(p->copy_stream, p->consumed[slot], 0));
