@@ -119,3 +119,31 @@ def test_product_does_not_import_oracle():
             if f.endswith((".py", ".cpp", ".cu", ".hpp", ".h")):
                 text = open(os.path.join(dirpath, f)).read()
                 assert "oracle" not in text.lower().replace("oracles", ""), f
+
+
+def test_operator_and_solver_entry_points_validate_arguments(ykb_lib):
+    # null plans and contexts are status codes, never a crash; the release
+    # functions accept NULL
+    assert ykb_lib.ykb_operator_apply(None, L.TASK_FP_JOSEPH, None, None, 0, None) == \
+        L.ERR_INVALID_CONFIG
+    assert ykb_lib.ykb_joseph_check(None, None) == L.ERR_INVALID_CONFIG
+    assert ykb_lib.ykb_fdk_execute_host_out(None, None, 0, 0, 1, None, None, 1, None) == \
+        L.ERR_INVALID_CONFIG
+    assert ykb_lib.ykb_iter_create(0, None) == L.ERR_INVALID_BUFFER
+    assert ykb_lib.ykb_iter_destroy(None) == L.OK
+    assert ykb_lib.ykb_dot_f64(None, None, None, 0, None, None) == L.ERR_INVALID_CONFIG
+    assert ykb_lib.ykb_cgls_update_xr(None, None, None, None, None, 0, None, None, 0, None) == \
+        L.ERR_INVALID_CONFIG
+    assert ykb_lib.ykb_cgls_update_p(None, None, None, None, None, 0, None) == \
+        L.ERR_INVALID_CONFIG
+    assert ykb_lib.ykb_joseph_plan_destroy(None) == L.OK
+
+
+def test_solver_context_without_gpu(ykb_lib):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    h = C.c_void_p()
+    assert ykb_lib.ykb_iter_create(0, C.byref(h)) in (L.ERR_CUDA, L.ERR_INVALID_CONFIG)
+    assert not h.value
+    assert ykb_lib.ykb_last_error()
