@@ -260,6 +260,24 @@ def test_bf16_form_c1(oracle, cuda_device):
     assert K.rel_rmse(out, ref) <= BF16_TOL
 
 
+@pytest.mark.parametrize("precision,tol", [("fp32", FP32_TOL), ("bf16", BF16_TOL)])
+@pytest.mark.parametrize("tilted", [False, True])
+def test_fdk_filter_column_tiles(oracle, cuda_device, precision, tol, tilted):
+    # nu = 300 runs the tensor-core filter in five 64-column tiles; the tap
+    # pair across each tile edge is written in halves by two CTAs.  The
+    # 37-row detector truncates the volume's projection, so the first and
+    # last rows are sampled too.
+    from fdk_cuda_impl_b200.geometry import CircularScan, VolumeGrid
+    kw = dict(tilt_rad=(0.01, -0.015, 0.02), offset_unv_mm=(2.1, 0.0, -1.3)) if tilted else {}
+    case = K.c1_small()
+    case.scan = CircularScan(40, 40, 500.0, 1000.0, 300, 37, 0.5, 1.7, **kw)
+    case.grid = VolumeGrid(64, 64, 40, (1.0, 1.0, 1.0))
+    out, ref, plan, *_ = _run_case(oracle, case, precision=precision)
+    assert np.isfinite(out).all()
+    assert K.rel_rmse(out, ref) <= tol
+    plan.close()
+
+
 @pytest.mark.parametrize("pinned", [True, False])
 @pytest.mark.parametrize("precision", ["fp32", "bf16"])
 def test_fdk_execute_host_matches_device(oracle, cuda_device, pinned, precision):
