@@ -375,7 +375,8 @@ ykb_status backproject_chunk(ykb_fdk_plan* p, const void* filtered, int layout, 
 // backprojection on `s`.  Batches grow geometrically from 16 views up to a
 // quarter of the views: the kernels wait only for the first, short copy,
 // and each later copy (a view copies in about a third of the time its
-// kernels take) completes while the previous batch is processed.  With
+// kernels take) completes while the previous batch is processed; a
+// remainder of between one and two batches runs as two halves.  With
 // h_volume, the last batch is backprojected in z slabs of whole 32-slice
 // tiles and each finished slab is copied to h_volume behind the next slab's
 // kernel; `s` then completes with the host volume.
@@ -408,7 +409,11 @@ ykb_status stream_host(ykb_fdk_plan* p, const void* h_proj, int proj_dtype, int 
     const int slab = std::max(32, (nz / 8 + 31) / 32 * 32);
     const size_t plane = static_cast<size_t>(p->volume.nx) * p->volume.ny;
     for (int c = 0, b = 0; c < n_views; ++b) {
-        const int cnt = std::min(next_batch, n_views - c);
+        // between one and two batches left: two halves, so that the last
+        // batch, whose slabs hide the volume download, is never a short tail
+        const int rest = n_views - c;
+        const int cnt = rest > next_batch && rest < 2 * next_batch ? (rest + 1) / 2
+                                                                  : std::min(next_batch, rest);
         next_batch = std::min(batch, 2 * next_batch);
         const int slot = b & 1;
         char* dst = static_cast<char*>(p->stage_in.ptr) + slot * slot_bytes;
