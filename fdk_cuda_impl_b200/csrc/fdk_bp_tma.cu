@@ -3,8 +3,10 @@
 // Same arithmetic as fdk_bp_kernel in fdk_kernels.cu (the math of
 // .../FDK/kernels/YkFDKBpKernels.cu:112-209 with exact software bilinear
 // weights), organised for Blackwell:
-//   * a CTA owns a 16x16x32 voxel tile; each of its 256 consumer threads walks
-//     a 32-voxel z-column and keeps the 32 sums in registers over all views;
+//   * a CTA owns a 16x16x48 voxel tile; each of its 256 consumer threads walks
+//     a 48-voxel z-column and keeps the 48 sums in registers over all views
+//     (the longer the column, the more voxels share the per-view column
+//     terms; 48 sums still fit two CTAs per SM);
 //   * one producer warp computes, per view, the detector box covering the
 //     tile's footprint (+1 bilinear tap, +1 pixel margin) and loads it with
 //     cp.async.bulk.tensor (3D tile mode, this GPU's memory only, no
@@ -33,7 +35,7 @@
 namespace ykb {
 namespace {
 
-constexpr int TX = 16, TY = 16, ZT = 32;
+constexpr int TX = 16, TY = 16, ZT = 48;
 constexpr int NCONS = TX * TY;          // consumer threads
 constexpr int NCWARPS = NCONS / 32;
 constexpr int NTHREADS = NCONS + 32;    // + producer warp
@@ -700,6 +702,8 @@ cudaError_t fdk_tma_box(const FdkViewCoef* coef, int n_views, const VolumeGrid& 
     if (*bh > 256) *bw = 0;
     return cudaSuccess;
 }
+
+int fdk_tma_z_tile() { return ZT; }
 
 // Stages that fit the shared-memory budget for a box (0 when fewer than 2).
 int fdk_tma_stages(int bw, int bh, int layout)

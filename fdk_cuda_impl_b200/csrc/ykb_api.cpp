@@ -342,7 +342,7 @@ ykb_status filter_chunk(ykb_fdk_plan* p, const void* proj, int proj_dtype, int f
 // weighted backprojection of `count` filtered views (FilteredLayout
 // `layout`, row pitch ld elements) starting at plan view `first`
 // z_begin/z_count restrict the work to volume slices [z_begin, z_begin +
-// z_count) (z_count < 0: all); z_begin must be a multiple of 32, the z tile
+// z_count) (z_count < 0: all); z_begin must be a multiple of fdk_tma_z_tile()
 // of the TMA backprojection, so that its tiles are those of the box pre-pass
 ykb_status backproject_chunk(ykb_fdk_plan* p, const void* filtered, int layout, int ld, int first,
     int count, float* vol, int accumulate, cudaStream_t s, int z_begin = 0, int z_count = -1)
@@ -377,7 +377,7 @@ ykb_status backproject_chunk(ykb_fdk_plan* p, const void* filtered, int layout, 
 // and each later copy (a view copies in about a third of the time its
 // kernels take) completes while the previous batch is processed; a
 // remainder of between one and two batches runs as two halves.  With
-// h_volume, the last batch is backprojected in z slabs of whole 32-slice
+// h_volume, the last batch is backprojected in z slabs of whole z
 // tiles and each finished slab is copied to h_volume behind the next slab's
 // kernel; `s` then completes with the host volume.
 ykb_status stream_host(ykb_fdk_plan* p, const void* h_proj, int proj_dtype, int view_offset,
@@ -405,8 +405,10 @@ ykb_status stream_host(ykb_fdk_plan* p, const void* h_proj, int proj_dtype, int 
     const size_t slot_bytes = static_cast<size_t>(p->stage_views) * view_bytes;
     int next_batch = std::min(batch, 16);
     const int nz = p->volume.nz;
-    // eighths of the volume: the download of the last slab is what stays exposed
-    const int slab = std::max(32, (nz / 8 + 31) / 32 * 32);
+    // eighths of the volume in whole z tiles: the download of the last slab
+    // is what stays exposed
+    const int zt = fdk_tma_z_tile();
+    const int slab = std::max(zt, (nz / 8 + zt - 1) / zt * zt);
     const size_t plane = static_cast<size_t>(p->volume.nx) * p->volume.ny;
     for (int c = 0, b = 0; c < n_views; ++b) {
         // between one and two batches left: two halves, so that the last

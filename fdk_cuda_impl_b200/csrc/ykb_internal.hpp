@@ -213,6 +213,8 @@ cudaError_t launch_fdk_backproject(const void* filtered, int dtype,
 // TMA-staged backprojection (fdk_bp_tma.cu)
 bool fdk_tma_available();
 int fdk_tma_stages(int bw, int bh, int layout);
+// z slices per tile of the TMA backprojection (slab work starts on a tile)
+int fdk_tma_z_tile();
 cudaError_t fdk_tma_box(const FdkViewCoef* coef, int n_views, const VolumeGrid& g,
     int* scratch2, int* bw, int* bh, cudaStream_t s);
 // pseudo != nullptr: the pseudo-matched weight of PseudoViewCoef replaces the

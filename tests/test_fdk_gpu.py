@@ -308,8 +308,8 @@ def test_fdk_execute_host_matches_device(oracle, cuda_device, pinned, precision)
 @pytest.mark.parametrize("nz", [48, 100])
 def test_fdk_execute_host_out(oracle, cuda_device, nz):
     # host projections in, host volume out: the last batch runs in z slabs of
-    # 32 slices whose downloads overlap the next slab (nz = 100: slabs of 32,
-    # 32, 32 and 4 slices)
+    # whole 48-slice z tiles whose downloads overlap the next slab (nz = 48:
+    # one slab; nz = 100: slabs of 48, 48 and 4 slices)
     import torch
     from fdk_cuda_impl_b200.geometry import VolumeGrid
     from fdk_cuda_impl_b200.projectors import FdkPlan
