@@ -6,7 +6,8 @@
 //   * a CTA owns a 16x16x48 voxel tile; each of its 256 consumer threads walks
 //     a 48-voxel z-column and keeps the 48 sums in registers over all views
 //     (the longer the column, the more voxels share the per-view column
-//     terms; 48 sums still fit two CTAs per SM);
+//     terms; 48 sums still fit two CTAs per SM); a remainder of at most 32
+//     slices runs as 32-voxel columns in a second launch;
 //   * one producer warp computes, per view, the detector box covering the
 //     tile's footprint (+1 bilinear tap, +1 pixel margin) and loads it with
 //     cp.async.bulk.tensor (3D tile mode, this GPU's memory only, no
@@ -36,6 +37,7 @@ namespace ykb {
 namespace {
 
 constexpr int TX = 16, TY = 16, ZT = 48;
+constexpr int kZTail = 32;  // column length of a short last z tile
 constexpr int NCONS = TX * TY;          // consumer threads
 constexpr int NCWARPS = NCONS / 32;
 constexpr int NTHREADS = NCONS + 32;    // + producer warp
@@ -249,16 +251,16 @@ struct TileGeom {
     double x0, x1, y0, y1, z0, z1;
 };
 
-__device__ __forceinline__ TileGeom tile_geom(const VolumeGrid& g, int bx, int by, int bz)
+__device__ __forceinline__ TileGeom tile_geom(const VolumeGrid& g, int bx, int by, int bz, int zc)
 {
     TileGeom t;
-    const int xa = bx * TX, ya = by * TY, za = bz * ZT;
+    const int xa = bx * TX, ya = by * TY, za = bz * zc;
     t.x0 = g.ox + xa * g.vx;
     t.x1 = g.ox + min(xa + TX - 1, g.nx - 1) * g.vx;
     t.y0 = g.oy + ya * g.vy;
     t.y1 = g.oy + min(ya + TY - 1, g.ny - 1) * g.vy;
     t.z0 = g.oz + za * g.vz;
-    t.z1 = g.oz + (za + ZT - 1) * g.vz;  // all ZT slices are evaluated
+    t.z1 = g.oz + (za + zc - 1) * g.vz;  // all zc slices are evaluated
     return t;
 }
 
@@ -275,7 +277,7 @@ __global__ void box_extent_kernel(const FdkViewCoef* __restrict__ coef, int n_vi
         const int bx = static_cast<int>(t % tiles_x);
         const int by = static_cast<int>((t / tiles_x) % tiles_y);
         const int bz = static_cast<int>(t / (static_cast<long>(tiles_x) * tiles_y));
-        const TileGeom tg = tile_geom(g, bx, by, bz);
+        const TileGeom tg = tile_geom(g, bx, by, bz, ZT);
         double umin = 1e300, umax = -1e300, vmin = 1e300, vmax = -1e300;
         for (int q = 0; q < 8; ++q) {
             double u, v;
@@ -297,7 +299,7 @@ constexpr size_t kRingBudget = 108 * 1024;
 
 // PSEUDO: the weight of the pseudo-matched backprojection instead of the FDK
 // depth weight (tap pairs only)
-template <int BW, bool AXIAL, bool PAIR, bool PSEUDO>
+template <int BW, bool AXIAL, bool PAIR, bool PSEUDO, int ZC>
 __global__ void __launch_bounds__(NTHREADS, 2) fdk_bp_tma_kernel(const __grid_constant__ CUtensorMap map,
     const FdkViewCoef* __restrict__ coef, int n_views, VolumeGrid g, int BH, int stages,
     float* __restrict__ vol, int accumulate, int* __restrict__ err,
@@ -333,7 +335,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) fdk_bp_tma_kernel(const __grid_co
     }
     __syncthreads();
     if (abort_flag) return;
-    const TileGeom tg = tile_geom(g, blockIdx.x, blockIdx.y, blockIdx.z);
+    const TileGeom tg = tile_geom(g, blockIdx.x, blockIdx.y, blockIdx.z, ZC);
 
     if (warp == NCWARPS) {
         // ------------------------------------------------------ producer ---
@@ -400,12 +402,12 @@ __global__ void __launch_bounds__(NTHREADS, 2) fdk_bp_tma_kernel(const __grid_co
     const int lx = 8 * (warp & 1) + 4 * (lane >> 4) + (lane & 3);
     const int ly = 4 * (warp >> 1) + ((lane >> 2) & 3);
     const int x = blockIdx.x * TX + lx, y = blockIdx.y * TY + ly;
-    const int z0 = blockIdx.z * ZT;
+    const int z0 = blockIdx.z * ZC;
     const bool active = x < g.nx && y < g.ny;
     const double X = g.ox + x * g.vx, Y = g.oy + y * g.vy, Z0 = g.oz + z0 * g.vz;
-    float acc[ZT];
+    float acc[ZC];
 #pragma unroll
-    for (int i = 0; i < ZT; ++i) acc[i] = 0.f;
+    for (int i = 0; i < ZC; ++i) acc[i] = 0.f;
     bool bad = false;
     ColTerms cur{};
     if (AXIAL) cur = axial_terms<PSEUDO>(coef[0], pseudo, X, Y, Z0, g.vz);
@@ -434,13 +436,13 @@ __global__ void __launch_bounds__(NTHREADS, 2) fdk_bp_tma_kernel(const __grid_co
             float alp = cur.alp, bet = cur.bet, gam = cur.gam;
             // rows of the column's end points (the rounding map is monotonic)
             const int na = static_cast<int>(__float_as_uint(vbq + kRoundMagic) - kRoundMagicBits);
-            const int nb = static_cast<int>(__float_as_uint(fmaf(static_cast<float>(ZT - 1), vs, vbq) +
+            const int nb = static_cast<int>(__float_as_uint(fmaf(static_cast<float>(ZC - 1), vs, vbq) +
                 kRoundMagic) - kRoundMagicBits);
             const int lo = min(na, nb), hi = max(na, nb) + 1;
             // |v| < 2^21 along the column keeps the rounding word exact
             const bool finite = fabsf(u) < 1e6f && fabsf(vbq) < 1e6f && fabsf(vs) < 3e4f &&
                 fabsf(w) < 1e30f && (!PSEUDO || (alp > 0.f && alp < 1e30f &&
-                fmaf(static_cast<float>(ZT - 1), fmaf(static_cast<float>(ZT - 1), gam, bet), alp) > 0.f &&
+                fmaf(static_cast<float>(ZC - 1), fmaf(static_cast<float>(ZC - 1), gam, bet), alp) > 0.f &&
                 fabsf(bet) < 1e30f && fabsf(gam) < 1e30f));
             int col = iu - b.x;
             if (!active || !finite || iu < b.x || iu + 1 > b.z || lo < b.y || hi > b.w) {
@@ -463,7 +465,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) fdk_bp_tma_kernel(const __grid_co
                 // L(i) is a square root of a quadratic in i; the FP64 column
                 // terms keep its sqrt argument positive along the column
 #pragma unroll
-                for (int j = 0; j < ZT / 2; ++j) {
+                for (int j = 0; j < ZC / 2; ++j) {
                     const float i0 = 2.f * j, i1 = 2.f * j + 1.f;
                     const f2 vq = f2pack(fmaf(i0, vs, vbq), fmaf(i1, vs, vbq));
                     const f2 t = f2add(vq, M2);
@@ -485,7 +487,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) fdk_bp_tma_kernel(const __grid_co
                 }
             } else if constexpr (PAIR) {
 #pragma unroll
-                for (int j = 0; j < ZT / 2; ++j) {
+                for (int j = 0; j < ZC / 2; ++j) {
                     const f2 vq = f2pack(fmaf(2.f * j, vs, vbq), fmaf(2.f * j + 1.f, vs, vbq));
                     const f2 t = f2add(vq, M2);
                     const f2 fr = f2add(f2sub(vq, f2sub(t, M2)), H2);
@@ -506,7 +508,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) fdk_bp_tma_kernel(const __grid_co
                 }
             } else {
 #pragma unroll
-            for (int j = 0; j < ZT / 2; ++j) {
+            for (int j = 0; j < ZC / 2; ++j) {
                 // rows and vertical weights of z = 2j, 2j+1 in packed pairs;
                 // the taps themselves stay scalar so that no load result has
                 // to be moved into a register pair
@@ -540,9 +542,9 @@ __global__ void __launch_bounds__(NTHREADS, 2) fdk_bp_tma_kernel(const __grid_co
             const float vv = static_cast<float>(vn0), dvn = static_cast<float>(c.cv[2] * g.vz);
             const float dp = static_cast<float>(dp0), ddp = static_cast<float>(c.cr[2] * g.vz);
             // end points: u(z) and v(z) are monotonic along the column
-            const float ra = 1.f / dn, rb = 1.f / fmaf(ZT - 1.f, ddn, dn);
-            const float ua = uu * ra, ub = fmaf(ZT - 1.f, dun, uu) * rb;
-            const float va = vv * ra, vb2 = fmaf(ZT - 1.f, dvn, vv) * rb;
+            const float ra = 1.f / dn, rb = 1.f / fmaf(ZC - 1.f, ddn, dn);
+            const float ua = uu * ra, ub = fmaf(ZC - 1.f, dun, uu) * rb;
+            const float va = vv * ra, vb2 = fmaf(ZC - 1.f, dvn, vv) * rb;
             // u(z), v(z) are monotonic; one row/column of slack covers the
             // rounding of the interior samples
             const int ulo = static_cast<int>(floorf(fminf(ua, ub))) - 1;
@@ -552,8 +554,8 @@ __global__ void __launch_bounds__(NTHREADS, 2) fdk_bp_tma_kernel(const __grid_co
             float scale = s0;
             float gdn = dn, gddn = ddn, guu = uu, gdun = dun, gvv = vv, gdvn = dvn, gdp = dp, gddp = ddp;
             const bool finite = fabsf(ua) < 1e7f && fabsf(ub) < 1e7f && fabsf(va) < 1e7f &&
-                fabsf(vb2) < 1e7f && dn > 0.f && fmaf(ZT - 1.f, ddn, dn) > 0.f &&
-                dp > 0.f && fmaf(ZT - 1.f, ddp, dp) > 0.f;
+                fabsf(vb2) < 1e7f && dn > 0.f && fmaf(ZC - 1.f, ddn, dn) > 0.f &&
+                dp > 0.f && fmaf(ZC - 1.f, ddp, dp) > 0.f;
             if (!active || !finite || ulo < b.x || uhi > b.z || vlo < b.y || vhi > b.w) {
                 if (active) bad = true;
                 scale = 0.f;  // no contribution; reads stay at the stage origin
@@ -562,7 +564,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) fdk_bp_tma_kernel(const __grid_co
             }
             const int cb = -b.x - b.y * BW;
 #pragma unroll
-            for (int i = 0; i < ZT; ++i) {
+            for (int i = 0; i < ZC; ++i) {
                 const float fi = static_cast<float>(i);
                 const float rden = 1.f / fmaf(fi, gddn, gdn);
                 const float u = fmaf(fi, gdun, guu) * rden;
@@ -602,7 +604,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) fdk_bp_tma_kernel(const __grid_co
     const long plane = static_cast<long>(g.nx) * g.ny;
     float* dst = vol + static_cast<long>(y) * g.nx + x;
 #pragma unroll
-    for (int i = 0; i < ZT; ++i) {
+    for (int i = 0; i < ZC; ++i) {
         const int z = z0 + i;
         if (z < g.nz) {
             float* p = dst + z * plane;
@@ -627,12 +629,12 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
 
 constexpr int kWidths[] = {36, 52, 68, 100, 132, 196, 256};
 
-template <typename K>
+template <int ZC, typename K>
 cudaError_t launch_kernel(K k, const CUtensorMap& map, const FdkViewCoef* coef, int n_views,
     const VolumeGrid& g, int BH, int stages, size_t smem, float* vol, int accumulate, int* err,
     const PseudoViewCoef* pseudo, cudaStream_t s)
 {
-    const dim3 grid((g.nx + TX - 1) / TX, (g.ny + TY - 1) / TY, (g.nz + ZT - 1) / ZT);
+    const dim3 grid((g.nx + TX - 1) / TX, (g.ny + TY - 1) / TY, (g.nz + ZC - 1) / ZC);
     const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
         static_cast<int>(smem));
     if (e != cudaSuccess) return e;
@@ -640,43 +642,68 @@ cudaError_t launch_kernel(K k, const CUtensorMap& map, const FdkViewCoef* coef, 
     return cudaGetLastError();
 }
 
-template <int BW, bool PAIR>
+template <int BW, bool PAIR, int ZC>
 cudaError_t launch_bw(const CUtensorMap& map, const FdkViewCoef* coef, int n_views,
     const VolumeGrid& g, int BH, int stages, size_t smem, bool axial, float* vol, int accumulate,
     int* err, const PseudoViewCoef* pseudo, cudaStream_t s)
 {
     if constexpr (PAIR) {
         if (pseudo && axial)
-            return launch_kernel(fdk_bp_tma_kernel<BW, true, true, true>, map, coef, n_views, g,
-                BH, stages, smem, vol, accumulate, err, pseudo, s);
+            return launch_kernel<ZC>(fdk_bp_tma_kernel<BW, true, true, true, ZC>, map, coef,
+                n_views, g, BH, stages, smem, vol, accumulate, err, pseudo, s);
         if (pseudo)
-            return launch_kernel(fdk_bp_tma_kernel<BW, false, true, true>, map, coef, n_views, g,
-                BH, stages, smem, vol, accumulate, err, pseudo, s);
+            return launch_kernel<ZC>(fdk_bp_tma_kernel<BW, false, true, true, ZC>, map, coef,
+                n_views, g, BH, stages, smem, vol, accumulate, err, pseudo, s);
     } else {
         if (pseudo) return cudaErrorInvalidValue;  // pseudo-matched input is staged as pairs
     }
     if (axial)
-        return launch_kernel(fdk_bp_tma_kernel<BW, true, PAIR, false>, map, coef, n_views, g, BH,
-            stages, smem, vol, accumulate, err, pseudo, s);
-    return launch_kernel(fdk_bp_tma_kernel<BW, false, PAIR, false>, map, coef, n_views, g, BH,
-        stages, smem, vol, accumulate, err, pseudo, s);
+        return launch_kernel<ZC>(fdk_bp_tma_kernel<BW, true, PAIR, false, ZC>, map, coef, n_views,
+            g, BH, stages, smem, vol, accumulate, err, pseudo, s);
+    return launch_kernel<ZC>(fdk_bp_tma_kernel<BW, false, PAIR, false, ZC>, map, coef, n_views,
+        g, BH, stages, smem, vol, accumulate, err, pseudo, s);
 }
 
+template <bool PAIR, int ZC>
+cudaError_t launch_width(const CUtensorMap& map, const FdkViewCoef* coef, int n_views,
+    const VolumeGrid& g, int bw, int bh, int stages, size_t smem, bool axial, float* vol,
+    int accumulate, int* err, const PseudoViewCoef* pseudo, cudaStream_t s)
+{
+    switch (bw) {
+    case 36: return launch_bw<36, PAIR, ZC>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, s);
+    case 52: return launch_bw<52, PAIR, ZC>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, s);
+    case 68: return launch_bw<68, PAIR, ZC>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, s);
+    case 100: return launch_bw<100, PAIR, ZC>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, s);
+    case 132: return launch_bw<132, PAIR, ZC>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, s);
+    case 196: return launch_bw<196, PAIR, ZC>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, s);
+    case 256: return launch_bw<256, PAIR, ZC>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, s);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+// The volume runs in ZT-slice columns.  A remainder of at most kZTail slices
+// runs as kZTail-slice columns in a second launch instead of a ZT-slice
+// tile that is mostly outside the volume; its tiles lie inside the ZT-slice
+// tiles of the box pre-pass, so their footprints fit the same box.
 template <bool PAIR>
 cudaError_t launch_layout(const CUtensorMap& map, const FdkViewCoef* coef, int n_views,
     const VolumeGrid& g, int bw, int bh, int stages, size_t smem, bool axial, float* vol,
     int accumulate, int* err, const PseudoViewCoef* pseudo, cudaStream_t s)
 {
-    switch (bw) {
-    case 36: return launch_bw<36, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, s);
-    case 52: return launch_bw<52, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, s);
-    case 68: return launch_bw<68, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, s);
-    case 100: return launch_bw<100, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, s);
-    case 132: return launch_bw<132, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, s);
-    case 196: return launch_bw<196, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, s);
-    case 256: return launch_bw<256, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, s);
-    default: return cudaErrorInvalidValue;
+    const int rem = g.nz % ZT;
+    const int main_nz = rem > 0 && rem <= kZTail ? g.nz - rem : g.nz;
+    if (main_nz > 0) {
+        VolumeGrid gm = g;
+        gm.nz = main_nz;
+        const cudaError_t e = launch_width<PAIR, ZT>(map, coef, n_views, gm, bw, bh, stages, smem,
+            axial, vol, accumulate, err, pseudo, s);
+        if (e != cudaSuccess || main_nz == g.nz) return e;
     }
+    VolumeGrid gt = g;
+    gt.nz = g.nz - main_nz;
+    gt.oz = g.oz + main_nz * g.vz;
+    return launch_width<PAIR, kZTail>(map, coef, n_views, gt, bw, bh, stages, smem, axial,
+        vol + static_cast<size_t>(main_nz) * g.nx * g.ny, accumulate, err, pseudo, s);
 }
 
 } // namespace
