@@ -79,12 +79,6 @@ def chunk_views() -> int:
     return max(1, min(N_VIEWS, (8 << 30) // (12 * N_DET * N_DET)))
 
 
-def bp_launches(nz: int) -> int:
-    """Launches of one FDK backprojection: 48-slice voxel columns, plus one
-    launch of 32-slice columns for a remainder of 1 to 32 slices."""
-    return 2 if 0 < nz % 48 <= 32 else 1
-
-
 def object_seed(rank: int) -> int:
     """Seed of rank's phantom: each rank reconstructs its own object (weak
     scaling, no data exchanged between ranks)."""
@@ -571,7 +565,7 @@ def main():
         "fp32_form": fp32_form,
         "joseph": joseph,
         # preweight, filter and backprojection per workspace chunk
-        "gpu_launches": (2 + bp_launches(N_VOX)) * -(-N_VIEWS // chunk_views()) * args.steps,
+        "gpu_launches": 3 * -(-N_VIEWS // chunk_views()) * args.steps,
         "clocks": clock_info,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

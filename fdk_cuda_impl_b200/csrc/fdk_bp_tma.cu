@@ -7,7 +7,7 @@
 //     a 48-voxel z-column and keeps the 48 sums in registers over all views
 //     (the longer the column, the more voxels share the per-view column
 //     terms; 48 sums still fit two CTAs per SM); a remainder of at most 32
-//     slices runs as 32-voxel columns in a second launch;
+//     slices runs as 32-voxel columns, the same launch's last z layer;
 //   * one producer warp computes, per view, the detector box covering the
 //     tile's footprint (+1 bilinear tap, +1 pixel margin) and loads it with
 //     cp.async.bulk.tensor (3D tile mode, this GPU's memory only, no
@@ -251,10 +251,10 @@ struct TileGeom {
     double x0, x1, y0, y1, z0, z1;
 };
 
-__device__ __forceinline__ TileGeom tile_geom(const VolumeGrid& g, int bx, int by, int bz, int zc)
+__device__ __forceinline__ TileGeom tile_geom(const VolumeGrid& g, int bx, int by, int za, int zc)
 {
     TileGeom t;
-    const int xa = bx * TX, ya = by * TY, za = bz * zc;
+    const int xa = bx * TX, ya = by * TY;
     t.x0 = g.ox + xa * g.vx;
     t.x1 = g.ox + min(xa + TX - 1, g.nx - 1) * g.vx;
     t.y0 = g.oy + ya * g.vy;
@@ -277,7 +277,7 @@ __global__ void box_extent_kernel(const FdkViewCoef* __restrict__ coef, int n_vi
         const int bx = static_cast<int>(t % tiles_x);
         const int by = static_cast<int>((t / tiles_x) % tiles_y);
         const int bz = static_cast<int>(t / (static_cast<long>(tiles_x) * tiles_y));
-        const TileGeom tg = tile_geom(g, bx, by, bz, ZT);
+        const TileGeom tg = tile_geom(g, bx, by, bz * ZT, ZT);
         double umin = 1e300, umax = -1e300, vmin = 1e300, vmax = -1e300;
         for (int q = 0; q < 8; ++q) {
             double u, v;
@@ -300,10 +300,10 @@ constexpr size_t kRingBudget = 108 * 1024;
 // PSEUDO: the weight of the pseudo-matched backprojection instead of the FDK
 // depth weight (tap pairs only)
 template <int BW, bool AXIAL, bool PAIR, bool PSEUDO, int ZC>
-__global__ void __launch_bounds__(NTHREADS, 2) fdk_bp_tma_kernel(const __grid_constant__ CUtensorMap map,
-    const FdkViewCoef* __restrict__ coef, int n_views, VolumeGrid g, int BH, int stages,
+__device__ __forceinline__ void bp_tile(const CUtensorMap& map,
+    const FdkViewCoef* __restrict__ coef, int n_views, const VolumeGrid& g, int BH, int stages,
     float* __restrict__ vol, int accumulate, int* __restrict__ err,
-    const PseudoViewCoef* __restrict__ pseudo)
+    const PseudoViewCoef* __restrict__ pseudo, int za)
 {
     extern __shared__ unsigned char smem_raw[];
     // 128-byte aligned base (the launch requests 128 bytes of slack)
@@ -335,7 +335,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) fdk_bp_tma_kernel(const __grid_co
     }
     __syncthreads();
     if (abort_flag) return;
-    const TileGeom tg = tile_geom(g, blockIdx.x, blockIdx.y, blockIdx.z, ZC);
+    const TileGeom tg = tile_geom(g, blockIdx.x, blockIdx.y, za, ZC);
 
     if (warp == NCWARPS) {
         // ------------------------------------------------------ producer ---
@@ -402,7 +402,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) fdk_bp_tma_kernel(const __grid_co
     const int lx = 8 * (warp & 1) + 4 * (lane >> 4) + (lane & 3);
     const int ly = 4 * (warp >> 1) + ((lane >> 2) & 3);
     const int x = blockIdx.x * TX + lx, y = blockIdx.y * TY + ly;
-    const int z0 = blockIdx.z * ZC;
+    const int z0 = za;
     const bool active = x < g.nx && y < g.ny;
     const double X = g.ox + x * g.vx, Y = g.oy + y * g.vy, Z0 = g.oz + z0 * g.vz;
     float acc[ZC];
@@ -613,6 +613,24 @@ __global__ void __launch_bounds__(NTHREADS, 2) fdk_bp_tma_kernel(const __grid_co
     }
 }
 
+// blockIdx.z < main_tiles: ZT-slice tiles from slice 0; above: kZTail-slice
+// tiles after them (a short last part of the volume).  The short tiles are
+// the grid's last blocks, so they fill the final wave of the long ones.
+template <int BW, bool AXIAL, bool PAIR, bool PSEUDO>
+__global__ void __launch_bounds__(NTHREADS, 2) fdk_bp_tma_kernel(const __grid_constant__ CUtensorMap map,
+    const FdkViewCoef* __restrict__ coef, int n_views, VolumeGrid g, int BH, int stages,
+    float* __restrict__ vol, int accumulate, int* __restrict__ err,
+    const PseudoViewCoef* __restrict__ pseudo, int main_tiles)
+{
+    const int bz = static_cast<int>(blockIdx.z);
+    if (bz < main_tiles)
+        bp_tile<BW, AXIAL, PAIR, PSEUDO, ZT>(map, coef, n_views, g, BH, stages, vol, accumulate,
+            err, pseudo, bz * ZT);
+    else
+        bp_tile<BW, AXIAL, PAIR, PSEUDO, kZTail>(map, coef, n_views, g, BH, stages, vol,
+            accumulate, err, pseudo, main_tiles * ZT + (bz - main_tiles) * kZTail);
+}
+
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
 {
     static std::once_flag once;
@@ -629,81 +647,64 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
 
 constexpr int kWidths[] = {36, 52, 68, 100, 132, 196, 256};
 
-template <int ZC, typename K>
+// z tiling: ZT-slice tiles, except that a remainder of at most kZTail
+// slices becomes one kZTail-slice tile instead of a ZT-slice tile that is
+// mostly outside the volume.  The short tile lies inside the ZT-slice tile
+// of the box pre-pass, so its footprints fit the same box.
+template <typename K>
 cudaError_t launch_kernel(K k, const CUtensorMap& map, const FdkViewCoef* coef, int n_views,
     const VolumeGrid& g, int BH, int stages, size_t smem, float* vol, int accumulate, int* err,
     const PseudoViewCoef* pseudo, cudaStream_t s)
 {
-    const dim3 grid((g.nx + TX - 1) / TX, (g.ny + TY - 1) / TY, (g.nz + ZC - 1) / ZC);
+    const int rem = g.nz % ZT;
+    const bool tail = rem > 0 && rem <= kZTail;
+    const int main_tiles = tail ? g.nz / ZT : (g.nz + ZT - 1) / ZT;
+    const dim3 grid((g.nx + TX - 1) / TX, (g.ny + TY - 1) / TY, main_tiles + (tail ? 1 : 0));
     const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
         static_cast<int>(smem));
     if (e != cudaSuccess) return e;
-    k<<<grid, NTHREADS, smem, s>>>(map, coef, n_views, g, BH, stages, vol, accumulate, err, pseudo);
+    k<<<grid, NTHREADS, smem, s>>>(map, coef, n_views, g, BH, stages, vol, accumulate, err, pseudo,
+        main_tiles);
     return cudaGetLastError();
 }
 
-template <int BW, bool PAIR, int ZC>
+template <int BW, bool PAIR>
 cudaError_t launch_bw(const CUtensorMap& map, const FdkViewCoef* coef, int n_views,
     const VolumeGrid& g, int BH, int stages, size_t smem, bool axial, float* vol, int accumulate,
     int* err, const PseudoViewCoef* pseudo, cudaStream_t s)
 {
     if constexpr (PAIR) {
         if (pseudo && axial)
-            return launch_kernel<ZC>(fdk_bp_tma_kernel<BW, true, true, true, ZC>, map, coef,
-                n_views, g, BH, stages, smem, vol, accumulate, err, pseudo, s);
+            return launch_kernel(fdk_bp_tma_kernel<BW, true, true, true>, map, coef, n_views, g,
+                BH, stages, smem, vol, accumulate, err, pseudo, s);
         if (pseudo)
-            return launch_kernel<ZC>(fdk_bp_tma_kernel<BW, false, true, true, ZC>, map, coef,
-                n_views, g, BH, stages, smem, vol, accumulate, err, pseudo, s);
+            return launch_kernel(fdk_bp_tma_kernel<BW, false, true, true>, map, coef, n_views, g,
+                BH, stages, smem, vol, accumulate, err, pseudo, s);
     } else {
         if (pseudo) return cudaErrorInvalidValue;  // pseudo-matched input is staged as pairs
     }
     if (axial)
-        return launch_kernel<ZC>(fdk_bp_tma_kernel<BW, true, PAIR, false, ZC>, map, coef, n_views,
-            g, BH, stages, smem, vol, accumulate, err, pseudo, s);
-    return launch_kernel<ZC>(fdk_bp_tma_kernel<BW, false, PAIR, false, ZC>, map, coef, n_views,
-        g, BH, stages, smem, vol, accumulate, err, pseudo, s);
+        return launch_kernel(fdk_bp_tma_kernel<BW, true, PAIR, false>, map, coef, n_views, g, BH,
+            stages, smem, vol, accumulate, err, pseudo, s);
+    return launch_kernel(fdk_bp_tma_kernel<BW, false, PAIR, false>, map, coef, n_views, g, BH,
+        stages, smem, vol, accumulate, err, pseudo, s);
 }
 
-template <bool PAIR, int ZC>
-cudaError_t launch_width(const CUtensorMap& map, const FdkViewCoef* coef, int n_views,
-    const VolumeGrid& g, int bw, int bh, int stages, size_t smem, bool axial, float* vol,
-    int accumulate, int* err, const PseudoViewCoef* pseudo, cudaStream_t s)
-{
-    switch (bw) {
-    case 36: return launch_bw<36, PAIR, ZC>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, s);
-    case 52: return launch_bw<52, PAIR, ZC>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, s);
-    case 68: return launch_bw<68, PAIR, ZC>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, s);
-    case 100: return launch_bw<100, PAIR, ZC>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, s);
-    case 132: return launch_bw<132, PAIR, ZC>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, s);
-    case 196: return launch_bw<196, PAIR, ZC>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, s);
-    case 256: return launch_bw<256, PAIR, ZC>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, s);
-    default: return cudaErrorInvalidValue;
-    }
-}
-
-// The volume runs in ZT-slice columns.  A remainder of at most kZTail slices
-// runs as kZTail-slice columns in a second launch instead of a ZT-slice
-// tile that is mostly outside the volume; its tiles lie inside the ZT-slice
-// tiles of the box pre-pass, so their footprints fit the same box.
 template <bool PAIR>
 cudaError_t launch_layout(const CUtensorMap& map, const FdkViewCoef* coef, int n_views,
     const VolumeGrid& g, int bw, int bh, int stages, size_t smem, bool axial, float* vol,
     int accumulate, int* err, const PseudoViewCoef* pseudo, cudaStream_t s)
 {
-    const int rem = g.nz % ZT;
-    const int main_nz = rem > 0 && rem <= kZTail ? g.nz - rem : g.nz;
-    if (main_nz > 0) {
-        VolumeGrid gm = g;
-        gm.nz = main_nz;
-        const cudaError_t e = launch_width<PAIR, ZT>(map, coef, n_views, gm, bw, bh, stages, smem,
-            axial, vol, accumulate, err, pseudo, s);
-        if (e != cudaSuccess || main_nz == g.nz) return e;
+    switch (bw) {
+    case 36: return launch_bw<36, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, s);
+    case 52: return launch_bw<52, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, s);
+    case 68: return launch_bw<68, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, s);
+    case 100: return launch_bw<100, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, s);
+    case 132: return launch_bw<132, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, s);
+    case 196: return launch_bw<196, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, s);
+    case 256: return launch_bw<256, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, s);
+    default: return cudaErrorInvalidValue;
     }
-    VolumeGrid gt = g;
-    gt.nz = g.nz - main_nz;
-    gt.oz = g.oz + main_nz * g.vz;
-    return launch_width<PAIR, kZTail>(map, coef, n_views, gt, bw, bh, stages, smem, axial,
-        vol + static_cast<size_t>(main_nz) * g.nx * g.ny, accumulate, err, pseudo, s);
 }
 
 } // namespace
