@@ -17,9 +17,8 @@
 //   * filtered rows arrive either as plain floats or as tap pairs, element
 //     (v, kPairLead + u) = (f[v][u], f[v][u+1]), zero outside the detector
 //     (written so by the filter epilogues).  With pairs one 8-byte shared
-//     load returns both
-//     horizontal taps of a detector row, and the vertical lerp runs as one
-//     packed f32x2 operation on the (left, right) pair;
+//     load returns both horizontal taps of a detector row, and the vertical
+//     lerp runs as one packed f32x2 operation on the (left, right) pair;
 //   * consumers read the four taps from shared memory without bounds checks:
 //     the box is sized by a pre-pass over all (tile, view) pairs with the same
 //     footprint function, and each (column, view) checks its end points.
