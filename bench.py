@@ -11,13 +11,21 @@ value   = voxel x view updates per second of the whole job (all ranks), with
 e2e     = the same metric through the C-ABI with host buffers: each step
           copies the projections host->device (pinned) and the volume
           device->host inside the timed region.
+rel_rmse_vs_oracle = the FP32 volume against the FP64 oracle on a 16-slice
+          slab over all views (the oracle's run is also the CPU baseline).
 Inputs (1.7 GB projections, 0.54 GB volume) exceed the 126 MB L2, so no
 flush is needed between steps.
 
+Beside the headline: the BF16 form (BF16-stored projections, Shepp-Logan
+window, tensor-core BF16 filter) on the same views; the 1024^3 x 1440 x 1536^2
+workload with BF16-stored projections ("large", one GPU only); the
+differentiable Joseph pair at 256^3 x 360 x 384^2 ("joseph").
+
 --impl reference times the reference's own implementation on the same
 workload: its CUDA build (the reference has no CPU path), compiled for sm_100a
-from its sources into oracle/_ref, through its stock FDK pipeline; the FP64
-CPU oracle on a bounded sample when that build is absent.
+from its sources into oracle/_ref, through its stock FDK pipeline, with inputs
+from its own Joseph projector (no part of this package's library runs in that
+arm); the FP64 CPU oracle on a bounded sample when that build is absent.
 """
 from __future__ import annotations
 
@@ -34,49 +42,16 @@ sys.path.insert(0, ROOT)
 
 # the headline metric: FDK GUPS is `value`; the FP+BP gradient step of the
 # differentiable Joseph pair is reported beside it ("joseph")
-METRIC = "FDK backprojection GUPS (voxel\u00d7view/s) & FP+BP grad step ms at stated RMSE"
+METRIC = "FDK backprojection GUPS (voxel×view/s) & FP+BP grad step ms at stated RMSE"
 
-# the workload the metric is quoted on, and a small case of the same kernels
-# (inputs still larger than L2) used for profiler captures
-# "large": the 1024^3 x 1440-view x 1536^2 FDK with BF16-stored projections
-# (6.8 GB), tensor-core BF16 filter and FP32 backprojection; its phantom adds
-# 200 small high-contrast spheres and it is noise-free
-CONFIGS = {
-    "c2": dict(N_VOX=512, N_VIEWS=720, N_DET=768, VOX_MM=0.25, PIX_MM=0.4, N_ELL=20, N_SPH=0,
-               I0=1e5, PRECISION="fp32"),
-    "small": dict(N_VOX=256, N_VIEWS=360, N_DET=384, VOX_MM=0.5, PIX_MM=0.8, N_ELL=20, N_SPH=0,
-                  I0=1e5, PRECISION="fp32"),
-    "large": dict(N_VOX=1024, N_VIEWS=1440, N_DET=1536, VOX_MM=0.125, PIX_MM=0.2, N_ELL=40,
-                  N_SPH=200, I0=None, PRECISION="bf16"),
-}
-N_VOX = 512
-N_VIEWS = 720
-N_DET = 768
-VOX_MM = 0.25
-PIX_MM = 0.4
-SID, SDD = 500.0, 1000.0
-N_ELL = 20
-N_SPH = 0
-I0 = 1e5
-PRECISION = "fp32"
-UPDATES = N_VOX ** 3 * N_VIEWS
-WORKLOAD = "fdk-512^3-720v-768^2"
-
-
-def select_config(name: str) -> None:
-    global N_VOX, N_VIEWS, N_DET, VOX_MM, PIX_MM, N_ELL, N_SPH, I0, PRECISION, UPDATES, WORKLOAD
-    c = CONFIGS[name]
-    N_VOX, N_VIEWS, N_DET, VOX_MM, PIX_MM = (c["N_VOX"], c["N_VIEWS"], c["N_DET"], c["VOX_MM"],
-                                             c["PIX_MM"])
-    N_ELL, N_SPH, I0, PRECISION = c["N_ELL"], c["N_SPH"], c["I0"], c["PRECISION"]
-    UPDATES = N_VOX ** 3 * N_VIEWS
-    WORKLOAD = f"fdk-{N_VOX}^3-{N_VIEWS}v-{N_DET}^2" + ("-bf16" if PRECISION == "bf16" else "")
-
-
-def chunk_views() -> int:
-    """Views per workspace chunk of an FDK plan: a budget of 8 GiB at 12 bytes
-    per detector pixel (preweighted rows + filtered tap pairs)."""
-    return max(1, min(N_VIEWS, (8 << 30) // (12 * N_DET * N_DET)))
+# z slab [z0, z0 + nz) of each workload that the FP64 oracle reconstructs:
+# off-centre for the 512^3 workload (its rays cross about 70 detector rows),
+# the centre for the 1024^3 one (a few rows: the oracle's direct-convolution
+# filter is the cost)
+PARITY_SLABS = {"c2": (384, 16), "small": (192, 16), "det768": (192, 16), "large": (510, 4)}
+FILTERS = {"f32": "ramlak", "bf16": "shepplogan"}
+# timed steps of the 1024^3 workload (1.3 s each) within the default run
+LARGE_STEPS, LARGE_WARMUP = 3, 3
 
 
 def object_seed(rank: int) -> int:
@@ -103,6 +78,15 @@ def job_gups(world: int, updates: int, ms: float) -> float:
     return world * updates / (ms * 1e-3) / 1e9
 
 
+def bench_config(w, world: int) -> dict:
+    """The workload description both arms report (one dict, same keys and
+    values, so the two lines are comparable)."""
+    return dict(w.describe(), filter=FILTERS[w.projections], host_memory="pinned",
+                l2=f"inputs larger than L2 ({w.n_views * w.n_det ** 2 * (2 if w.projections == 'bf16' else 4) / 1e9:.1f} GB "
+                   f"projections, {4 * w.n_vox ** 3 / 1e9:.2f} GB volume)",
+                parallelism=f"independent objects x{world}")
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -112,7 +96,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-bf16", action="store_true")
     ap.add_argument("--no-joseph", action="store_true")
-    ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
+    ap.add_argument("--no-large", action="store_true")
+    ap.add_argument("--config", default="c2", choices=["c2", "small", "det768", "large"])
     return ap.parse_args()
 
 
@@ -183,36 +168,64 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
 
 
-def cpu_baseline(n_views_sample=96, z_slab=64):
-    """FP64 oracle FDK on a bounded sample of the same workload: a subset of
-    views (full 768x768 projections: preweight + filter) backprojected into
-    a z-slab of the volume.  Returns GUPS on the host cores."""
+def rel_rmse(a, ref) -> float:
+    import numpy as np
+    a = np.asarray(a, dtype=np.float64)
+    ref = np.asarray(ref, dtype=np.float64)
+    return float(np.sqrt(np.mean((a - ref) ** 2)) / max(np.sqrt(np.mean(ref ** 2)), 1e-300))
+
+
+# ----------------------------------------------------------- CPU baseline ---
+def cpu_baseline_leg(w, views, scan_range, forms):
+    """The FP64 CPU oracle (a restatement of the reference FDK) on a bounded
+    sample of workload w, timed on the host cores: all views, preweighted and
+    filtered on the detector rows that the parity slab reads, backprojected
+    into that slab.  The same oracle volumes check the GPU results.
+
+    forms: {name: (host projections [views][rows][cols] tensor or array,
+    filter name, GPU slab or None)}.  Returns (cpu_baseline of the first
+    form, {name: rel RMSE of its GPU slab against the oracle})."""
     import numpy as np
     from oracle import oracle as O
-    views_all = O.build_circular_flat(N_VIEWS, N_VIEWS, SID, SDD, N_DET, N_DET, PIX_MM, PIX_MM)
-    step = N_VIEWS // n_views_sample
-    views = np.ascontiguousarray(views_all[::step][:n_views_sample])
-    rng = O.regular_scan_range(N_VIEWS, N_VIEWS)
-    proj = O.uniform((n_views_sample, N_DET, N_DET), 0.0, 1.0, 17)
-    vol = O.volume_struct((z_slab, N_VOX, N_VOX), VOX_MM)
-    filt = O.filter_struct(1)
-    t0 = time.perf_counter()
-    O.fdk(views, N_DET, N_DET, rng, vol, filt, proj)
-    dt = time.perf_counter() - t0
-    updates = n_views_sample * z_slab * N_VOX * N_VOX
-    return {"value": updates / dt / 1e9, "unit": "GUPS", "cores": O.num_threads(), "kind": "port",
-            "sample": f"{n_views_sample} of {N_VIEWS} views (full {N_DET}x{N_DET} preweight+ramp "
-                      f"filter) backprojected into a {N_VOX}x{N_VOX}x{z_slab} slab, FP64, {dt:.1f} s"}
+    from fdk_cuda_impl_b200.geometry import RampFilter
+    from fdk_cuda_impl_b200.workloads import slab
+    z0, nz = PARITY_SLABS[w.name]
+    g = slab(w, z0, nz)
+    vol = O.volume_struct(g.shape, g.voxel_mm, g.center_mm)
+    r0, nr = O.fdk_row_band(views, w.n_det, w.n_det, scan_range, vol)
+    baseline, errors = None, {}
+    for name, (host_proj, filt, gpu_slab) in forms.items():
+        rows = host_proj[:, r0:r0 + nr, :]
+        rows = np.ascontiguousarray(rows.float().numpy() if hasattr(rows, "float") else rows,
+                                    dtype=np.float32)
+        f = RampFilter.named(filt)
+        of = O.filter_struct(f.type, f.cutoff, f.gain, f.butterworth_order, f.kaiser_beta,
+                             f.tukey_alpha)
+        t0 = time.perf_counter()
+        ref = O.fdk_rows(views, w.n_det, w.n_det, scan_range, vol, of, rows, r0)
+        dt = time.perf_counter() - t0
+        if baseline is None:
+            updates = w.n_views * nz * w.n_vox * w.n_vox
+            baseline = {"value": updates / dt / 1e9, "unit": "GUPS", "cores": O.num_threads(),
+                        "kind": "port",
+                        "sample": f"all {w.n_views} views (preweight + {filt} filter of the "
+                                  f"{nr} detector rows the slab reads) backprojected into slices "
+                                  f"{z0}..{z0 + nz - 1} ({w.n_vox}x{w.n_vox}x{nz}), FP64, "
+                                  f"{dt:.1f} s"}
+        if gpu_slab is not None:
+            errors[name] = rel_rmse(gpu_slab, ref)
+    return baseline, errors
 
 
+# ------------------------------------------------------------ Joseph pair ---
 # Differentiable Joseph pair (the metric's "FP+BP grad step"): 256^3 of
 # 0.5 mm voxels, 360 views of a 384x384 detector of 0.8 mm at 500/1000 mm
 J_VOX, J_VIEWS, J_DET, J_VOX_MM, J_PIX_MM = 256, 360, 384, 0.5, 0.8
 
 
 def joseph_workload():
-    from fdk_cuda_impl_b200 import CircularScan, VolumeGrid
-    scan = CircularScan(J_VIEWS, J_VIEWS, SID, SDD, J_DET, J_DET, J_PIX_MM, J_PIX_MM)
+    from fdk_cuda_impl_b200.geometry import CircularScan, VolumeGrid
+    scan = CircularScan(J_VIEWS, J_VIEWS, 500.0, 1000.0, J_DET, J_DET, J_PIX_MM, J_PIX_MM)
     return scan, VolumeGrid.cube(J_VOX, J_VOX_MM)
 
 
@@ -266,137 +279,210 @@ def joseph_step(local: int, steps: int, warmup: int, timed_fn):
             "siddon_fp_ms": siddon_fp_ms, "siddon_bp_ms": siddon_bp_ms}
 
 
-def make_workload(rank: int, local: int):
-    """The benchmark's seeded inputs on cuda:local: ellipsoid phantom (one
-    independent object per rank), Joseph forward projection, Poisson noise."""
-    import torch
-    from fdk_cuda_impl_b200 import CircularScan, VolumeGrid
-    from fdk_cuda_impl_b200 import phantom as PH
-    from fdk_cuda_impl_b200.projectors import JosephPlan
-    import numpy as np
-    scan = CircularScan(N_VIEWS, N_VIEWS, SID, SDD, N_DET, N_DET, PIX_MM, PIX_MM)
-    grid = VolumeGrid.cube(N_VOX, VOX_MM)
-    views = scan.views()
-    seed = object_seed(rank)
-    ell = PH.random_ellipsoids(seed, N_ELL)
-    if N_SPH:
-        ell = np.concatenate([ell, PH.random_spheres(seed, N_SPH)])
-    phantom = PH.voxelize(grid, ell, device=f"cuda:{local}")
-    dtype = torch.bfloat16 if PRECISION == "bf16" else torch.float32
-    proj = torch.empty((N_VIEWS, N_DET, N_DET), dtype=dtype, device=f"cuda:{local}")
-    # Joseph projection in view chunks (its plan holds a 20-byte ray record
-    # per detector pixel of its views)
-    step = max(1, min(N_VIEWS, (4 << 30) // (20 * N_DET * N_DET)))
-    for v0 in range(0, N_VIEWS, step):
-        jp = JosephPlan(views[v0:v0 + step], N_DET, N_DET, grid, device=local)
-        part = jp.forward(phantom)
-        if I0 is not None and dtype != torch.float32:
-            PH.poisson_noise_(part, I0, seed=7 + rank + v0)
-        proj[v0:v0 + step] = part
-        jp.close()
-        del jp, part
-    del phantom
-    if I0 is not None and dtype == torch.float32:
-        PH.poisson_noise_(proj, I0, seed=7 + rank)
-    torch.cuda.synchronize()
-    torch.cuda.empty_cache()
-    return scan, grid, views, proj
-
-
+# -------------------------------------------------------- reference arm ---
 def run_reference(args):
     """The reference's own implementation of the path on the same workload.
 
     The reference has no CPU path (its FDK and Joseph operators are CUDA
     only), so its own implementation is its CUDA build: oracle/_ref/libykref.so,
     compiled for sm_100a from the reference sources by oracle/ref_build.py,
-    driven through its stock FdkPipeline (the path its Session runs).  value =
-    projections already on the device (chunked device-to-device uploads inside
-    the pipeline), e2e = host projections and the volume read back, as its
-    Session requires.  Without that build, the FP64 CPU oracle port is timed on
-    a bounded sample instead.  Under torchrun only rank 0 runs."""
+    driven through its stock FdkPipeline (the path its Session runs).  Its
+    inputs come from the same seeded phantom projected by its own FP_Joseph;
+    views for the oracle come from the oracle's builder (bit-identical to the
+    reference builders).  Nothing of this package's library runs here.
+    value = projections already on the device (chunked device-to-device
+    uploads inside the pipeline), e2e = pinned host projections in and the
+    volume read back to pinned host memory, as its Session's host path does.
+    Without that build, the FP64 CPU oracle port is timed on a bounded sample
+    instead.  Under torchrun only rank 0 runs."""
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
     import numpy as np
-    from oracle import ref as R
-    cfg = {"workload": WORKLOAD, "volume": [N_VOX] * 3, "voxel_mm": VOX_MM, "views": N_VIEWS,
-           "detector": [N_DET, N_DET], "pixel_mm": PIX_MM, "sid_sdd_mm": [SID, SDD],
-           "ellipsoids": N_ELL, "noise_i0": I0, "filter": "ramlak"}
-    line = {"metric": METRIC, "unit": "GUPS",
-            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "data": "synthetic", "impl": "reference"}
     import torch
-    if R.available() and torch.cuda.is_available():
-        from fdk_cuda_impl_b200 import RampFilter
-        scan, grid, _, proj = make_workload(0, 0)
-        h_proj = proj.float().cpu().numpy()  # the reference takes FP32 projections
+    from oracle import oracle as O
+    from oracle import ref as R
+    from fdk_cuda_impl_b200.geometry import RampFilter
+    from fdk_cuda_impl_b200.workloads import WORKLOADS, make_projections
+    w = WORKLOADS[args.config]
+    line = {"metric": METRIC, "unit": "GUPS", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "data": "synthetic", "impl": "reference",
+            "config": bench_config(w, world)}
+    if not (R.available() and torch.cuda.is_available()):
+        scan = w.scan()
+        views = O.build_circular_flat(w.n_views, w.n_views, scan.sid_mm, scan.sdd_mm, w.n_det,
+                                      w.n_det, w.pix_mm, w.pix_mm)
+        host = O.uniform((w.n_views, w.n_det, w.n_det), 0.0, 1.0, 17)
+        cb, _ = cpu_baseline_leg(w, views, O.regular_scan_range(w.n_views, w.n_views),
+                                 {"f32": (host, FILTERS[w.projections], None)})
+        line.update({"value": cb["value"], "ms_per_step": w.updates / (cb["value"] * 1e9) * 1e3,
+                     "dtype": "f64", "cpu_baseline": cb,
+                     "implementation": "FP64 CPU oracle port (no reference build present)",
+                     "e2e": {"value": cb["value"], "unit": "GUPS", "h2d_bytes_per_step": 0,
+                             "d2h_bytes_per_step": 0}})
+        print(json.dumps(line), flush=True)
+        return
+
+    def reference_fdk(w, seed, warmup, steps):
+        scan, grid = w.scan(), w.grid()
+        views = O.build_circular_flat(w.n_views, w.n_views, scan.sid_mm, scan.sdd_mm, w.n_det,
+                                      w.n_det, w.pix_mm, w.pix_mm)
+        scan_range = O.regular_scan_range(w.n_views, w.n_views)
+
+        def ref_forward(_views, phantom):
+            out, _ = R.joseph_fp(scan, grid, phantom.cpu().numpy())
+            return torch.from_numpy(out).cuda()
+
+        _, proj = make_projections(w, seed, 0, forward=ref_forward, views=views,
+                                   chunk_views=w.n_views)
+        # the reference takes FP32 projections (BF16-stored ones widen exactly)
+        h_proj = proj.float().cpu().numpy()
         del proj
         torch.cuda.empty_cache()
-        ms_dev, ms_host = R.fdk_time(scan, grid, RampFilter(), h_proj, warmup=args.warmup,
-                                     reps=args.steps, timeout=1800)
-        value = UPDATES / (ms_dev * 1e-3) / 1e9
-        cb = cpu_baseline(n_views_sample=24, z_slab=32)
-        # the reference's FP_Joseph / BP_Joseph operators on the same Joseph
-        # workload (each call re-uploads its texture, as its stock apply does)
-        jscan, jgrid = joseph_workload()
-        gen = np.random.default_rng(11)
-        jx = gen.random(jgrid.shape, dtype=np.float32)
-        jy = gen.standard_normal((J_VIEWS, J_DET, J_DET)).astype(np.float32)
-        _, fp_ms = R.joseph_fp(jscan, jgrid, jx, warmup=args.warmup, reps=args.steps)
-        _, bp_ms = R.joseph_bp(jscan, jgrid, jy, warmup=args.warmup, reps=args.steps)
-        _, pseudo_ms = R.bp_pseudo(jscan, jgrid, jy, warmup=args.warmup, reps=args.steps)
-        _, siddon_fp_ms = R.siddon_fp(jscan, jgrid, jx, warmup=args.warmup, reps=args.steps)
-        _, siddon_bp_ms = R.siddon_bp(jscan, jgrid, jy, warmup=args.warmup, reps=args.steps)
-        samples = J_VIEWS * J_DET * J_DET * J_VOX
-        joseph = {"workload": f"joseph-{J_VOX}^3-{J_VIEWS}v-{J_DET}^2", "fp_ms": fp_ms,
-                  "bp_ms": bp_ms, "grad_step_ms": fp_ms + bp_ms,
-                  "fp_gsamples": samples / (fp_ms * 1e-3) / 1e9,
-                  "bp_gsamples": samples / (bp_ms * 1e-3) / 1e9,
-                  "bp_pseudo_matched_ms": pseudo_ms,
-                  "bp_pseudo_matched_gups": J_VOX ** 3 * J_VIEWS / (pseudo_ms * 1e-3) / 1e9,
-                  "siddon_fp_ms": siddon_fp_ms, "siddon_bp_ms": siddon_bp_ms}
-        line.update({
-            "value": value, "ms_per_step": ms_dev, "dtype": "f32",
-            "config": dict(cfg, implementation="reference CUDA build (YKCBCT FdkPipeline, "
-                           "sm_100a, -O3 -use_fast_math), oracle/_ref/libykref.so",
-                           l2="inputs larger than L2"),
-            "e2e": {"value": UPDATES / (ms_host * 1e-3) / 1e9, "unit": "GUPS",
-                    "ms_per_step": ms_host, "h2d_bytes_per_step": int(h_proj.nbytes),
-                    "d2h_bytes_per_step": int(4 * N_VOX ** 3)},
-            "cpu_baseline": cb,
-            "joseph": joseph,
-            "gpu_launches": None,
-        })
-    else:
-        from oracle import oracle as O  # noqa: F401  (the CPU port)
-        for _ in range(args.warmup):
-            cpu_baseline(n_views_sample=8, z_slab=8)
-        vals = [cpu_baseline(n_views_sample=36, z_slab=32) for _ in range(args.steps)]
-        value = sum(v["value"] for v in vals) / len(vals)
-        cb = dict(vals[-1], value=value)
-        line.update({
-            "value": value, "ms_per_step": UPDATES / (value * 1e9) * 1e3, "dtype": "f64",
-            "config": dict(cfg, implementation="FP64 CPU oracle port (no reference build present)",
-                           sample_per_step=cb["sample"]),
-            "cpu_baseline": cb,
-            "e2e": {"value": value, "unit": "GUPS", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0},
-        })
+        filt = RampFilter.named(FILTERS[w.projections])
+        ms_dev, ms_host, vol = R.fdk_time(scan, grid, filt, h_proj, warmup=warmup, reps=steps,
+                                          timeout=1800)
+        z0, nz = PARITY_SLABS[w.name]
+        cb, err = cpu_baseline_leg(w, views, scan_range,
+                                   {"f32": (h_proj, FILTERS[w.projections], vol[z0:z0 + nz])})
+        return ms_dev, ms_host, h_proj.nbytes, cb, err["f32"]
+
+    ms_dev, ms_host, h2d, cb, err = reference_fdk(w, object_seed(0), args.warmup, args.steps)
+    # the reference's FP_Joseph / BP_Joseph operators on the same Joseph
+    # workload (each call re-uploads its texture, as its stock apply does)
+    jscan, jgrid = joseph_workload()
+    gen = np.random.default_rng(11)
+    jx = gen.random(jgrid.shape, dtype=np.float32)
+    jy = gen.standard_normal((J_VIEWS, J_DET, J_DET)).astype(np.float32)
+    _, fp_ms = R.joseph_fp(jscan, jgrid, jx, warmup=args.warmup, reps=args.steps)
+    _, bp_ms = R.joseph_bp(jscan, jgrid, jy, warmup=args.warmup, reps=args.steps)
+    _, pseudo_ms = R.bp_pseudo(jscan, jgrid, jy, warmup=args.warmup, reps=args.steps)
+    _, siddon_fp_ms = R.siddon_fp(jscan, jgrid, jx, warmup=args.warmup, reps=args.steps)
+    _, siddon_bp_ms = R.siddon_bp(jscan, jgrid, jy, warmup=args.warmup, reps=args.steps)
+    samples = J_VIEWS * J_DET * J_DET * J_VOX
+    joseph = {"workload": f"joseph-{J_VOX}^3-{J_VIEWS}v-{J_DET}^2", "fp_ms": fp_ms,
+              "bp_ms": bp_ms, "grad_step_ms": fp_ms + bp_ms,
+              "fp_gsamples": samples / (fp_ms * 1e-3) / 1e9,
+              "bp_gsamples": samples / (bp_ms * 1e-3) / 1e9,
+              "bp_pseudo_matched_ms": pseudo_ms,
+              "bp_pseudo_matched_gups": J_VOX ** 3 * J_VIEWS / (pseudo_ms * 1e-3) / 1e9,
+              "siddon_fp_ms": siddon_fp_ms, "siddon_bp_ms": siddon_bp_ms}
+    line.update({
+        "value": w.updates / (ms_dev * 1e-3) / 1e9, "ms_per_step": ms_dev, "dtype": "f32",
+        "implementation": "reference CUDA build (YKCBCT FdkPipeline, sm_100a, -O3 "
+                          "-use_fast_math), oracle/_ref/libykref.so; inputs from its FP_Joseph",
+        "rel_rmse_vs_oracle": err,
+        "e2e": {"value": w.updates / (ms_host * 1e-3) / 1e9, "unit": "GUPS",
+                "ms_per_step": ms_host, "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(4 * w.n_vox ** 3)},
+        "cpu_baseline": cb,
+        "joseph": joseph,
+        "gpu_launches": None,
+    })
+    if args.config == "c2" and not args.no_large:
+        # the 1024^3 workload, FP32 projections (the reference stores no BF16)
+        wl = WORKLOADS["large"]
+        try:
+            l_dev, l_host, l_h2d, _, l_err = reference_fdk(wl, object_seed(0), LARGE_WARMUP,
+                                                           LARGE_STEPS)
+            line["large"] = {"config": bench_config(wl, world), "steps": LARGE_STEPS,
+                             "warmup": LARGE_WARMUP,
+                             "gups": wl.updates / (l_dev * 1e-3) / 1e9, "ms_per_step": l_dev,
+                             "e2e_gups": wl.updates / (l_host * 1e-3) / 1e9,
+                             "e2e_ms_per_step": l_host, "h2d_bytes_per_step": int(l_h2d),
+                             "rel_rmse_vs_oracle": l_err, "projections_given": "f32"}
+        except Exception as exc:  # reported, never required
+            line["large"] = {"error": str(exc)}
     print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------- our arm ---
+def fdk_form(plan, d_proj, h_proj, vol, h_vol, steps, warmup, timed, slab):
+    """Device-resident and end-to-end timings of one FDK plan; returns
+    (ms, e2e ms, host copy of the parity slab of the device-resident volume)."""
+    for _ in range(warmup):
+        plan.execute(d_proj, vol)
+    ms = timed(lambda: plan.execute(d_proj, vol), steps)
+    plan.check()
+    z0, nz = slab
+    gpu_slab = vol[z0:z0 + nz].cpu().numpy()
+
+    def e2e():
+        plan.execute_host(h_proj, vol, host_out=h_vol)
+
+    for _ in range(max(1, warmup - 1)):
+        e2e()
+    ms_e2e = timed(e2e, steps)
+    plan.check()
+    return ms, ms_e2e, gpu_slab
+
+
+def large_block(world, rank, local, timed, cpu_leg: bool):
+    """The 1024^3 x 1440 x 1536^2 workload, BF16-stored projections: the BF16
+    form (tensor-core BF16 filter, FP32 backprojection) device-resident and
+    end to end, the FP32 form on the same data, both against the oracle."""
+    import torch
+    from fdk_cuda_impl_b200.geometry import RampFilter
+    from fdk_cuda_impl_b200.projectors import FdkPlan
+    from fdk_cuda_impl_b200.workloads import WORKLOADS, make_projections
+    w = WORKLOADS["large"]
+    scan, grid = w.scan(), w.grid()
+    views, proj = make_projections(w, object_seed(rank), local)
+    sl = RampFilter.named(FILTERS[w.projections])
+    plan = FdkPlan(views, w.n_det, w.n_det, scan.scan_range, grid, sl, "bf16", device=local)
+    vol = torch.empty(grid.shape, dtype=torch.float32, device=f"cuda:{local}")
+    h_proj = torch.empty(proj.shape, dtype=proj.dtype, pin_memory=True)
+    h_proj.copy_(proj)
+    h_vol = torch.empty(grid.shape, dtype=torch.float32, pin_memory=True)
+    slab = PARITY_SLABS[w.name]
+    ms, ms_e2e, slab_b = fdk_form(plan, proj, h_proj, vol, h_vol, LARGE_STEPS, LARGE_WARMUP,
+                                  timed, slab)
+    filtered = plan.filter(proj)
+    plan.backproject(filtered, vol)
+    ms_bp = timed(lambda: plan.backproject(filtered, vol), LARGE_STEPS)
+    plan.check()
+    del filtered
+    plan.close()
+    torch.cuda.empty_cache()
+    plan_s = FdkPlan(views, w.n_det, w.n_det, scan.scan_range, grid, sl, "fp32", device=local)
+    plan_s.execute(proj, vol)
+    ms_s = timed(lambda: plan_s.execute(proj, vol), LARGE_STEPS)
+    plan_s.check()
+    slab_s = vol[slab[0]:slab[0] + slab[1]].cpu().numpy()
+    plan_s.close()
+    del proj, vol
+    torch.cuda.empty_cache()
+    out = {"config": bench_config(w, world), "steps": LARGE_STEPS, "warmup": LARGE_WARMUP,
+           "ms_per_step": ms, "gups": job_gups(world, w.updates, ms),
+           "e2e_ms_per_step": ms_e2e, "e2e_gups": job_gups(world, w.updates, ms_e2e),
+           "h2d_bytes_per_step": int(h_proj.numel() * 2), "d2h_bytes_per_step": int(h_vol.numel() * 4),
+           "backproject_ms": ms_bp, "backproject_gups": w.updates / (ms_bp * 1e-3) / 1e9,
+           "fp32_form": {"ms_per_step": ms_s, "gups": job_gups(world, w.updates, ms_s),
+                         "bf16_speedup": ms_s / ms}}
+    if cpu_leg:
+        cb, err = cpu_baseline_leg(w, views, scan.scan_range,
+                                   {"bf16": (h_proj, FILTERS[w.projections], slab_b),
+                                    "fp32": (h_proj, FILTERS[w.projections], slab_s)})
+        out["rel_rmse_vs_oracle"] = err["bf16"]
+        out["fp32_form"]["rel_rmse_vs_oracle"] = err["fp32"]
+        out["oracle_slab"] = list(slab)
+        out["cpu_baseline"] = cb
+    return out
 
 
 def main():
     args = parse()
-    select_config(args.config)
     if args.impl == "reference":
         run_reference(args)
         return
-    import numpy as np
     import torch
     import torch.distributed as dist
-    from fdk_cuda_impl_b200 import CircularScan, RampFilter, VolumeGrid
-    from fdk_cuda_impl_b200 import phantom as PH
-    from fdk_cuda_impl_b200.projectors import FdkPlan, JosephPlan
+    from fdk_cuda_impl_b200 import _lib as L
+    from fdk_cuda_impl_b200.geometry import RampFilter
+    from fdk_cuda_impl_b200.projectors import FdkPlan
+    from fdk_cuda_impl_b200.workloads import WORKLOADS, make_projections
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -406,13 +492,15 @@ def main():
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device(f"cuda:{local}"))
-
-    scan, grid, views, proj = make_workload(rank, local)
-
-    plan = FdkPlan(views, N_DET, N_DET, scan.scan_range, grid, RampFilter(), PRECISION,
-                   device=local)
+    w = WORKLOADS[args.config]
+    scan, grid = w.scan(), w.grid()
+    views, proj = make_projections(w, object_seed(rank), local)
+    precision = "bf16" if w.projections == "bf16" else "fp32"
+    filt = RampFilter.named(FILTERS[w.projections])
+    plan = FdkPlan(views, w.n_det, w.n_det, scan.scan_range, grid, filt, precision, device=local)
     vol = torch.empty(grid.shape, dtype=torch.float32, device=f"cuda:{local}")
     stream = torch.cuda.current_stream()
+    slab = PARITY_SLABS[w.name]
 
     def barrier():
         if world > 1:
@@ -435,8 +523,10 @@ def main():
         plan.execute(proj, vol)
     with ClockSampler(local) as clocks:
         ms = timed(lambda: plan.execute(proj, vol), args.steps)
+    plan.check()
     clock_info = clocks.summary()
-    value = job_gups(world, UPDATES, ms)
+    value = job_gups(world, w.updates, ms)
+    gpu_slab = vol[slab[0]:slab[0] + slab[1]].cpu().numpy()
 
     # stage timings for the roofline (same stream, CUDA events)
     filtered = plan.filter(proj)
@@ -444,6 +534,7 @@ def main():
         plan.backproject(filtered, vol)
     ms_bp = timed(lambda: plan.backproject(filtered, vol), args.steps)
     ms_filter = timed(lambda: plan.filter(proj), args.steps)
+    plan.check()
     del filtered
 
     # end to end through the C-ABI with pinned host buffers: the projections
@@ -452,8 +543,6 @@ def main():
     h_proj = torch.empty(proj.shape, dtype=proj.dtype, pin_memory=True)
     h_proj.copy_(proj)
     h_vol = torch.empty(grid.shape, dtype=torch.float32, pin_memory=True)
-    d_in = proj
-    del proj
 
     def e2e_step():
         plan.execute_host(h_proj, vol, host_out=h_vol)
@@ -461,66 +550,49 @@ def main():
     for _ in range(max(1, args.warmup - 1)):
         e2e_step()
     ms_e2e = timed(e2e_step, args.steps)
-    e2e_value = job_gups(world, UPDATES, ms_e2e)
+    plan.check()
+    e2e_value = job_gups(world, w.updates, ms_e2e)
+    plan.close()
 
     # BF16 form on the same views: projections stored in BF16 (host and
     # device), Shepp-Logan window, tcgen05 split hi/lo Toeplitz filter, the
-    # same backprojection.  Its error is taken against the FP32 form (itself
-    # within 1e-5 of the FP64 oracle) on the same BF16-stored projections.
-    bf16 = fp32_form = None
-    if PRECISION == "bf16":
-        # the FP32 form on the same BF16-stored projections: the error of the
-        # tensor-core filter, and the speed-up it buys
-        plan_s = FdkPlan(views, N_DET, N_DET, scan.scan_range, grid, RampFilter(), "fp32",
-                         device=local)
-        vs = torch.empty_like(vol)
-        for _ in range(max(1, args.warmup - 1)):
-            plan_s.execute(d_in, vs)
-        ms_s = timed(lambda: plan_s.execute(d_in, vs), args.steps)
-        plan.execute(d_in, vol)
-        diff = (vol.double() - vs.double()).pow(2).mean().sqrt() / vs.double().pow(2).mean().sqrt()
-        fp32_form = {"ms_per_step": ms_s, "gups": world * UPDATES / (ms_s * 1e-3) / 1e9,
-                     "bf16_speedup": ms_s / ms, "bf16_rel_rmse_vs_fp32_form": float(diff)}
-        plan_s.close()
-        del vs
-    elif not args.no_bf16:
+    # same backprojection; against the FP64 oracle on the same BF16-stored
+    # projections (cpu leg) and against the FP32 form on them
+    bf16 = None
+    h_proj_b = None
+    if precision == "fp32" and not args.no_bf16:
         sl = RampFilter.named("shepplogan")
-        plan_b = FdkPlan(views, N_DET, N_DET, scan.scan_range, grid, sl, "bf16", device=local)
-        h_proj_b = torch.empty(h_proj.shape, dtype=torch.bfloat16, pin_memory=True)
-        h_proj_b.copy_(h_proj)
-        d_in_b = d_in.to(torch.bfloat16)
-        plan_s = FdkPlan(views, N_DET, N_DET, scan.scan_range, grid, sl, "fp32", device=local)
+        d_in_b = proj.to(torch.bfloat16)
+        plan_s = FdkPlan(views, w.n_det, w.n_det, scan.scan_range, grid, sl, "fp32", device=local)
         ref_vol = plan_s.execute(d_in_b, vol).clone()
+        plan_s.check()
         plan_s.close()
+        plan_b = FdkPlan(views, w.n_det, w.n_det, scan.scan_range, grid, sl, "bf16", device=local)
+        h_proj_b = torch.empty(h_proj.shape, dtype=torch.bfloat16, pin_memory=True)
+        h_proj_b.copy_(d_in_b)
         vb = torch.empty_like(vol)
-        for _ in range(args.warmup):
-            plan_b.execute(d_in_b, vb)
-        ms_b = timed(lambda: plan_b.execute(d_in_b, vb), args.steps)
+        ms_b, ms_be, gpu_slab_b = fdk_form(plan_b, d_in_b, h_proj_b, vb, h_vol, args.steps,
+                                           args.warmup, timed, slab)
         diff = (vb.double() - ref_vol.double()).pow(2).mean().sqrt() / ref_vol.double().pow(2).mean().sqrt()
-
-        def e2e_b():
-            plan_b.execute_host(h_proj_b, vb, host_out=h_vol)
-
-        for _ in range(max(1, args.warmup - 1)):
-            e2e_b()
-        ms_be = timed(e2e_b, args.steps)
-        bf16 = {"ms_per_step": ms_b, "gups": world * UPDATES / (ms_b * 1e-3) / 1e9,
+        bf16 = {"ms_per_step": ms_b, "gups": job_gups(world, w.updates, ms_b),
                 "speedup_vs_fp32": ms / ms_b, "rel_rmse_vs_fp32_form": float(diff),
-                "e2e_ms_per_step": ms_be, "e2e_gups": world * UPDATES / (ms_be * 1e-3) / 1e9,
+                "e2e_ms_per_step": ms_be, "e2e_gups": job_gups(world, w.updates, ms_be),
                 "e2e_speedup_vs_fp32": ms_e2e / ms_be,
                 "h2d_bytes_per_step": int(h_proj_b.numel() * 2), "filter": "shepplogan",
                 "projections": "bf16"}
         plan_b.close()
-        del ref_vol, vb, d_in_b, h_proj_b
+        del ref_vol, vb, d_in_b
+    del proj
+    torch.cuda.empty_cache()
 
     joseph = None
-    if not args.no_joseph and PRECISION == "fp32":
+    if not args.no_joseph and args.config == "c2":
         joseph = joseph_step(local, args.steps, args.warmup, timed)
 
     peaks, peak_src = measured_peaks()
     # HBM roofline of the dominant kernel (backprojection): compulsory bytes
     # per launch = filtered projections read once + volume written once.
-    bp_bytes = 4.0 * N_VIEWS * N_DET * N_DET + 4.0 * N_VOX ** 3
+    bp_bytes = 4.0 * w.n_views * w.n_det ** 2 + 4.0 * w.n_vox ** 3
     achieved = bp_bytes / (ms_bp * 1e-3) / 1e9
     # DRAM traffic of one launch: ncu (dram__bytes_read + write) on the
     # 256^3 x 360 x 384^2 case gave 830.8 MB against 279.4 MB compulsory
@@ -530,31 +602,31 @@ def main():
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "peak_source": peak_src,
                 "traffic_source": "ncu 256^3x360x384^2 capture scaled by compulsory bytes",
-                "kernel": "fdk_bp_tma_kernel<52,1,1> (TMA-staged tap pairs)", "kernel_ms": ms_bp,
+                "kernel": "fdk_bp_tma_kernel (TMA-staged tap pairs)", "kernel_ms": ms_bp,
                 "algorithmic_bytes_per_launch": bp_bytes}
-    # on-chip view of the same kernel: 16 B of bilinear taps per update
-    sm_mhz = clock_info.get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
-    onchip_peak = 148 * 128 * sm_mhz * 1e6 / 1e9  # GB/s of shared/L1 bandwidth
-    onchip = {"tap_bytes_per_update": 16, "achieved_gbs": 16 * UPDATES / (ms_bp * 1e-3) / 1e9,
-              "peak_gbs_nominal": onchip_peak,
-              "frac": 16 * UPDATES / (ms_bp * 1e-3) / 1e9 / onchip_peak,
-              "bp_gups": UPDATES / (ms_bp * 1e-3) / 1e9}
+    # the bound that binds: 16 B of bilinear taps per update, loaded from
+    # shared memory as two 8-byte tap pairs, against the measured 8-byte
+    # shared-load bandwidth of this GPU
+    import ctypes as C
+    smem = C.c_double(0.0)
+    smem_status = L.load().ykb_measure_shared_load_gbs(local, 8, C.byref(smem))
+    tap_gbs = 16 * w.updates / (ms_bp * 1e-3) / 1e9
+    onchip = {"tap_bytes_per_update": 16, "achieved_gbs": tap_gbs,
+              "bp_gups": w.updates / (ms_bp * 1e-3) / 1e9}
+    if smem_status == L.OK:
+        onchip.update({"peak_gbs": smem.value, "frac": tap_gbs / smem.value,
+                       "peak_source": "measured: ykb_measure_shared_load_gbs, 8-byte "
+                                      "conflict-free shared loads, 4 CTAs per SM"})
+    else:
+        onchip["peak_error"] = L.load().ykb_last_error().decode()
 
     line = {
         "metric": METRIC,
         "value": value, "unit": "GUPS", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32" if PRECISION == "fp32" else "bf16 filter, f32 backprojection",
+        "vs_baseline": None, "dtype": "f32" if precision == "fp32" else "bf16 filter, f32 backprojection",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "volume": [N_VOX] * 3, "voxel_mm": VOX_MM,
-                   "views": N_VIEWS, "detector": [N_DET, N_DET], "pixel_mm": PIX_MM,
-                   "sid_sdd_mm": [SID, SDD], "ellipsoids": N_ELL, "spheres": N_SPH,
-                   "noise_i0": I0, "filter": "ramlak", "precision": PRECISION,
-                   "projections": "bf16" if PRECISION == "bf16" else "f32",
-                   "l2": f"inputs larger than L2 ({h_proj.numel() * h_proj.element_size() / 1e9:.1f} GB "
-                         f"projections, {4 * N_VOX ** 3 / 1e9:.2f} GB volume)",
-                   "chunk_views": chunk_views(),
-                   "parallelism": f"independent objects x{world}"},
+        "config": bench_config(w, world),
         "stages_ms": {"filter": ms_filter, "backproject": ms_bp},
         "roofline": roofline,
         "onchip": onchip,
@@ -562,23 +634,41 @@ def main():
                 "h2d_bytes_per_step": int(h_proj.numel() * h_proj.element_size()),
                 "d2h_bytes_per_step": int(h_vol.numel() * 4)},
         "bf16": bf16,
-        "fp32_form": fp32_form,
         "joseph": joseph,
         # preweight, filter and backprojection per workspace chunk
-        "gpu_launches": 3 * -(-N_VIEWS // chunk_views()) * args.steps,
+        "gpu_launches": 3 * -(-w.n_views // plan_chunk_views(w)) * args.steps,
         "clocks": clock_info,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            line["cpu_baseline"] = (cpu_baseline() if N_DET <= 768 else
-                                    cpu_baseline(n_views_sample=24, z_slab=32))
+            forms = {"f32": (h_proj, FILTERS[w.projections], gpu_slab)}
+            if h_proj_b is not None:
+                forms["bf16"] = (h_proj_b, "shepplogan", gpu_slab_b)
+            cb, err = cpu_baseline_leg(w, views, scan.scan_range, forms)
+            line["cpu_baseline"] = cb
+            line["rel_rmse_vs_oracle"] = err["f32"]
+            line["oracle_slab"] = list(slab)
+            if bf16 is not None:
+                bf16["rel_rmse_vs_oracle"] = err["bf16"]
         except Exception as exc:  # the baseline is reported, never required
             line["cpu_baseline"] = {"error": str(exc)}
+    del h_proj, h_proj_b, h_vol
+    if world == 1 and args.config == "c2" and not args.no_large:
+        try:
+            line["large"] = large_block(world, rank, local, timed,
+                                        cpu_leg=rank == 0 and not args.no_cpu_baseline)
+        except Exception as exc:
+            line["large"] = {"error": str(exc)}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    plan.close()
     if world > 1:
         dist.destroy_process_group()
+
+
+def plan_chunk_views(w) -> int:
+    """Views per workspace chunk of an FDK plan: a budget of 8 GiB at 12 bytes
+    per detector pixel (preweighted rows + filtered tap pairs)."""
+    return max(1, min(w.n_views, (8 << 30) // (12 * w.n_det * w.n_det)))
 
 
 if __name__ == "__main__":

@@ -85,6 +85,7 @@ SIGNATURES = {
     "ykb_fdk_backproject": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_int, _P, C.c_int, _P]),
     "ykb_fdk_workspace_bytes": (C.c_size_t, [_P]),
     "ykb_fdk_check": (C.c_int, [_P, _P]),
+    "ykb_fdk_test_pipeline_wait": (C.c_int, [_P, C.c_ulonglong, C.c_int]),
     "ykb_fdk_filter_static": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_float, C.POINTER(Filter),
                                         _P, C.c_int, _P, _P]),
     "ykb_joseph_plan_create": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.POINTER(Volume),
@@ -100,6 +101,7 @@ SIGNATURES = {
     "ykb_dot_f64": (C.c_int, [_P, _P, _P, C.c_size_t, _P, _P]),
     "ykb_cgls_update_xr": (C.c_int, [_P, _P, _P, _P, _P, C.c_size_t, _P, _P, C.c_size_t, _P]),
     "ykb_cgls_update_p": (C.c_int, [_P, _P, _P, _P, _P, C.c_size_t, _P]),
+    "ykb_measure_shared_load_gbs": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_double)]),
 }
 
 # ykb_task == YK::ETask values

@@ -22,8 +22,10 @@
 //   * consumers read the four taps from shared memory without bounds checks:
 //     the box is sized by a pre-pass over all (tile, view) pairs with the same
 //     footprint function, and each (column, view) checks its end points.
-// Every mbarrier wait is bounded (~2 s of %globaltimer); a timeout sets the
-// plan's error word, stops the CTA and drains the copies in flight.
+// Every mbarrier wait is bounded (~2 s of %globaltimer by default; the
+// pipeline waits take the limit as a kernel argument, so that a test can
+// shorten it); a timeout sets the plan's error word, stops the CTA and drains
+// the copies in flight, each drain wait with the full limit.
 #include "ykb_internal.hpp"
 
 #include <cuda.h>
@@ -92,13 +94,14 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
     return ok != 0;
 }
 
-// bounded wait: false after ~2 s
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
+// bounded wait: false after limit_ns
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
+    unsigned long long limit_ns = kWaitNs)
 {
     if (mbar_try_wait(bar, parity)) return true;
     const unsigned long long t0 = global_ns();
     while (!mbar_try_wait(bar, parity))
-        if (global_ns() - t0 > kWaitNs) return false;
+        if (global_ns() - t0 > limit_ns) return false;
     return true;
 }
 
@@ -302,7 +305,7 @@ template <int BW, bool AXIAL, bool PAIR, bool PSEUDO, int ZC>
 __device__ __forceinline__ void bp_tile(const CUtensorMap& map,
     const FdkViewCoef* __restrict__ coef, int n_views, const VolumeGrid& g, int BH, int stages,
     float* __restrict__ vol, int accumulate, int* __restrict__ err,
-    const PseudoViewCoef* __restrict__ pseudo, int za)
+    const PseudoViewCoef* __restrict__ pseudo, int za, PipelineWait pw)
 {
     extern __shared__ unsigned char smem_raw[];
     // 128-byte aligned base (the launch requests 128 bytes of slack)
@@ -345,11 +348,17 @@ __device__ __forceinline__ void bp_tile(const CUtensorMap& map,
         for (int k = 0; k < n_views; ++k, (++s == stages ? (s = 0, ++use) : 0)) {
             int go = 1;
             if (lane == 0) {
-                if (use > 0 && !mbar_wait(&empty[s], (use - 1) & 1)) go = 0;
+                if (use > 0 && !mbar_wait(&empty[s], (use - 1) & 1, pw.limit_ns)) go = 0;
                 if (*(volatile int*)&abort_flag) go = 0;
             }
             go = __shfl_sync(0xffffffffu, go, 0);
             if (!go) { ok = false; break; }
+            if (k == pw.withheld_view) {
+                // test hook: no copy and no arrival for this view, so every
+                // wait for it runs out
+                issued = k + 1;
+                continue;
+            }
             double umin = 1e300, umax = -1e300, vmin = 1e300, vmax = -1e300;
             if (lane < 8) {
                 corner_uv(coef[k], (lane & 1) ? tg.x1 : tg.x0, (lane & 2) ? tg.y1 : tg.y0,
@@ -388,7 +397,8 @@ __device__ __forceinline__ void bp_tile(const CUtensorMap& map,
             *(volatile int*)&abort_flag = 1;
             // drain: every issued copy must land before the CTA exits
             const int first = max(0, issued - stages);
-            for (int k = first; k < issued; ++k) mbar_wait(&full[k % stages], (k / stages) & 1);
+            for (int k = first; k < issued; ++k)
+                if (k != pw.withheld_view) mbar_wait(&full[k % stages], (k / stages) & 1);
         }
         return;
     }
@@ -414,9 +424,13 @@ __device__ __forceinline__ void bp_tile(const CUtensorMap& map,
     int s = 0;
     uint32_t phase = 0;
     for (int k = 0; k < n_views; ++k, (++s == stages ? (s = 0, phase ^= 1u) : 0)) {
-        if (!mbar_wait(&full[s], phase)) {
-            atomicOr(err, kErrTimeout);
-            *(volatile int*)&abort_flag = 1;
+        // the warp leaves together: a lane whose wait ran out takes its whole
+        // warp with it, so no lane is left waiting at the warp barrier below
+        if (!__all_sync(0xffffffffu, mbar_wait(&full[s], phase, pw.limit_ns))) {
+            if (lane == 0) {
+                atomicOr(err, kErrTimeout);
+                *(volatile int*)&abort_flag = 1;
+            }
             return;
         }
         const int4 b = boxes[s];
@@ -619,15 +633,15 @@ template <int BW, bool AXIAL, bool PAIR, bool PSEUDO>
 __global__ void __launch_bounds__(NTHREADS, 2) fdk_bp_tma_kernel(const __grid_constant__ CUtensorMap map,
     const FdkViewCoef* __restrict__ coef, int n_views, VolumeGrid g, int BH, int stages,
     float* __restrict__ vol, int accumulate, int* __restrict__ err,
-    const PseudoViewCoef* __restrict__ pseudo, int main_tiles)
+    const PseudoViewCoef* __restrict__ pseudo, int main_tiles, PipelineWait pw)
 {
     const int bz = static_cast<int>(blockIdx.z);
     if (bz < main_tiles)
         bp_tile<BW, AXIAL, PAIR, PSEUDO, ZT>(map, coef, n_views, g, BH, stages, vol, accumulate,
-            err, pseudo, bz * ZT);
+            err, pseudo, bz * ZT, pw);
     else
         bp_tile<BW, AXIAL, PAIR, PSEUDO, kZTail>(map, coef, n_views, g, BH, stages, vol,
-            accumulate, err, pseudo, main_tiles * ZT + (bz - main_tiles) * kZTail);
+            accumulate, err, pseudo, main_tiles * ZT + (bz - main_tiles) * kZTail, pw);
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
@@ -653,7 +667,7 @@ constexpr int kWidths[] = {36, 52, 68, 100, 132, 196, 256};
 template <typename K>
 cudaError_t launch_kernel(K k, const CUtensorMap& map, const FdkViewCoef* coef, int n_views,
     const VolumeGrid& g, int BH, int stages, size_t smem, float* vol, int accumulate, int* err,
-    const PseudoViewCoef* pseudo, cudaStream_t s)
+    const PseudoViewCoef* pseudo, PipelineWait pw, cudaStream_t s)
 {
     const int rem = g.nz % ZT;
     const bool tail = rem > 0 && rem <= kZTail;
@@ -663,45 +677,45 @@ cudaError_t launch_kernel(K k, const CUtensorMap& map, const FdkViewCoef* coef, 
         static_cast<int>(smem));
     if (e != cudaSuccess) return e;
     k<<<grid, NTHREADS, smem, s>>>(map, coef, n_views, g, BH, stages, vol, accumulate, err, pseudo,
-        main_tiles);
+        main_tiles, pw);
     return cudaGetLastError();
 }
 
 template <int BW, bool PAIR>
 cudaError_t launch_bw(const CUtensorMap& map, const FdkViewCoef* coef, int n_views,
     const VolumeGrid& g, int BH, int stages, size_t smem, bool axial, float* vol, int accumulate,
-    int* err, const PseudoViewCoef* pseudo, cudaStream_t s)
+    int* err, const PseudoViewCoef* pseudo, PipelineWait pw, cudaStream_t s)
 {
     if constexpr (PAIR) {
         if (pseudo && axial)
             return launch_kernel(fdk_bp_tma_kernel<BW, true, true, true>, map, coef, n_views, g,
-                BH, stages, smem, vol, accumulate, err, pseudo, s);
+                BH, stages, smem, vol, accumulate, err, pseudo, pw, s);
         if (pseudo)
             return launch_kernel(fdk_bp_tma_kernel<BW, false, true, true>, map, coef, n_views, g,
-                BH, stages, smem, vol, accumulate, err, pseudo, s);
+                BH, stages, smem, vol, accumulate, err, pseudo, pw, s);
     } else {
         if (pseudo) return cudaErrorInvalidValue;  // pseudo-matched input is staged as pairs
     }
     if (axial)
         return launch_kernel(fdk_bp_tma_kernel<BW, true, PAIR, false>, map, coef, n_views, g, BH,
-            stages, smem, vol, accumulate, err, pseudo, s);
+            stages, smem, vol, accumulate, err, pseudo, pw, s);
     return launch_kernel(fdk_bp_tma_kernel<BW, false, PAIR, false>, map, coef, n_views, g, BH,
-        stages, smem, vol, accumulate, err, pseudo, s);
+        stages, smem, vol, accumulate, err, pseudo, pw, s);
 }
 
 template <bool PAIR>
 cudaError_t launch_layout(const CUtensorMap& map, const FdkViewCoef* coef, int n_views,
     const VolumeGrid& g, int bw, int bh, int stages, size_t smem, bool axial, float* vol,
-    int accumulate, int* err, const PseudoViewCoef* pseudo, cudaStream_t s)
+    int accumulate, int* err, const PseudoViewCoef* pseudo, PipelineWait pw, cudaStream_t s)
 {
     switch (bw) {
-    case 36: return launch_bw<36, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, s);
-    case 52: return launch_bw<52, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, s);
-    case 68: return launch_bw<68, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, s);
-    case 100: return launch_bw<100, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, s);
-    case 132: return launch_bw<132, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, s);
-    case 196: return launch_bw<196, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, s);
-    case 256: return launch_bw<256, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, s);
+    case 36: return launch_bw<36, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, pw, s);
+    case 52: return launch_bw<52, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, pw, s);
+    case 68: return launch_bw<68, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, pw, s);
+    case 100: return launch_bw<100, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, pw, s);
+    case 132: return launch_bw<132, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, pw, s);
+    case 196: return launch_bw<196, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, pw, s);
+    case 256: return launch_bw<256, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, pw, s);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -747,7 +761,7 @@ bool fdk_tma_available() { return encode_fn() != nullptr; }
 cudaError_t launch_fdk_backproject_tma(const float* filtered, int layout, int ld,
     int rows_total_views, const FdkViewCoef* coef, int n_views, int nu, int nv,
     const VolumeGrid& g, bool axial, int bw, int bh, float* vol, int accumulate, int* err,
-    cudaStream_t s, const PseudoViewCoef* pseudo)
+    cudaStream_t s, const PseudoViewCoef* pseudo, PipelineWait pw)
 {
     auto enc = encode_fn();
     if (!enc) return cudaErrorNotSupported;
@@ -772,9 +786,9 @@ cudaError_t launch_fdk_backproject_tma(const float* filtered, int layout, int ld
     const size_t ring = static_cast<size_t>(stage_stride_floats(bw, bh, pair)) * sizeof(float) * stages;
     const size_t smem = 128 + ring + 2 * stages * sizeof(uint64_t) + stages * sizeof(int4) + 16;
     return pair ? launch_layout<true>(map, coef, n_views, g, bw, bh, stages, smem, axial, vol,
-                      accumulate, err, pseudo, s)
+                      accumulate, err, pseudo, pw, s)
                 : launch_layout<false>(map, coef, n_views, g, bw, bh, stages, smem, axial, vol,
-                      accumulate, err, pseudo, s);
+                      accumulate, err, pseudo, pw, s);
 }
 
 // Scalar filtered rows [rows][ld_in] -> tap pairs [rows][ldp]: element

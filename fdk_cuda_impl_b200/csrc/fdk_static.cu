@@ -15,7 +15,9 @@
 namespace ykb {
 namespace {
 
-// 32 MiB per device, held by every GPU that loads the library until exit.
+// 32 MiB per device, held by every GPU that loads the library until exit:
+// 64 KiB of ramp lags, 2.5 MiB of per-view records and 30,867,456 bytes
+// (29.4 MiB) for the preweighted rows of the views filtered at once.
 constexpr size_t kStaticBytes = size_t(32) << 20;
 constexpr int kStaticMaxNu = 8192;       // ramp lags: 2*nu-1 floats
 constexpr int kStaticMaxViews = 16384;   // per-view records
@@ -73,6 +75,14 @@ extern "C" YKB_API ykb_status ykb_fdk_filter_static(const ykb_cone_view* views, 
         return (set_error("ykb_fdk_filter_static limits: nu <= 8192, n_views <= 16384 and one "
                           "view's nu*nv*4 bytes <= " + std::to_string(kRowsBytes) + " bytes"),
             YKB_ERR_INVALID_CONFIG);
+    // a short scan needs Parker redundancy weights between the preweight and
+    // the filter, which take the scan's start angle and direction: a plan
+    // (ykb_fdk_plan_create_ex) applies them; this entry point has no such
+    // arguments and refuses rather than return unweighted rows
+    if (scan_range_rad < 6.28318530717958647692f - 1e-5f)
+        return (set_error("ykb_fdk_filter_static filters full scans only (scan range >= 2 pi): "
+                          "a short scan needs Parker weights, which a plan from "
+                          "ykb_fdk_plan_create_ex applies"), YKB_ERR_INVALID_CONFIG);
     int device = 0;
     if (const cudaError_t e = cudaGetDevice(&device)) return cuda_status(e, "cudaGetDevice");
     unsigned char* base = nullptr;

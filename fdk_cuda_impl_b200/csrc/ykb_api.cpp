@@ -358,11 +358,11 @@ ykb_status backproject_chunk(ykb_fdk_plan* p, const void* filtered, int layout, 
     if (layout == kFilteredPairs) {
         YKB_TRY_CUDA(launch_fdk_backproject_tma(static_cast<const float*>(filtered), layout, ld,
             count, coef, count, p->nu, p->nv, grid, p->axial, p->tma_bw, p->tma_bh, vol,
-            accumulate, p->err_flag.as<int>(), s));
+            accumulate, p->err_flag.as<int>(), s, nullptr, p->bp_wait));
     } else if (p->use_tma && ld % 4 == 0 && aligned) {
         YKB_TRY_CUDA(launch_fdk_backproject_tma(static_cast<const float*>(filtered), layout, ld,
             count, coef, count, p->nu, p->nv, grid, p->axial, p->tma_bw, p->tma_bh, vol,
-            accumulate, p->err_flag.as<int>(), s));
+            accumulate, p->err_flag.as<int>(), s, nullptr, p->bp_wait));
     } else {
         YKB_TRY_CUDA(launch_fdk_backproject(filtered, YKB_DTYPE_F32, coef, count, p->nu, p->nv,
             ld, grid, p->axial, vol, accumulate, s));
@@ -557,6 +557,17 @@ YKB_API ykb_status ykb_fdk_execute_host_out(ykb_fdk_plan* p, const void* h_proj,
     DeviceGuard guard(p->device);
     return stream_host(p, h_proj, proj_dtype, view_offset, n_views, d_volume, h_volume,
         clear_output, reinterpret_cast<cudaStream_t>(stream));
+}
+
+YKB_API ykb_status ykb_fdk_test_pipeline_wait(ykb_fdk_plan* p, unsigned long long wait_ns,
+    int withheld_view)
+{
+    clear_error();
+    if (!p) return fail(YKB_ERR_INVALID_BUFFER, "null plan");
+    if (withheld_view < -1) return fail(YKB_ERR_INVALID_CONFIG, "withheld_view must be >= -1");
+    p->bp_wait.limit_ns = wait_ns ? wait_ns : PipelineWait{}.limit_ns;
+    p->bp_wait.withheld_view = withheld_view;
+    return YKB_OK;
 }
 
 YKB_API ykb_status ykb_fdk_check(ykb_fdk_plan* p, ykb_stream stream)

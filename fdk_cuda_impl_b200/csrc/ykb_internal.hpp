@@ -217,12 +217,20 @@ int fdk_tma_stages(int bw, int bh, int layout);
 int fdk_tma_z_tile();
 cudaError_t fdk_tma_box(const FdkViewCoef* coef, int n_views, const VolumeGrid& g,
     int* scratch2, int* bw, int* bh, cudaStream_t s);
+// Limit of the TMA backprojection's pipeline waits (a wait that runs out
+// sets the error word and stops the CTA) and, for tests of that path, a view
+// whose copy the producer withholds (-1: none).  Waits that drain copies in
+// flight keep the default limit.
+struct PipelineWait {
+    unsigned long long limit_ns = 2000000000ull;
+    int withheld_view = -1;
+};
 // pseudo != nullptr: the pseudo-matched weight of PseudoViewCoef replaces the
 // FDK depth weight (tap-pair layout only)
 cudaError_t launch_fdk_backproject_tma(const float* filtered, int layout, int ld,
     int views_in_buffer, const FdkViewCoef* coef, int n_views, int nu, int nv,
     const VolumeGrid& g, bool axial, int bw, int bh, float* vol, int accumulate, int* err,
-    cudaStream_t s, const PseudoViewCoef* pseudo = nullptr);
+    cudaStream_t s, const PseudoViewCoef* pseudo = nullptr, PipelineWait pw = PipelineWait{});
 // Pseudo-matched backprojection straight from projections [n][nv][nu] with
 // bounds-checked loads (used when the TMA box does not fit)
 cudaError_t launch_pseudo_backproject(const float* proj, const FdkViewCoef* coef,
@@ -276,6 +284,7 @@ struct ykb_fdk_plan {
     int lda = 0;                 // row pitch of the bf16 GEMM operands (tensor-core filter)
     bool use_tma = false;        // TMA-staged backprojection
     int tma_bw = 0, tma_bh = 0;  // its projection box
+    ykb::PipelineWait bp_wait;   // its pipeline-wait limit (tests shorten it)
     std::vector<ykb::FdkDerived> derived;
     ykb::DeviceBuffer coef;      // FdkViewCoef[n_views]
     ykb::DeviceBuffer pwv;       // FdkPreweightView[n_views]

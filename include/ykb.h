@@ -227,19 +227,33 @@ YKB_API size_t ykb_fdk_workspace_bytes(const ykb_fdk_plan* plan);
  * equivalent: it aborts the process on CUDA errors (src/global/YkMacro.hpp:35-41). */
 YKB_API ykb_status ykb_fdk_check(ykb_fdk_plan* plan, ykb_stream stream);
 
+/* Test hook for the timeout path of the TMA backprojection: sets the limit
+ * of its pipeline waits to wait_ns (0 restores the default, about 2 s) and,
+ * when withheld_view >= 0, makes the copy producer skip that view (an index
+ * within each backprojection launch) so that every wait for it runs out.  A
+ * wait that runs out sets the plan's error word, which ykb_fdk_check
+ * reports; the kernel ends without hanging, its copies in flight drained, and
+ * the plan stays usable (call again with 0, -1 to restore).  Waits that drain
+ * copies keep the default limit.  No counterpart in the reference. */
+YKB_API ykb_status ykb_fdk_test_pipeline_wait(ykb_fdk_plan* plan,
+    unsigned long long wait_ns, int withheld_view);
+
 /* The preweight + ramp filter stage of ykb_fdk_filter for callers that
  * cannot call cudaMalloc (an application whose memory pool owns the GPU,
  * a real-time loop that forbids allocation after start-up): no plan and no
  * device allocation.  This entry point has no counterpart in the reference.
  * Geometry and filter come from the host arguments (as ykb_fdk_plan_create
  * takes them); d_proj holds [n_views][nv][nu] (proj_dtype), d_filtered
- * receives [n_views][nv][nu] float.  Scratch is one fixed 32 MiB device
- * array inside the library, present on every GPU that loads it until exit;
- * limits: nu <= 8192, n_views <= 16384, nu*nv*4 bytes <= 31.8 MiB per view,
- * else YKB_ERR_INVALID_CONFIG.  The first call on a device looks up that
- * device's scratch address (make it before any stream capture).  All calls
- * share the one array: calls that overlap on the GPU (different streams,
- * without ordering between them) race and corrupt each other. */
+ * receives [n_views][nv][nu] float.  Full scans only (scan_range_rad >=
+ * 2 pi): a short scan needs Parker weights, which only a plan applies, and
+ * returns YKB_ERR_INVALID_CONFIG.  Scratch is one fixed 32 MiB device array
+ * inside the library, present on every GPU that loads it until exit;
+ * limits: nu <= 8192, n_views <= 16384, nu*nv*4 <= 30,867,456 bytes
+ * (29.4 MiB) per view, else YKB_ERR_INVALID_CONFIG.  The first call on a
+ * device looks up that device's scratch address (make it before any stream
+ * capture).  All calls share the one array: calls that overlap on the GPU
+ * (different streams, without ordering between them) race and corrupt each
+ * other. */
 YKB_API ykb_status ykb_fdk_filter_static(const ykb_cone_view* views,
     int n_views, int nu, int nv, float scan_range_rad, const ykb_filter* filter,
     const void* d_proj, int proj_dtype, float* d_filtered, ykb_stream stream);
@@ -337,6 +351,16 @@ YKB_API ykb_status ykb_cgls_update_xr(ykb_iter* ctx, const double* d_gamma, cons
     ykb_stream stream);
 YKB_API ykb_status ykb_cgls_update_p(ykb_iter* ctx, const double* d_gamma_new,
     const double* d_gamma_old, float* d_p, const float* d_z, size_t n, ykb_stream stream);
+
+/* ----------------------------------------------------------- diagnostics --- */
+
+/* Measures the shared-memory load bandwidth of `device` (GB/s over all its
+ * SMs): 4 CTAs per SM stream 16 KB of shared memory with conflict-free
+ * vector loads of bytes_per_lane (8 or 16) bytes, best of five timed
+ * launches (CUDA events) after one warm-up.  The on-chip peak that the
+ * backprojection's two 8-byte tap-pair loads per voxel update are reported
+ * against.  Synchronous; no counterpart in the reference. */
+YKB_API ykb_status ykb_measure_shared_load_gbs(int device, int bytes_per_lane, double* gbs);
 
 #ifdef __cplusplus
 }

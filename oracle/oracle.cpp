@@ -704,24 +704,23 @@ int orc_fdk_filter(const orc_view* views, int n, int nu, int nv, float range,
     return orc_fdk_filter_weighted(views, n, nu, nv, range, filter, proj, nullptr, filtered);
 }
 
-int orc_fdk_filter_weighted(const orc_view* views, int n, int nu, int nv, float range,
-    const orc_filter* filter, const float* proj, const double* row_weights, double* filtered)
+namespace {
+
+// Rows [row0, row0 + nrows) of the preweighted and ramp-filtered
+// projections (proj and filtered hold only those rows, [n][nrows][nu]).  The
+// filter acts on each detector row alone, so a band of rows filters exactly
+// as it would inside the full detector.
+void filter_rows(const std::vector<Derived>& g, const std::vector<double>& h, int n, int nu,
+    int row0, int nrows, const float* proj, const double* row_weights, double* filtered)
 {
-    if (!filter || !proj || !filtered) return -1;
-    std::vector<Derived> g;
-    if (!derive(views, n, nu, nv, range, g)) return -2;
-    std::vector<double> h;
-    // the reference builds the weights once, with du of the first view of the
-    // first chunk (.../FDK/YkFDKFilterProcessor.hpp:111,216-232)
-    ramp_kernel(nu, g[0].du, *filter, h);
     const int N = padded_n(nu);
 #pragma omp parallel
     {
         std::vector<double> row(nu);
 #pragma omp for schedule(static)
-        for (long r = 0; r < static_cast<long>(n) * nv; ++r) {
-            const int i = static_cast<int>(r / nv);
-            const int iv = static_cast<int>(r % nv);
+        for (long r = 0; r < static_cast<long>(n) * nrows; ++r) {
+            const int i = static_cast<int>(r / nrows);
+            const int iv = row0 + static_cast<int>(r % nrows);
             const Derived& d = g[i];
             const double wgeom = d.dsd / d.sid / 2.0;
             const float* src = proj + static_cast<size_t>(r) * nu;
@@ -742,22 +741,16 @@ int orc_fdk_filter_weighted(const orc_view* views, int n, int nu, int nv, float 
             }
         }
     }
-    return 0;
 }
 
 // Voxel-driven weighted backprojection (.../FDK/kernels/YkFDKBpKernels.cu:
 // 112-209 with the coefficient definitions of YkFDKBpPrecompute.cu:14-138):
 // vol += sum_views bilinear(u,v) * SID^2 * dtheta * (2pi/range) / depth^2,
-// bilinear with zero border at pixel coordinates (u,v).
-int orc_fdk_backproject(const orc_view* views, int n, int nu, int nv,
-    float range, const orc_volume* vol, const double* filtered, double* volume,
-    int flags)
+// bilinear with zero border at pixel coordinates (u,v).  The filtered rows
+// present are [row0, row0 + nrows); rows outside read as zero.
+void backproject_rows(const std::vector<Derived>& g, int n, int nu, int row0, int nrows,
+    const orc_volume& V, const double* filtered, double* volume, bool tex)
 {
-    if (!valid_volume(vol) || !filtered || !volume) return -1;
-    std::vector<Derived> g;
-    if (!derive(views, n, nu, nv, range, g)) return -2;
-    const bool tex = (flags & 1) != 0;
-    const orc_volume V = *vol;
 #pragma omp parallel for collapse(2) schedule(static)
     for (int z = 0; z < V.nz; ++z)
         for (int y = 0; y < V.ny; ++y)
@@ -771,11 +764,84 @@ int orc_fdk_backproject(const orc_view* views, int n, int nu, int nv,
                     double u, v, depth;
                     project_point(d, P, u, v, depth);
                     const double w = d.sid * d.sid * d.dtheta * d.fscale / (depth * depth);
-                    acc += w * bilerp_zero(filtered + static_cast<size_t>(i) * nu * nv,
-                        nu, nv, u, v, tex);
+                    acc += w * bilerp_zero(filtered + static_cast<size_t>(i) * nu * nrows,
+                        nu, nrows, u, v - row0, tex);
                 }
                 volume[(static_cast<size_t>(z) * V.ny + y) * V.nx + x] += acc;
             }
+}
+
+} // namespace
+
+int orc_fdk_filter_weighted(const orc_view* views, int n, int nu, int nv, float range,
+    const orc_filter* filter, const float* proj, const double* row_weights, double* filtered)
+{
+    if (!filter || !proj || !filtered) return -1;
+    std::vector<Derived> g;
+    if (!derive(views, n, nu, nv, range, g)) return -2;
+    std::vector<double> h;
+    // the reference builds the weights once, with du of the first view of the
+    // first chunk (.../FDK/YkFDKFilterProcessor.hpp:111,216-232)
+    ramp_kernel(nu, g[0].du, *filter, h);
+    filter_rows(g, h, n, nu, 0, nv, proj, row_weights, filtered);
+    return 0;
+}
+
+int orc_fdk_backproject(const orc_view* views, int n, int nu, int nv,
+    float range, const orc_volume* vol, const double* filtered, double* volume,
+    int flags)
+{
+    if (!valid_volume(vol) || !filtered || !volume) return -1;
+    std::vector<Derived> g;
+    if (!derive(views, n, nu, nv, range, g)) return -2;
+    backproject_rows(g, n, nu, 0, nv, *vol, filtered, volume, (flags & 1) != 0);
+    return 0;
+}
+
+int orc_fdk_row_band(const orc_view* views, int n, int nu, int nv, float range,
+    const orc_volume* vol, int* row0, int* nrows)
+{
+    if (!valid_volume(vol) || !row0 || !nrows) return -1;
+    std::vector<Derived> g;
+    if (!derive(views, n, nu, nv, range, g)) return -2;
+    const orc_volume& V = *vol;
+    const double xs[2] = {vox_centre(0, V.nx, V.vox_x, V.center_x),
+                          vox_centre(V.nx - 1, V.nx, V.vox_x, V.center_x)};
+    const double ys[2] = {vox_centre(0, V.ny, V.vox_y, V.center_y),
+                          vox_centre(V.ny - 1, V.ny, V.vox_y, V.center_y)};
+    const double zs[2] = {vox_centre(0, V.nz, V.vox_z, V.center_z),
+                          vox_centre(V.nz - 1, V.nz, V.vox_z, V.center_z)};
+    double vmin = 1e300, vmax = -1e300;
+    for (int i = 0; i < n; ++i)
+        for (int q = 0; q < 8; ++q) {
+            double u, v, depth;
+            project_point(g[i], md(xs[q & 1], ys[(q >> 1) & 1], zs[q >> 2]), u, v, depth);
+            if (!(depth > 0.0)) return -3;  // a corner behind the source
+            vmin = std::min(vmin, v);
+            vmax = std::max(vmax, v);
+        }
+    const long lo = std::max(0L, static_cast<long>(std::floor(vmin)) - 1);
+    const long hi = std::min(static_cast<long>(nv) - 1, static_cast<long>(std::floor(vmax)) + 2);
+    if (lo > hi) { *row0 = 0; *nrows = 0; return 0; }
+    *row0 = static_cast<int>(lo);
+    *nrows = static_cast<int>(hi - lo + 1);
+    return 0;
+}
+
+int orc_fdk_rows(const orc_view* views, int n, int nu, int nv, int row0, int nrows,
+    float range, const orc_volume* vol, const orc_filter* filter, const float* proj_rows,
+    const double* row_weights, double* volume_out, int flags)
+{
+    if (!valid_volume(vol) || !filter || !proj_rows || !volume_out) return -1;
+    if (row0 < 0 || nrows <= 0 || row0 + nrows > nv) return -1;
+    std::vector<Derived> g;
+    if (!derive(views, n, nu, nv, range, g)) return -2;
+    std::vector<double> h;
+    ramp_kernel(nu, g[0].du, *filter, h);
+    std::vector<double> flt(static_cast<size_t>(n) * nu * nrows);
+    filter_rows(g, h, n, nu, row0, nrows, proj_rows, row_weights, flt.data());
+    std::fill(volume_out, volume_out + static_cast<size_t>(vol->nx) * vol->ny * vol->nz, 0.0);
+    backproject_rows(g, n, nu, row0, nrows, *vol, flt.data(), volume_out, (flags & 1) != 0);
     return 0;
 }
 

@@ -74,6 +74,10 @@ def lib():
             "orc_fdk_filter_weighted": [P, C.c_int, C.c_int, C.c_int, C.c_float, C.POINTER(Filter),
                                         P, P, P],
             "orc_parker_weights": [P, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int, P],
+            "orc_fdk_row_band": [P, C.c_int, C.c_int, C.c_int, C.c_float, C.POINTER(Volume),
+                                 C.POINTER(C.c_int), C.POINTER(C.c_int)],
+            "orc_fdk_rows": [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,
+                             C.POINTER(Volume), C.POINTER(Filter), P, P, P, C.c_int],
             "orc_fdk_fp32": [P, C.c_int, C.c_int, C.c_int, C.c_float, C.POINTER(Volume), C.POINTER(Filter), P, P],
             "orc_fdk_derived": [P, C.c_int, C.c_int, C.c_int, C.c_float, P],
             "orc_ramp_kernel": [C.c_int, C.c_double, C.POINTER(Filter), P],
@@ -198,6 +202,30 @@ def fdk_filter_weighted(views, nu, nv, scan_range, filt: Filter, proj, row_weigh
     _check(lib().orc_fdk_filter_weighted(_ptr(views), len(views), nu, nv, scan_range,
                                          C.byref(filt), _ptr(proj), _ptr(w), _ptr(out)),
            "fdk_filter_weighted")
+    return out
+
+
+def fdk_row_band(views, nu, nv, scan_range, vol: Volume):
+    """(row0, nrows): the detector rows that the volume grid's bilinear
+    footprint reads over all views, one row of margin each side."""
+    r0, nr = C.c_int(0), C.c_int(0)
+    _check(lib().orc_fdk_row_band(_ptr(views), len(views), nu, nv, scan_range, C.byref(vol),
+                                  C.byref(r0), C.byref(nr)), "fdk_row_band")
+    return r0.value, nr.value
+
+
+def fdk_rows(views, nu, nv, scan_range, vol: Volume, filt: Filter, proj_rows, row0,
+             row_weights=None, flags=0) -> np.ndarray:
+    """FDK of a grid whose footprint lies in detector rows [row0, row0 +
+    len(proj_rows[0])) of the full nu x nv detector; proj_rows holds only
+    those rows.  Equal to fdk() on the full projections for such a grid."""
+    proj_rows = np.ascontiguousarray(proj_rows, dtype=np.float32)
+    nrows = proj_rows.shape[1]
+    w = None if row_weights is None else np.ascontiguousarray(row_weights, dtype=np.float64)
+    out = np.zeros((vol.nz, vol.ny, vol.nx), dtype=np.float64)
+    _check(lib().orc_fdk_rows(_ptr(views), len(views), nu, nv, row0, nrows, scan_range,
+                              C.byref(vol), C.byref(filt), _ptr(proj_rows),
+                              _ptr(w) if w is not None else None, _ptr(out), flags), "fdk_rows")
     return out
 
 

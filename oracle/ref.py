@@ -36,14 +36,14 @@ def _fp(a):
     return a.ctypes.data_as(C.POINTER(C.c_float))
 
 
-def _child(op, scan_kw, grid_kw, filt_kw, paths, opts, q):
+def _child(op, scan_kw, grid_kw, filt_kw, paths, out_dir, opts, q):
     # the reference library logs to stdout; keep the caller's stdout for its
     # own output (the benchmark's single JSON line)
     sys.stdout.flush()
     os.dup2(2, 1)
     try:
         from fdk_cuda_impl_b200.geometry import CircularScan, RampFilter, VolumeGrid
-        arrays = [np.load(p, mmap_mode="r") for p in paths]
+        arrays = [np.load(p) for p in paths]
         scan = CircularScan(**scan_kw)
         grid = VolumeGrid(**grid_kw)
         lib = _load()
@@ -80,9 +80,11 @@ def _child(op, scan_kw, grid_kw, filt_kw, paths, opts, q):
             f = RampFilter(**filt_kw).struct()
             proj = np.ascontiguousarray(arrays[0], dtype=np.float32)
             ms = (C.c_float * 2)()
+            out = np.zeros(grid.shape, dtype=np.float32)
             rc = lib.ykref_fdk_time(C.byref(s), C.byref(v), C.byref(f), _fp(proj),
-                                    C.c_int(opts["warmup"]), C.c_int(opts["reps"]), ms, dev)
-            res = (ms[0], ms[1])
+                                    C.c_int(opts["warmup"]), C.c_int(opts["reps"]), ms, _fp(out),
+                                    dev)
+            res = (ms[0], ms[1], out)
         else:
             x = np.ascontiguousarray(arrays[0], dtype=np.float32)
             out = np.zeros(nproj if op in ("fp", "siddon_fp") else grid.shape, dtype=np.float32)
@@ -96,9 +98,28 @@ def _child(op, scan_kw, grid_kw, filt_kw, paths, opts, q):
         if rc != 0:
             q.put(("error", lib.ykref_last_error().decode()))
         else:
-            q.put(("ok", res))
+            q.put(("ok", _to_files(res, out_dir)))
     except Exception as e:  # reported to the parent
         q.put(("error", repr(e)))
+
+
+def _to_files(res, out_dir):
+    """Arrays of a result travel back as .npy files (they can be GBs)."""
+    if isinstance(res, np.ndarray):
+        path = os.path.join(out_dir, f"out{len(os.listdir(out_dir))}.npy")
+        np.save(path, res)
+        return ("npy", path)
+    if isinstance(res, tuple):
+        return tuple(_to_files(r, out_dir) for r in res)
+    return res
+
+
+def _from_files(res):
+    if isinstance(res, tuple) and len(res) == 2 and res[0] == "npy":
+        return np.load(res[1])
+    if isinstance(res, tuple):
+        return tuple(_from_files(r) for r in res)
+    return res
 
 
 def _run(op, scan, grid, filt, arrays, **opts):
@@ -117,13 +138,17 @@ def _run(op, scan, grid, filt, arrays, **opts):
         ctx = mp.get_context("spawn")
         q = ctx.Queue()
         filt_kw = dataclasses.asdict(filt) if filt is not None else None
+        out_dir = os.path.join(tmp, "out")
+        os.makedirs(out_dir)
         p = ctx.Process(target=_child, args=(op, dataclasses.asdict(scan), dataclasses.asdict(grid),
-                                             filt_kw, paths, opts, q))
+                                             filt_kw, paths, out_dir, opts, q))
         p.start()
         try:
             status, res = q.get(timeout=opts.get("timeout", 900))
         finally:
             p.join(timeout=60)
+        if status == "ok":
+            res = _from_files(res)
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
     if status != "ok":
@@ -143,7 +168,9 @@ def fdk_stages(scan, grid, filt, proj):
 
 
 def fdk_time(scan, grid, filt, proj, warmup=2, reps=5, timeout=900):
-    """(device-resident ms, host-input ms) per full FDK sequence."""
+    """(device-resident ms, host-input ms, volume) per full FDK sequence: host
+    projections and volume in pinned memory; the volume is the last
+    device-resident run's."""
     return _run("fdk_time", scan, grid, filt, [proj], warmup=warmup, reps=reps, timeout=timeout)
 
 

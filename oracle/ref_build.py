@@ -15,6 +15,7 @@ src/FlatFpBp/BP/kernels/YkFlatJosephBpLaunch.cuh:4 includes
 reference was developed on a case-insensitive file system.
 
 Usage: python oracle/ref_build.py [--reference DIR] [-j N]
+The reference tree is DIR, else $YKB_REFERENCE_DIR, else /root/reference.
 Exits 0 without building when the reference tree is absent.
 """
 from __future__ import annotations
@@ -29,7 +30,12 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 OUT = os.path.join(HERE, "_ref")
-DEFAULT_REFERENCE = "/root/reference"
+DEFAULT_REFERENCE = os.environ.get("YKB_REFERENCE_DIR", "/root/reference")
+
+
+def reference_present(reference: str = DEFAULT_REFERENCE) -> bool:
+    return os.path.isdir(os.path.join(reference, "src"))
+
 
 # translation units of the FDK pipeline, the flat FP/BP operators and the
 # iterative vector kernels their CGLS uses
@@ -81,7 +87,7 @@ def _compile(src: str, obj: str, inc: list[str]) -> tuple[str, int, str]:
 
 
 def build(reference: str = DEFAULT_REFERENCE, jobs: int = 8) -> str | None:
-    if not os.path.isdir(os.path.join(reference, "src")):
+    if not reference_present(reference):
         print(f"reference tree not found at {reference}; oracle/_ref not built")
         return None
     objdir = os.path.join(OUT, "obj")

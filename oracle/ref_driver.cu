@@ -25,6 +25,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
+#include <cstring>
 #include <string>
 #include <vector>
 
@@ -192,11 +193,15 @@ __attribute__((visibility("default"))) int ykref_fdk_stages(const ykb_circular_f
 // Times the reference FDK pipeline over `reps` full sequences after `warmup`.
 // ms[0]: device-resident projections (DeviceToDevice chunk uploads inside the
 // pipeline), volume on the device.  ms[1]: host projections, as the Session
-// requires (src/interface/YkSession.cpp:702-707), plus the volume read back.
-// Both are CUDA-event times on the pipeline's stream, averaged per sequence.
+// requires (src/interface/YkSession.cpp:702-707), plus the volume read back
+// to the host.  The host projections and volume live in pinned memory
+// (cudaMallocHost; the input is copied there before timing), the same kind
+// of host memory the timed end-to-end path of libykb gets.  Both are
+// CUDA-event times on the pipeline's stream, averaged per sequence.
+// h_vol_out (optional) receives the volume of the last device-resident run.
 __attribute__((visibility("default"))) int ykref_fdk_time(const ykb_circular_flat* scan,
     const ykb_volume* volume, const ykb_filter* filter, const float* h_proj, int warmup, int reps,
-    float* ms, int device)
+    float* ms, float* h_vol_out, int device)
 {
     if (!scan || !volume || !filter || !h_proj || !ms || reps <= 0) return fail("bad argument");
     if (cudaSetDevice(device) != cudaSuccess) return fail("cudaSetDevice");
@@ -209,8 +214,14 @@ __attribute__((visibility("default"))) int ykref_fdk_time(const ykb_circular_fla
     const size_t nproj = size_t(scan->channels) * scan->rows * scan->total_views;
     Dev<float> d_vol(nvox), d_proj(nproj);
     if (!d_vol.p || !d_proj.p) return fail("cudaMalloc");
-    std::vector<float> h_vol(nvox);
-    if (cudaMemcpy(d_proj.p, h_proj, nproj * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess)
+    struct Pinned {
+        float* p = nullptr;
+        explicit Pinned(size_t n) { if (cudaMallocHost(&p, n * sizeof(float)) != cudaSuccess) p = nullptr; }
+        ~Pinned() { if (p) cudaFreeHost(p); }
+    } pin_proj(nproj), pin_vol(nvox);
+    if (!pin_proj.p || !pin_vol.p) return fail("cudaMallocHost");
+    std::memcpy(pin_proj.p, h_proj, nproj * sizeof(float));
+    if (cudaMemcpy(d_proj.p, pin_proj.p, nproj * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess)
         return fail("cudaMemcpy projections");
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
@@ -218,12 +229,12 @@ __attribute__((visibility("default"))) int ykref_fdk_time(const ykb_circular_fla
     auto run = [&](bool device_input) {
         fdk.reset();
         YK::FdkProjectionBatch b{};
-        b.projection = device_input ? d_proj.p : h_proj;
+        b.projection = device_input ? d_proj.p : pin_proj.p;
         b.count = scan->total_views;
         b.location = device_input ? YK::EMemoryLocation::Device : YK::EMemoryLocation::Host;
         if (!fdk.processBatch(b, d_vol.p, true)) return false;
         if (!device_input)
-            cudaMemcpyAsync(h_vol.data(), d_vol.p, nvox * sizeof(float), cudaMemcpyDeviceToHost, stream.s);
+            cudaMemcpyAsync(pin_vol.p, d_vol.p, nvox * sizeof(float), cudaMemcpyDeviceToHost, stream.s);
         return true;
     };
     for (int mode = 0; mode < 2; ++mode) {
@@ -237,6 +248,9 @@ __attribute__((visibility("default"))) int ykref_fdk_time(const ykb_circular_fla
         cudaEventRecord(e1, stream.s);
         if (cudaEventSynchronize(e1) != cudaSuccess) return fail("cudaEventSynchronize");
         ms[mode] = elapsed(e0, e1) / reps;
+        if (device_input && h_vol_out &&
+            cudaMemcpy(h_vol_out, d_vol.p, nvox * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess)
+            return fail("cudaMemcpy volume");
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

@@ -391,3 +391,33 @@ def test_fdk_parker_modes(oracle, cuda_device):
     # Auto on a full turn: no weights
     plan = FdkPlan(full.scan.views(), 96, 64, full.scan.scan_range, full.grid, parker="auto")
     plan.close()
+
+
+@pytest.mark.parametrize("withheld", [0, 5, 59])
+def test_pipeline_wait_timeout_is_reported_and_the_plan_recovers(oracle, cuda_device, withheld):
+    # The TMA backprojection bounds every pipeline wait.  The test hook makes
+    # the copy producer withhold one view and shortens the waits to 1 ms:
+    # every CTA's consumers give up on that view, its producer gives up on
+    # the stage they never release, drains the copies it issued and ends.
+    # ykb_fdk_check reports the timeout; afterwards the same plan, with the
+    # default limit restored, reproduces its earlier result bit for bit.
+    import torch
+    from fdk_cuda_impl_b200 import _lib as L
+    from fdk_cuda_impl_b200.projectors import FdkPlan
+    case = K.c1_small()
+    views = case.scan.views()
+    p = torch.from_numpy(K.projections(oracle, case, views)).cuda()
+    plan = FdkPlan(views, case.scan.channels, case.scan.rows, case.scan.scan_range, case.grid,
+                   case.filt)
+    expected = plan.execute(p).clone()
+    plan.check()
+    lib = L.load()
+    L.check(lib.ykb_fdk_test_pipeline_wait(plan._h, 1_000_000, withheld))
+    plan.execute(p)
+    with pytest.raises(L.YkbError, match="pipeline wait timed out"):
+        plan.check()
+    L.check(lib.ykb_fdk_test_pipeline_wait(plan._h, 0, -1))
+    again = plan.execute(p)
+    plan.check()
+    assert torch.equal(again, expected)
+    plan.close()

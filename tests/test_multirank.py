@@ -8,6 +8,7 @@ import pytest
 import torch.multiprocessing as mp
 
 import bench
+from fdk_cuda_impl_b200.workloads import WORKLOADS
 
 
 def _free_port() -> int:
@@ -25,7 +26,7 @@ def _rank(rank, world, port, q):
         ms = 10.0 + 5.0 * rank  # rank 1 is the slower one
         slowest = bench.max_over_ranks(ms, world, "cpu")
         dist.barrier()
-        q.put((rank, slowest, bench.job_gups(world, bench.UPDATES, slowest),
+        q.put((rank, slowest, bench.job_gups(world, WORKLOADS["c2"].updates, slowest),
                bench.object_seed(rank)))
         dist.destroy_process_group()
     except Exception as e:  # reported to the parent
@@ -48,7 +49,7 @@ def test_two_gloo_ranks_reduce_to_the_slowest():
         assert p.exitcode == 0
     for r in range(world):
         assert out[r][0] == 15.0, out
-        assert out[r][1] == pytest.approx(2 * bench.UPDATES / 15e-3 / 1e9)
+        assert out[r][1] == pytest.approx(2 * WORKLOADS["c2"].updates / 15e-3 / 1e9)
     assert out[0][2] != out[1][2]
 
 

@@ -317,3 +317,26 @@ def test_siddon_oracle_pins(oracle, case_fn):
     lhs = float((oracle.siddon_fp(views, nu, nv, vol, x) * y).sum())
     rhs = float((x * oracle.siddon_bp(views, nu, nv, vol, y)).sum())
     assert abs(lhs - rhs) <= 1e-12 * abs(lhs)
+
+
+@pytest.mark.parametrize("case_fn,slabs", [(K.c1_small, [(0.0, 4), (14.0, 6), (-20.5, 3)]),
+                                           (K.odd_case, [(0.75, 3), (4.0, 2)])])
+def test_row_band_fdk_equals_full_detector(oracle, case_fn, slabs):
+    # the oracle slabs of the full-size workloads filter and backproject only
+    # the detector rows a few slices read; the result must equal the full
+    # detector's bit for bit (the filter acts on rows alone, and the band
+    # holds every row of each voxel's bilinear footprint)
+    case = case_fn()
+    views = case.scan.views()
+    nu, nv = case.scan.channels, case.scan.rows
+    p = K.projections(oracle, case, views)
+    f = K.oracle_filter(oracle, case.filt)
+    g = case.grid
+    for zc, nz in slabs:
+        vol = oracle.volume_struct((nz, g.ny, g.nx), g.voxel_mm,
+                                   (g.center_mm[0], g.center_mm[1], zc))
+        r0, nr = oracle.fdk_row_band(views, nu, nv, case.scan.scan_range, vol)
+        assert 0 < nr < nv
+        full = oracle.fdk(views, nu, nv, case.scan.scan_range, vol, f, p)
+        band = oracle.fdk_rows(views, nu, nv, case.scan.scan_range, vol, f, p[:, r0:r0 + nr], r0)
+        assert np.array_equal(full, band)
