@@ -18,6 +18,41 @@ bool has_bytes(uint32_t actual, size_t required) { return actual >= required; }
 
 bool valid_location(EMemoryLocation l) { return l == EMemoryLocation::Host || l == EMemoryLocation::Device; }
 
+static_assert(sizeof(SConeProjGeomVec) == sizeof(ykb_cone_view), "view layout");
+
+ykb_cone_view to_view(const SConeProjGeomVec& f)
+{
+    auto c = [](const float4& v) { return ykb_float4{v.x, v.y, v.z, v.w}; };
+    return ykb_cone_view{c(f.src), c(f.detS), c(f.detU), c(f.detV), c(f.angle)};
+}
+
+// Caller frames for forward projection: finite source and detector vectors,
+// detU and detV orthogonal to 1e-5 and a finite angle (PreparedGeometry::
+// initialize, src/common/YkExecutionContext.hpp:23-38)
+bool valid_frame(const SConeProjGeomVec& f)
+{
+    for (const float4& a : {f.src, f.detS, f.detU, f.detV})
+        if (!std::isfinite(a.x) || !std::isfinite(a.y) || !std::isfinite(a.z)) return false;
+    const double uu = double(f.detU.x) * f.detU.x + double(f.detU.y) * f.detU.y + double(f.detU.z) * f.detU.z;
+    const double vv = double(f.detV.x) * f.detV.x + double(f.detV.y) * f.detV.y + double(f.detV.z) * f.detV.z;
+    const double uv = double(f.detU.x) * f.detV.x + double(f.detU.y) * f.detV.y + double(f.detU.z) * f.detV.z;
+    return uu > 0 && vv > 0 && std::abs(uv) <= 1e-5 * std::sqrt(uu * vv) && std::isfinite(f.angle.x);
+}
+
+// FDK takes caller frames only where they follow the nominal orbit: every
+// x, y, z of src, detS, detU, detV and angle within 1e-3 of the views the
+// scan builds (src/interface/YkReconstructionApi.cpp:156-167)
+bool near_nominal(const SConeProjGeomVec& f, const ykb_cone_view& v)
+{
+    const float4 a[] = {f.src, f.detS, f.detU, f.detV, f.angle};
+    const ykb_float4 b[] = {v.src, v.detS, v.detU, v.detV, v.angle};
+    for (int j = 0; j < 5; ++j)
+        if (std::abs(a[j].x - b[j].x) > 1e-3f || std::abs(a[j].y - b[j].y) > 1e-3f ||
+            std::abs(a[j].z - b[j].z) > 1e-3f)
+            return false;
+    return true;
+}
+
 // SRigidTransform::aroundEulerPoint(centre, rx, ry, rz).inverse() applied to
 // a view (include/YKCBCT/geometry/YkRigidTransform.hpp,
 // transformProjectionGeometry in YkProjectionGeometry.hpp:229-247)
@@ -89,6 +124,26 @@ public:
             return fail_(EApiErrorCode::InvalidConfig, "unsupported SSystemSpec api_version");
         const auto& g = system.geometry;
         const auto& r = system.reconstruction;
+        // caller frames: the tail counts only when struct_size covers it whole
+        // (src/interface/YkReconstructionApi.cpp:144-168)
+        const bool frame_tail = has_bytes(system.struct_size,
+            offsetof(SSystemSpec, flat_frame_count) + sizeof(system.flat_frame_count));
+        if (system.struct_size > offsetof(SSystemSpec, flat_frames) && !frame_tail)
+            return fail_(EApiErrorCode::InvalidConfig, "Truncated flat-frame tail");
+        const SConeProjGeomVec* frames = frame_tail ? system.flat_frames : nullptr;
+        const int frame_count = frame_tail ? system.flat_frame_count : 0;
+        if ((frames == nullptr) != (frame_count == 0) || frame_count < 0)
+            return fail_(EApiErrorCode::InvalidConfig, "Invalid flat-frame buffer/count");
+        if (frames) {
+            const auto p = r.pipeline;
+            if (g.detector != EDetectorKind::Flat ||
+                (g.trajectory != ETrajectoryKind::Circular && g.trajectory != ETrajectoryKind::Helical) ||
+                (p != EPipeline::ForwardProjection && p != EPipeline::SART && p != EPipeline::SIRT &&
+                 p != EPipeline::OSSART && p != EPipeline::CGLS && p != EPipeline::FDK &&
+                 p != EPipeline::WFBP))
+                return fail_(EApiErrorCode::UnsupportedCombination,
+                    "Unsupported external flat-frame algorithm");
+        }
         if (static_cast<int>(g.detector) < 0 || static_cast<int>(g.detector) > 1 ||
             static_cast<int>(g.trajectory) < 0 || static_cast<int>(g.trajectory) > 3 ||
             static_cast<int>(r.pipeline) < 0 || static_cast<int>(r.pipeline) > 11)
@@ -107,6 +162,23 @@ public:
             !std::isfinite(pose.rotation_z_rad))
             return fail_(EApiErrorCode::InvalidGeometry,
                 "Forward-projection volume rotation must contain finite radians");
+        // the reference's regularisation and statistical tails: truncation is
+        // an error; a regularisation plugin belongs to its algebraic solvers
+        // (src/interface/YkReconstructionApi.cpp:207-222,241-244)
+        if (system.struct_size > offsetof(SSystemSpec, regularization) &&
+            !has_bytes(system.struct_size,
+                offsetof(SSystemSpec, regularization) + sizeof(system.regularization)))
+            return fail_(EApiErrorCode::InvalidConfig, "SSystemSpec regularization tail is truncated");
+        if (has_bytes(system.struct_size,
+                offsetof(SSystemSpec, regularization) + sizeof(system.regularization)) &&
+            system.regularization.plugin_id && system.regularization.plugin_id[0] &&
+            std::string(system.regularization.plugin_id) != "none")
+            return fail_(EApiErrorCode::UnsupportedCombination,
+                "TV plugins currently support flat SART/SIRT/OSSART only");
+        if (system.struct_size > offsetof(SSystemSpec, statistical) &&
+            !has_bytes(system.struct_size,
+                offsetof(SSystemSpec, statistical) + sizeof(system.statistical)))
+            return fail_(EApiErrorCode::InvalidConfig, "SSystemSpec statistical tail is truncated");
         if (r.pipeline == EPipeline::ForwardProjection &&
             r.forward_projector == EForwardProjector::SeparableFootprint)
             return fail_(EApiErrorCode::UnsupportedCombination,
@@ -146,8 +218,45 @@ public:
         if (spec.total_views <= 0)
             return fail_(EApiErrorCode::InvalidGeometry, "total_views must be positive");
         views_.assign(static_cast<size_t>(spec.total_views), ykb_cone_view{});
-        if (ykb_build_circular_flat(&spec, views_.data(), spec.total_views) != YKB_OK)
+        // caller frames replace the built views: FDK only near the nominal
+        // orbit (so the orbit is built to compare), forward projection any
+        // valid frames (the reference then builds no orbit,
+        // src/common/YkExecutionContext.hpp:23-38)
+        const bool frames_only = frames && r.pipeline == EPipeline::ForwardProjection;
+        if (!frames_only && ykb_build_circular_flat(&spec, views_.data(), spec.total_views) != YKB_OK) {
+            views_.clear();
             return fail_(EApiErrorCode::InvalidGeometry, ykb_last_error());
+        }
+        float parker_start = spec.start_angle_rad;
+        int parker_direction = spec.rotation_direction;
+        if (frames) {
+            if (frame_count != spec.total_views) {
+                views_.clear();
+                return fail_(EApiErrorCode::InvalidGeometry,
+                    r.pipeline == EPipeline::FDK
+                        ? "Analytic external geometry requires matching nominal trajectory"
+                        : "flat_frame_count must equal the scan's total_views");
+            }
+            for (int i = 0; i < frame_count; ++i) {
+                if (r.pipeline == EPipeline::FDK && !near_nominal(frames[i], views_[i])) {
+                    views_.clear();
+                    return fail_(EApiErrorCode::UnsupportedCombination,
+                        "External frames do not match analytic trajectory assumptions; use "
+                        "iterative reconstruction");
+                }
+                if (!valid_frame(frames[i])) {
+                    views_.clear();
+                    return fail_(EApiErrorCode::InvalidGeometry,
+                        "external frames must be finite with orthogonal detU and detV");
+                }
+            }
+            for (int i = 0; i < frame_count; ++i) views_[i] = to_view(frames[i]);
+            // the frames' angles are the only angle source: Parker starts at
+            // the first and turns the way the first two go
+            // (src/interface/YkSession.cpp:131-139)
+            parker_start = frames[0].angle.x;
+            if (frame_count >= 2) parker_direction = frames[1].angle.x >= frames[0].angle.x ? 1 : -1;
+        }
 
         volume_ = ykb_volume{g.volume.nx, g.volume.ny, g.volume.nz, g.volume.voxel_x_mm,
             g.volume.voxel_y_mm, g.volume.voxel_z_mm, g.volume.center_mm.x, g.volume.center_mm.y,
@@ -178,7 +287,7 @@ public:
             // Parker: EParkerMode values map one to one; Auto weights short
             // scans (resolveParkerEnabled, YkSystemReconstruction.hpp:29-39)
             if (ykb_fdk_plan_create_ex(views_.data(), spec.total_views, nu_, nv_, range,
-                    spec.start_angle_rad, spec.rotation_direction, &volume_, &filt,
+                    parker_start, parker_direction, &volume_, &filt,
                     YKB_PRECISION_FP32, static_cast<int>(r.fdk.parker.mode), device_,
                     &fdk_) != YKB_OK) {
                 const std::string msg = ykb_last_error();
@@ -219,6 +328,26 @@ public:
             return fail_(EApiErrorCode::InvalidConfig, "SExecutionRequest progress tail is truncated");
         if (request.api_version != 2)
             return fail_(EApiErrorCode::InvalidConfig, "unsupported SExecutionRequest api_version");
+        // projection readers and statistical weights feed the reference's
+        // iterative pipelines only (src/interface/YkReconstructionApi.cpp:327-343)
+        if (request.struct_size > offsetof(SExecutionRequest, projection_read) &&
+            request.struct_size < offsetof(SExecutionRequest, projection_batch_mib) +
+                sizeof(request.projection_batch_mib))
+            return fail_(EApiErrorCode::InvalidConfig, "SExecutionRequest projection source tail is truncated");
+        const bool weights_tail = has_bytes(request.struct_size,
+            offsetof(SExecutionRequest, projection_weights_read_user_data) +
+                sizeof(request.projection_weights_read_user_data));
+        if (request.struct_size > offsetof(SExecutionRequest, projection_weights) && !weights_tail)
+            return fail_(EApiErrorCode::InvalidConfig, "SExecutionRequest statistical weights tail is truncated");
+        if (weights_tail && (request.projection_weights.data || request.projection_weights_read))
+            return fail_(EApiErrorCode::UnsupportedCombination,
+                "Projection W is only accepted when statistical diagonal weights are enabled");
+        const bool source_tail = has_bytes(request.struct_size,
+            offsetof(SExecutionRequest, projection_batch_mib) + sizeof(request.projection_batch_mib));
+        if (source_tail && request.projection_read)
+            return fail_(EApiErrorCode::UnsupportedCombination,
+                "Projection reader requires supported flat SART/SIRT/OSSART or TIGRE "
+                "SART/OS-SART/SIRT/TV without Nesterov/FDK initialization");
         if (!request.projection.data || !request.volume.data ||
             !valid_location(request.projection.location) || !valid_location(request.volume.location))
             return fail_(EApiErrorCode::InvalidBuffer, "null projection/volume buffer or invalid location");

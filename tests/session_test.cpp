@@ -7,8 +7,13 @@
 //   session_test streaming                      full vs 47-view batches, streaming errors
 //   session_test fdk <proj.f32> <vol.f32> ...   FDK of a projection file (parity)
 //   session_test fp  <vol.f32> <proj.f32> ...   Joseph FP of a volume file (parity)
+//   session_test fdk|fp ... <frames.bin>        the same with caller geometry
+//                                               (SSystemSpec::flat_frames)
+//   session_test frames                         caller frames equal to the orbit
+//                                               vs the orbit; request tails
 // Prints one JSON object per mode; exit code 0 when the mode's checks pass.
 #include "ykb_session.hpp"
+#include "ykb.h"
 
 #include <cmath>
 #include <cstdio>
@@ -49,6 +54,30 @@ SSystemSpec small_system(EPipeline pipeline)
     s.reconstruction.back_projector = EBackProjector::JosephV3;
     s.reconstruction.fdk.filter.type = EFdkFilter::RamLak;
     return s;
+}
+
+// the scan's own orbit as caller frames, from libykb's builder (the
+// reference's buildSystemGeometry gives the same floats)
+std::vector<SConeProjGeomVec> nominal_frames(const SSystemSpec& s)
+{
+    const auto& c = s.geometry.circular;
+    const auto& d = s.geometry.flat_detector;
+    ykb_circular_flat spec{};
+    spec.total_views = c.total_views;
+    spec.views_per_turn = c.views_per_turn;
+    spec.start_angle_rad = c.start_angle_rad;
+    spec.rotation_direction = c.rotation_direction;
+    spec.sid_mm = c.sid_mm;
+    spec.sdd_mm = c.sdd_mm;
+    spec.z_mm = c.z_mm;
+    spec.channels = d.channels;
+    spec.rows = d.rows;
+    spec.channel_size_mm = d.channel_size_mm;
+    spec.row_size_mm = d.row_size_mm;
+    std::vector<SConeProjGeomVec> out(static_cast<size_t>(c.total_views));
+    if (ykb_build_circular_flat(&spec, reinterpret_cast<ykb_cone_view*>(out.data()), c.total_views) != YKB_OK)
+        out.clear();
+    return out;
 }
 
 std::vector<float> analytic_phantom(const SVolumeGridSpec& g)
@@ -139,6 +168,59 @@ int mode_validate()
         SSystemSpec spec = small_system(EPipeline::FDK);
         spec.geometry.circular.sdd_mm = 50.f;
         expect_code("sdd", s->initialize(spec), *s, EApiErrorCode::InvalidGeometry, failures);
+    }
+    // caller-frame tail (src/interface/YkReconstructionApi.cpp:144-168)
+    std::vector<SConeProjGeomVec> orbit = nominal_frames(small_system(EPipeline::FDK));
+    {
+        SSystemSpec spec = small_system(EPipeline::FDK);
+        spec.struct_size = static_cast<uint32_t>(offsetof(SSystemSpec, flat_frames) + 4);
+        expect_code("frame_tail_truncated", s->initialize(spec), *s, EApiErrorCode::InvalidConfig, failures);
+    }
+    {
+        SSystemSpec spec = small_system(EPipeline::FDK);
+        spec.flat_frame_count = 5;
+        expect_code("frame_count_no_buffer", s->initialize(spec), *s, EApiErrorCode::InvalidConfig, failures);
+    }
+    {
+        SSystemSpec spec = small_system(EPipeline::PWLS);
+        spec.flat_frames = orbit.data();
+        spec.flat_frame_count = static_cast<int>(orbit.size());
+        expect_code("frames_pwls", s->initialize(spec), *s, EApiErrorCode::UnsupportedCombination, failures);
+    }
+    {
+        SSystemSpec spec = small_system(EPipeline::FDK);
+        spec.flat_frames = orbit.data();
+        spec.flat_frame_count = static_cast<int>(orbit.size()) - 1;
+        expect_code("fdk_frames_count", s->initialize(spec), *s, EApiErrorCode::InvalidGeometry, failures);
+    }
+    {
+        std::vector<SConeProjGeomVec> off = orbit;
+        off[7].detS.x += 0.01f;  // 10 um off the orbit, beyond the 1e-3 mm the FDK accepts
+        SSystemSpec spec = small_system(EPipeline::FDK);
+        spec.flat_frames = off.data();
+        spec.flat_frame_count = static_cast<int>(off.size());
+        expect_code("fdk_frames_off_orbit", s->initialize(spec), *s,
+            EApiErrorCode::UnsupportedCombination, failures);
+    }
+    {
+        std::vector<SConeProjGeomVec> skew = orbit;
+        skew[3].detV.x += 0.1f;  // detU and detV no longer orthogonal
+        SSystemSpec spec = small_system(EPipeline::ForwardProjection);
+        spec.flat_frames = skew.data();
+        spec.flat_frame_count = static_cast<int>(skew.size());
+        expect_code("fp_frames_skewed", s->initialize(spec), *s, EApiErrorCode::InvalidGeometry, failures);
+    }
+    {
+        SSystemSpec spec = small_system(EPipeline::FDK);
+        spec.regularization.plugin_id = "huber_tv_prox";
+        expect_code("regularization_plugin", s->initialize(spec), *s,
+            EApiErrorCode::UnsupportedCombination, failures);
+    }
+    {
+        SSystemSpec spec = small_system(EPipeline::FDK);
+        spec.struct_size = static_cast<uint32_t>(offsetof(SSystemSpec, statistical) + 4);
+        expect_code("statistical_tail_truncated", s->initialize(spec), *s,
+            EApiErrorCode::InvalidConfig, failures);
     }
     {
         std::vector<float> a(10), b(10);
@@ -272,7 +354,8 @@ void write_f32(const char* path, const std::vector<float>& v)
     std::fclose(f);
 }
 
-// fdk|fp <in> <out> views per_turn sid sdd nu nv du dv nx ny nz vox filter
+// fdk|fp <in> <out> views per_turn sid sdd nu nv du dv nx ny nz vox filter [frames]
+// frames: a file of `views` SConeProjGeomVec records passed as flat_frames
 int mode_file(bool fdk, int argc, char** argv, bool siddon = false)
 {
     if (argc < 17) return 4;
@@ -296,6 +379,12 @@ int mode_file(bool fdk, int argc, char** argv, bool siddon = false)
     const size_t pn = size_t(spec.geometry.circular.total_views) * spec.geometry.flat_detector.channels *
         spec.geometry.flat_detector.rows;
     const size_t vn = size_t(spec.geometry.volume.nx) * spec.geometry.volume.ny * spec.geometry.volume.nz;
+    std::vector<float> frame_floats;
+    if (argc > 17) {
+        frame_floats = read_f32(argv[17], size_t(spec.geometry.circular.total_views) * 20);
+        spec.flat_frames = reinterpret_cast<const SConeProjGeomVec*>(frame_floats.data());
+        spec.flat_frame_count = spec.geometry.circular.total_views;
+    }
     auto s = make_session();
     if (!s->initialize(spec)) { std::fprintf(stderr, "init: %s\n", s->lastErrorMessage()); return 2; }
     std::vector<float> proj = fdk ? read_f32(argv[2], pn) : std::vector<float>(pn);
@@ -309,6 +398,61 @@ int mode_file(bool fdk, int argc, char** argv, bool siddon = false)
     return 0;
 }
 
+// Joseph FP through caller frames equal to the scan's orbit against FP of the
+// orbit itself (max difference < 1e-5, the reference's framework/
+// external-geometry pin, Yktest/test_pipeline_smoke.cpp:2029-2075), and the
+// request tails the reference's iterative pipelines own (a projection reader
+// or statistical weights make forward projection return UnsupportedCombination)
+int mode_frames()
+{
+    SSystemSpec spec = small_system(EPipeline::ForwardProjection);
+    const auto truth = analytic_phantom(spec.geometry.volume);
+    std::vector<float> vol = truth;
+    const size_t pn = size_t(48) * 32 * 96;
+    std::vector<float> a(pn), b(pn);
+    SExecutionRequest req{};
+    req.volume = host(vol);
+    req.projection = host(a);
+    auto orbit_session = make_session();
+    if (!orbit_session->initialize(spec) || !orbit_session->execute(req)) {
+        std::fprintf(stderr, "orbit: %s\n", orbit_session->lastErrorMessage());
+        return 2;
+    }
+    const std::vector<SConeProjGeomVec> frames = nominal_frames(spec);
+    spec.flat_frames = frames.data();
+    spec.flat_frame_count = static_cast<int>(frames.size());
+    auto frame_session = make_session();
+    req.projection = host(b);
+    if (!frame_session->initialize(spec) || !frame_session->execute(req)) {
+        std::fprintf(stderr, "frames: %s\n", frame_session->lastErrorMessage());
+        return 2;
+    }
+    double max_diff = 0.0;
+    for (size_t i = 0; i < pn; ++i) max_diff = std::max(max_diff, double(std::fabs(a[i] - b[i])));
+    int failures = 0;
+    std::printf("{");
+    {
+        SExecutionRequest r = req;
+        r.projection_read = [](void*, const int*, int, float*, size_t) { return true; };
+        expect_code("projection_reader", frame_session->execute(r), *frame_session,
+            EApiErrorCode::UnsupportedCombination, failures);
+    }
+    {
+        SExecutionRequest r = req;
+        r.projection_weights = host(a);
+        expect_code("projection_weights", frame_session->execute(r), *frame_session,
+            EApiErrorCode::UnsupportedCombination, failures);
+    }
+    {
+        SExecutionRequest r = req;
+        r.struct_size = static_cast<uint32_t>(offsetof(SExecutionRequest, projection_read) + 4);
+        expect_code("source_tail_truncated", frame_session->execute(r), *frame_session,
+            EApiErrorCode::InvalidConfig, failures);
+    }
+    std::printf("\"max_diff\": %.3e, \"failures\": %d}\n", max_diff, failures);
+    return (failures == 0 && max_diff < 1e-5) ? 0 : 1;
+}
+
 } // namespace
 
 int main(int argc, char** argv)
@@ -320,6 +464,7 @@ int main(int argc, char** argv)
     if (mode == "fdk") return mode_file(true, argc, argv);
     if (mode == "fp") return mode_file(false, argc, argv);
     if (mode == "fp_auto") return mode_file(false, argc, argv, true);
-    std::fprintf(stderr, "usage: session_test validate|roundtrip|streaming|fdk|fp|fp_auto ...\n");
+    if (mode == "frames") return mode_frames();
+    std::fprintf(stderr, "usage: session_test validate|roundtrip|streaming|frames|fdk|fp|fp_auto ...\n");
     return 4;
 }
