@@ -86,6 +86,9 @@ SIGNATURES = {
     "ykb_fdk_workspace_bytes": (C.c_size_t, [_P]),
     "ykb_fdk_check": (C.c_int, [_P, _P]),
     "ykb_fdk_test_pipeline_wait": (C.c_int, [_P, C.c_ulonglong, C.c_int]),
+    "ykb_fdk_stage_timing": (C.c_int, [_P, C.c_int]),
+    "ykb_fdk_stage_times": (C.c_int, [_P, _P, C.POINTER(C.c_double), C.POINTER(C.c_int),
+                                      C.POINTER(C.c_double), C.POINTER(C.c_int)]),
     "ykb_fdk_filter_static": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_float, C.POINTER(Filter),
                                         _P, C.c_int, _P, _P]),
     "ykb_joseph_plan_create": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.POINTER(Volume),

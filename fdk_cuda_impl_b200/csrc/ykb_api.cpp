@@ -310,9 +310,35 @@ ykb_status check_range(const ykb_fdk_plan* p, const void* buf, int dtype, int vi
 
 size_t dtype_bytes(int dtype) { return dtype == YKB_DTYPE_BF16 ? 2 : 4; }
 
+// Stage timing: the index of the event pair recorded around a stage's launch
+// group, or -1 when the plan does not time its stages (or its pool of 4096
+// pairs is full until the next ykb_fdk_stage_times)
+int stage_begin(ykb_fdk_plan* p, int stage, cudaStream_t s)
+{
+    if (!p->timing || p->stage_events_used >= 4096) return -1;
+    if (p->stage_events_used == p->stage_events.size()) {
+        ykb_fdk_plan::StageEvents e;
+        if (cudaEventCreate(&e.start) != cudaSuccess || cudaEventCreate(&e.stop) != cudaSuccess) {
+            if (e.start) cudaEventDestroy(e.start);
+            cudaGetLastError();
+            return -1;
+        }
+        p->stage_events.push_back(e);
+    }
+    ykb_fdk_plan::StageEvents& e = p->stage_events[p->stage_events_used];
+    e.stage = stage;
+    if (cudaEventRecord(e.start, s) != cudaSuccess) return -1;
+    return static_cast<int>(p->stage_events_used++);
+}
+
+void stage_end(ykb_fdk_plan* p, int i, cudaStream_t s)
+{
+    if (i >= 0) cudaEventRecord(p->stage_events[static_cast<size_t>(i)].stop, s);
+}
+
 // preweight + ramp for views [first, first+count) of the plan, input rows at
 // proj, output into dst (FilteredLayout `layout`, row pitch ldc elements)
-ykb_status filter_chunk(ykb_fdk_plan* p, const void* proj, int proj_dtype, int first, int count,
+ykb_status filter_chunk_(ykb_fdk_plan* p, const void* proj, int proj_dtype, int first, int count,
     float* dst, int layout, int ldc, cudaStream_t s)
 {
     const FdkPreweightView* pwv = p->pwv.as<FdkPreweightView>() + first;
@@ -339,13 +365,22 @@ ykb_status filter_chunk(ykb_fdk_plan* p, const void* proj, int proj_dtype, int f
     return YKB_OK;
 }
 
+ykb_status filter_chunk(ykb_fdk_plan* p, const void* proj, int proj_dtype, int first, int count,
+    float* dst, int layout, int ldc, cudaStream_t s)
+{
+    const int ev = stage_begin(p, 0, s);
+    const ykb_status st = filter_chunk_(p, proj, proj_dtype, first, count, dst, layout, ldc, s);
+    stage_end(p, ev, s);
+    return st;
+}
+
 // weighted backprojection of `count` filtered views (FilteredLayout
 // `layout`, row pitch ld elements) starting at plan view `first`
 // z_begin/z_count restrict the work to volume slices [z_begin, z_begin +
 // z_count) (z_count < 0: all); z_begin must be a multiple of fdk_tma_z_tile()
 // of the TMA backprojection, so that its tiles are those of the box pre-pass
-ykb_status backproject_chunk(ykb_fdk_plan* p, const void* filtered, int layout, int ld, int first,
-    int count, float* vol, int accumulate, cudaStream_t s, int z_begin = 0, int z_count = -1)
+ykb_status backproject_chunk_(ykb_fdk_plan* p, const void* filtered, int layout, int ld, int first,
+    int count, float* vol, int accumulate, cudaStream_t s, int z_begin, int z_count)
 {
     VolumeGrid grid = make_grid(p->volume);
     if (z_count >= 0) {
@@ -368,6 +403,16 @@ ykb_status backproject_chunk(ykb_fdk_plan* p, const void* filtered, int layout, 
             ld, grid, p->axial, vol, accumulate, s));
     }
     return YKB_OK;
+}
+
+ykb_status backproject_chunk(ykb_fdk_plan* p, const void* filtered, int layout, int ld, int first,
+    int count, float* vol, int accumulate, cudaStream_t s, int z_begin = 0, int z_count = -1)
+{
+    const int ev = stage_begin(p, 1, s);
+    const ykb_status st = backproject_chunk_(p, filtered, layout, ld, first, count, vol,
+        accumulate, s, z_begin, z_count);
+    stage_end(p, ev, s);
+    return st;
 }
 
 // Host projections streamed through the plan, copied on the plan's copy
@@ -557,6 +602,41 @@ YKB_API ykb_status ykb_fdk_execute_host_out(ykb_fdk_plan* p, const void* h_proj,
     DeviceGuard guard(p->device);
     return stream_host(p, h_proj, proj_dtype, view_offset, n_views, d_volume, h_volume,
         clear_output, reinterpret_cast<cudaStream_t>(stream));
+}
+
+YKB_API ykb_status ykb_fdk_stage_timing(ykb_fdk_plan* p, int enable)
+{
+    clear_error();
+    if (!p) return fail(YKB_ERR_INVALID_BUFFER, "null plan");
+    p->timing = enable != 0;
+    p->stage_events_used = 0;
+    return YKB_OK;
+}
+
+YKB_API ykb_status ykb_fdk_stage_times(ykb_fdk_plan* p, ykb_stream stream, double* filter_ms,
+    int* filter_groups, double* backproject_ms, int* backproject_groups)
+{
+    clear_error();
+    if (!p || !filter_ms || !filter_groups || !backproject_ms || !backproject_groups)
+        return fail(YKB_ERR_INVALID_BUFFER, "null plan or output");
+    DeviceGuard guard(p->device);
+    YKB_TRY_CUDA(cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(stream)));
+    double ms[2] = {0.0, 0.0};
+    int groups[2] = {0, 0};
+    for (size_t i = 0; i < p->stage_events_used; ++i) {
+        const auto& e = p->stage_events[i];
+        YKB_TRY_CUDA(cudaEventSynchronize(e.stop));
+        float t = 0.f;
+        YKB_TRY_CUDA(cudaEventElapsedTime(&t, e.start, e.stop));
+        ms[e.stage] += t;
+        ++groups[e.stage];
+    }
+    p->stage_events_used = 0;
+    *filter_ms = ms[0];
+    *filter_groups = groups[0];
+    *backproject_ms = ms[1];
+    *backproject_groups = groups[1];
+    return YKB_OK;
 }
 
 YKB_API ykb_status ykb_fdk_test_pipeline_wait(ykb_fdk_plan* p, unsigned long long wait_ns,

@@ -294,6 +294,13 @@ struct ykb_fdk_plan {
     ykb::DeviceBuffer work_a;    // preweighted rows: float, or the bf16 split parts in turn
     ykb::DeviceBuffer work_filtered;  // filtered projections (layout, pitch ld)
     ykb::DeviceBuffer err_flag;  // int[4]: device error word, box pre-pass scratch
+    // stage timing (ykb_fdk_stage_timing): a start and a stop event around
+    // each filter (stage 0) and backprojection (stage 1) launch group, on the
+    // stream that launches it; events are pooled and reused
+    struct StageEvents { cudaEvent_t start = nullptr, stop = nullptr; int stage = 0; };
+    bool timing = false;
+    std::vector<StageEvents> stage_events;
+    size_t stage_events_used = 0;
     // host-input streaming (ykb_fdk_execute_host), created on first use
     ykb::DeviceBuffer stage_in;  // two batches of input views
     int stage_views = 0;         // views per batch slot
@@ -302,6 +309,10 @@ struct ykb_fdk_plan {
     cudaEvent_t consumed[2] = {nullptr, nullptr};  // batch slot read by the filter
     ~ykb_fdk_plan()
     {
+        for (auto& e : stage_events) {
+            if (e.start) cudaEventDestroy(e.start);
+            if (e.stop) cudaEventDestroy(e.stop);
+        }
         for (cudaEvent_t e : copied) if (e) cudaEventDestroy(e);
         for (cudaEvent_t e : consumed) if (e) cudaEventDestroy(e);
         if (copy_stream) cudaStreamDestroy(copy_stream);

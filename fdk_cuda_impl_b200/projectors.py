@@ -83,6 +83,21 @@ class FdkPlan:
         """Synchronises the current stream and raises on a device-side error."""
         L.check(self.lib.ykb_fdk_check(self._h, _stream_handle(self.device)))
 
+    def stage_timing(self, enable: bool = True) -> None:
+        """Records CUDA events around each filter and backprojection launch
+        group of later calls (ykb_fdk_stage_timing)."""
+        L.check(self.lib.ykb_fdk_stage_timing(self._h, 1 if enable else 0))
+
+    def stage_times(self) -> dict:
+        """Summed device times (ms) and launch-group counts of each stage since
+        the last call; synchronises the current stream."""
+        fm, bm = C.c_double(0.0), C.c_double(0.0)
+        fg, bg = C.c_int(0), C.c_int(0)
+        L.check(self.lib.ykb_fdk_stage_times(self._h, _stream_handle(self.device), C.byref(fm),
+                                             C.byref(fg), C.byref(bm), C.byref(bg)))
+        return {"filter_ms": fm.value, "filter_groups": fg.value,
+                "backproject_ms": bm.value, "backproject_groups": bg.value}
+
     def _vol_out(self, volume):
         if volume is None:
             return torch.empty(self.grid.shape, dtype=torch.float32, device=f"cuda:{self.device}")

@@ -227,6 +227,19 @@ YKB_API size_t ykb_fdk_workspace_bytes(const ykb_fdk_plan* plan);
  * equivalent: it aborts the process on CUDA errors (src/global/YkMacro.hpp:35-41). */
 YKB_API ykb_status ykb_fdk_check(ykb_fdk_plan* plan, ykb_stream stream);
 
+/* Stage timing: while enabled, the plan records a CUDA event pair around
+ * each filter launch group (cosine preweight + ramp filter of one workspace
+ * chunk) and each backprojection launch group, on the stream that launches
+ * it.  ykb_fdk_stage_times synchronises `stream`, returns the summed event
+ * times (ms) and group counts of each stage since the last call (or since
+ * timing was enabled) and starts a new tally.  For measurement: the stages'
+ * own device times inside a full execute.  No counterpart in the
+ * reference. */
+YKB_API ykb_status ykb_fdk_stage_timing(ykb_fdk_plan* plan, int enable);
+YKB_API ykb_status ykb_fdk_stage_times(ykb_fdk_plan* plan, ykb_stream stream,
+    double* filter_ms, int* filter_groups, double* backproject_ms,
+    int* backproject_groups);
+
 /* Test hook for the timeout path of the TMA backprojection: sets the limit
  * of its pipeline waits to wait_ns (0 restores the default, about 2 s) and,
  * when withheld_view >= 0, makes the copy producer skip that view (an index
