@@ -251,6 +251,7 @@ __device__ __forceinline__ Box box_from_range(double umin, double umax, double v
 
 struct TileGeom {
     double x0, x1, y0, y1, z0, z1;
+    double xc, yc;  // centre of the nominal 16x16 tile (reference point of its column terms)
 };
 
 __device__ __forceinline__ TileGeom tile_geom(const VolumeGrid& g, int bx, int by, int za, int zc)
@@ -263,6 +264,8 @@ __device__ __forceinline__ TileGeom tile_geom(const VolumeGrid& g, int bx, int b
     t.y1 = g.oy + min(ya + TY - 1, g.ny - 1) * g.vy;
     t.z0 = g.oz + za * g.vz;
     t.z1 = g.oz + (za + zc - 1) * g.vz;  // all zc slices are evaluated
+    t.xc = g.ox + (xa + 0.5 * (TX - 1)) * g.vx;
+    t.yc = g.oy + (ya + 0.5 * (TY - 1)) * g.vy;
     return t;
 }
 
@@ -296,6 +299,60 @@ __global__ void box_extent_kernel(const FdkViewCoef* __restrict__ coef, int n_vi
     atomicMax(out + 1, h);
 }
 
+// Per-(tile, view) terms of the FDK axial path, FP64-derived by the producer
+// and stored beside the view's stage; each consumer evaluates its column's
+// terms from them in FP32.  With d = (X - xc, Y - yc) the column's offset
+// from the tile centre and P = (X, Y, z0) its first voxel:
+//   den = dc + gd . d                      (cd . P)
+//   u   = uc + (hu . d) / den              hu = (cu_x, cu_y) - u_c (cd_x, cd_y)
+//   vq  = vc + (hv . d) / den              hv = (cv_x, cv_y) - v_c (cd_x, cd_y)
+//   vs  = kz / den                         kz = cv_z vz, one slice up
+//   w   = wbase / dep^2,  dep = pc + gp . d (cr . P)
+// exact rewrites of u = cu.P / cd.P and v = cv.P / cd.P about the tile
+// centre (the numerators of u - u_c and v - v_c vanish there).  u and vq are
+// relative to the staged box (pixel c0; row r0, minus the 1/2 of the row
+// rounding), so they stay below the box size and round to within 4e-6 px.
+struct alignas(16) TileTerms {
+    float uc, hu0, hu1, vc;
+    float hv0, hv1, dc, gd0;
+    float gd1, kz, pc, gp0;
+    float gp1, wbase, unused0, unused1;
+};
+
+__device__ __forceinline__ TileTerms tile_terms(const FdkViewCoef& c, const TileGeom& tg,
+    double vz, int c0, int r0)
+{
+    const double den = fma(c.cd[1], tg.yc, fma(c.cd[0], tg.xc, c.cd[3]));
+    const double rd = 1.0 / den;
+    const double uc = fma(c.cu[1], tg.yc, fma(c.cu[0], tg.xc, c.cu[3])) * rd;
+    const double vc = fma(c.cv[2], tg.z0, fma(c.cv[1], tg.yc, fma(c.cv[0], tg.xc, c.cv[3]))) * rd;
+    const double dep = fma(c.cr[1], tg.yc, fma(c.cr[0], tg.xc, c.cr[3]));
+    TileTerms t;
+    t.uc = static_cast<float>(uc - c0);
+    t.hu0 = static_cast<float>(c.cu[0] - uc * c.cd[0]);
+    t.hu1 = static_cast<float>(c.cu[1] - uc * c.cd[1]);
+    t.vc = static_cast<float>(vc - r0 - 0.5);
+    t.hv0 = static_cast<float>(c.cv[0] - vc * c.cd[0]);
+    t.hv1 = static_cast<float>(c.cv[1] - vc * c.cd[1]);
+    t.dc = static_cast<float>(den);
+    t.gd0 = static_cast<float>(c.cd[0]);
+    t.gd1 = static_cast<float>(c.cd[1]);
+    t.kz = static_cast<float>(c.cv[2] * vz);
+    t.pc = static_cast<float>(dep);
+    t.gp0 = static_cast<float>(c.cr[0]);
+    t.gp1 = static_cast<float>(c.cr[1]);
+    t.wbase = static_cast<float>(c.wbase);
+    t.unused0 = t.unused1 = 0.f;
+    return t;
+}
+
+__device__ __forceinline__ float rcp_approx(float x)
+{
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 // Shared-memory ring budget of one CTA; two CTAs share an SM.
 constexpr size_t kRingBudget = 108 * 1024;
 
@@ -318,7 +375,10 @@ __device__ __forceinline__ void bp_tile(const CUtensorMap& map,
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + ring_bytes);
     uint64_t* empty = full + stages;
     int4* boxes = reinterpret_cast<int4*>(empty + stages);
-    int* abort_ptr = reinterpret_cast<int*>(boxes + stages);
+    // FDK axial tap-pair path: the producer's tile terms of each stage's view
+    constexpr bool COLS = AXIAL && PAIR && !PSEUDO;
+    TileTerms* terms = reinterpret_cast<TileTerms*>(boxes + stages);
+    int* abort_ptr = reinterpret_cast<int*>(terms + stages);
     int& abort_flag = *abort_ptr;
 
     const int tid = threadIdx.x;
@@ -380,6 +440,7 @@ __device__ __forceinline__ void bp_tile(const CUtensorMap& map,
                     aligned = 0;  // never issue a copy the hardware would reject
                 } else {
                     boxes[s] = make_int4(b.c0, b.r0, b.c1, b.r1);
+                    if constexpr (COLS) terms[s] = tile_terms(coef[k], tg, g.vz, b.c0, b.r0);
                     mbar_arrive_expect_tx(&full[s], box_bytes);
                     tma_load_3d(dst, &map, &full[s], b.c0 + (PAIR ? kPairLead : 0), b.r0, k);
                 }
@@ -419,7 +480,14 @@ __device__ __forceinline__ void bp_tile(const CUtensorMap& map,
     for (int i = 0; i < ZC; ++i) acc[i] = 0.f;
     bool bad = false;
     ColTerms cur{};
-    if (AXIAL) cur = axial_terms<PSEUDO>(coef[0], pseudo, X, Y, Z0, g.vz);
+    if (AXIAL && !COLS) cur = axial_terms<PSEUDO>(coef[0], pseudo, X, Y, Z0, g.vz);
+    // the column's offset from the tile centre (exact: a few voxel pitches)
+    float dx = 0.f, dy = 0.f;
+    if constexpr (COLS) {
+        const TileGeom tg = tile_geom(g, blockIdx.x, blockIdx.y, za, ZC);
+        dx = static_cast<float>(X - tg.xc);
+        dy = static_cast<float>(Y - tg.yc);
+    }
 
     int s = 0;
     uint32_t phase = 0;
@@ -433,8 +501,68 @@ __device__ __forceinline__ void bp_tile(const CUtensorMap& map,
             }
             return;
         }
-        const int4 b = boxes[s];
         const float* S = ring + static_cast<size_t>(s) * stage_floats;
+        if constexpr (COLS) {
+            // the column's terms in FP32 from the tile terms of this view
+            const TileTerms& T = terms[s];
+            const float4 t0 = *reinterpret_cast<const float4*>(&T.uc);
+            const float4 t1 = *reinterpret_cast<const float4*>(&T.hv0);
+            const float4 t2 = *reinterpret_cast<const float4*>(&T.gd1);
+            const float2 t3 = *reinterpret_cast<const float2*>(&T.gp1);
+            const float den = fmaf(t2.x, dy, fmaf(t1.w, dx, t1.z));
+            float rd = rcp_approx(den);
+            rd = fmaf(rd, fmaf(-den, rd, 1.f), rd);  // one Newton step: vs walks 48 slices
+            float u = fmaf(fmaf(t0.z, dy, t0.y * dx), rd, t0.x);
+            float vbq = fmaf(fmaf(t1.y, dy, t1.x * dx), rd, t0.w);
+            float vs = t2.y * rd;
+            const float dep = fmaf(t3.x, dy, fmaf(t2.w, dx, t2.z));
+            const float rp = rcp_approx(dep);
+            float w = t3.y * rp * rp;
+            const float fu = floorf(u);
+            int col = static_cast<int>(fu);
+            float au = u - fu;
+            // rows of the column's end points (the rounding map is monotonic)
+            const int na = static_cast<int>(__float_as_uint(vbq + kRoundMagic) - kRoundMagicBits);
+            const int nb = static_cast<int>(__float_as_uint(fmaf(static_cast<float>(ZC - 1), vs, vbq) +
+                kRoundMagic) - kRoundMagicBits);
+            // every tap inside the staged BW x BH box (it holds the detector's
+            // values, zero outside the detector); |v| < 2^21 keeps the
+            // rounding word exact
+            const bool inside = fabsf(u) < 1e6f && fabsf(vbq) < 1e6f && fabsf(vs) < 3e4f &&
+                w < 1e30f && col >= 0 && col <= BW - 1 && min(na, nb) >= 0 && max(na, nb) <= BH - 2;
+            if (!active || !inside) {
+                if (active) bad = true;
+                // no contribution; every read stays at the stage origin
+                w = 0.f; au = 0.f; vs = 0.f; vbq = 0.f;
+                col = 0;
+            }
+            const uint32_t base = smem_addr(S) + 8u * static_cast<uint32_t>(col) -
+                8u * BW * kRoundMagicBits;
+            const float w1 = w * au, w0 = w - w1;
+            const f2 M2 = f2pack(kRoundMagic, kRoundMagic), H2 = f2pack(0.5f, 0.5f);
+#pragma unroll
+            for (int j = 0; j < ZC / 2; ++j) {
+                const f2 vq = f2pack(fmaf(2.f * j, vs, vbq), fmaf(2.f * j + 1.f, vs, vbq));
+                const f2 t = f2add(vq, M2);
+                const f2 fr = f2add(f2sub(vq, f2sub(t, M2)), H2);
+                float t0f, t1f, f0, f1;
+                f2unpack(t, t0f, t1f);
+                f2unpack(fr, f0, f1);
+                const uint32_t a0 = __float_as_uint(t0f) * (8u * BW) + base;
+                const uint32_t a1 = __float_as_uint(t1f) * (8u * BW) + base;
+                const f2 A0 = lds2<0>(a0), B0 = lds2<8 * BW>(a0);
+                const f2 A1 = lds2<0>(a1), B1 = lds2<8 * BW>(a1);
+                float l0, r0, l1, r1;
+                f2unpack(f2fma(f2pack(f0, f0), f2sub(B0, A0), A0), l0, r0);
+                f2unpack(f2fma(f2pack(f1, f1), f2sub(B1, A1), A1), l1, r1);
+                acc[2 * j] = fmaf(w1, r0, fmaf(w0, l0, acc[2 * j]));
+                acc[2 * j + 1] = fmaf(w1, r1, fmaf(w0, l1, acc[2 * j + 1]));
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[s]);
+            continue;
+        }
+        const int4 b = boxes[s];
         const FdkViewCoef& c = coef[k];
         if (AXIAL) {
             // next view's terms first: independent of this view's stage
@@ -784,7 +912,8 @@ cudaError_t launch_fdk_backproject_tma(const float* filtered, int layout, int ld
     const int stages = fdk_tma_stages(bw, bh, layout);
     if (stages == 0) return cudaErrorInvalidConfiguration;
     const size_t ring = static_cast<size_t>(stage_stride_floats(bw, bh, pair)) * sizeof(float) * stages;
-    const size_t smem = 128 + ring + 2 * stages * sizeof(uint64_t) + stages * sizeof(int4) + 16;
+    const size_t smem = 128 + ring + 2 * stages * sizeof(uint64_t) +
+        stages * (sizeof(int4) + sizeof(TileTerms)) + 16;
     return pair ? launch_layout<true>(map, coef, n_views, g, bw, bh, stages, smem, axial, vol,
                       accumulate, err, pseudo, pw, s)
                 : launch_layout<false>(map, coef, n_views, g, bw, bh, stages, smem, axial, vol,

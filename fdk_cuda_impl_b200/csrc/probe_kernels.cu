@@ -5,9 +5,11 @@
 // Every CTA fills 16 KB of shared memory and its 256 threads stream it back
 // with vector loads: lane i reads the WORDS 32-bit words at word offset
 // WORDS * i of a row of 256 * WORDS words, so the 32 lanes of a warp cover
-// consecutive banks (no conflicts).  Loads are volatile (never hoisted or
-// merged) and XOR-folded into registers that a never-taken store keeps
-// alive.  Four CTAs per SM keep enough warps in flight to saturate the pipe.
+// consecutive banks (no conflicts).  The loaded words are XOR-folded into
+// registers that a never-taken store keeps
+// alive; volatile shared loads are never hoisted out of the loop or merged
+// (the loaded words do not change, so plain loads would be).  Four CTAs per
+// SM keep enough warps in flight to saturate the pipe.
 #include "ykb_internal.hpp"
 
 #include <algorithm>
@@ -28,11 +30,11 @@ __device__ __forceinline__ void probe_load(uint32_t addr, uint32_t& a, uint32_t&
 {
     if constexpr (WORDS == 2) {
         uint32_t x, y;
-        asm volatile("ld.shared.v2.u32 {%0, %1}, [%2+%3];" : "=r"(x), "=r"(y) : "r"(addr), "n"(OFF));
+        asm volatile("ld.volatile.shared.v2.u32 {%0, %1}, [%2+%3];" : "=r"(x), "=r"(y) : "r"(addr), "n"(OFF));
         a ^= x; b ^= y;
     } else {
         uint32_t x, y, z, w;
-        asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4+%5];"
+        asm volatile("ld.volatile.shared.v4.u32 {%0, %1, %2, %3}, [%4+%5];"
             : "=r"(x), "=r"(y), "=r"(z), "=r"(w) : "r"(addr), "n"(OFF));
         a ^= x ^ z; b ^= y ^ w;
     }
