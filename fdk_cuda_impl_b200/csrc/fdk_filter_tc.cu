@@ -12,20 +12,27 @@
 //   NSEG 6 (FP32 plans): A0 T0 + A0 T1 + A1 T0 + A0 T2 + A1 T1 + A2 T0, the
 //     24 bits of FP32 (the dropped products are below 2^-24 of the result).
 //
-// CTA = 128 output rows x TN output columns, 4 warps:
+// Persistent CTAs, one per SM, walk the output tiles (128 rows x TN
+// columns) with six warps:
 //   warp 0 lane 0 : TMA producer (A and T tiles, 128-byte swizzle, this
-//                   GPU's memory only, no multicast) into a 4-stage ring;
-//   warp 1 lane 0 : MMA issuer (tcgen05.mma kind::f16, M=128, N=TN, K=16),
-//                   releases stages with tcgen05.commit;
-//   all 4 warps   : epilogue, tcgen05.ld of their 32 TMEM lanes, placement
-//                   mask, FP32 store.
+//                   GPU's memory only, no multicast) into a 4-stage ring,
+//                   running ahead across tile boundaries;
+//   warp 1 lane 0 : MMA issuer (tcgen05.mma kind::f16, M=128, N=TN, K=16)
+//                   into one of two TMEM accumulators, releases stages with
+//                   tcgen05.commit; warp 1 also owns the TMEM allocation;
+//   warps 2-5     : epilogue of the other accumulator, overlapping the next
+//                   tile's MMAs: tcgen05.ld of their 32 TMEM lanes, the
+//                   placement mask, a transpose through shared memory so that
+//                   each global store writes one row's 16 (or 32 tap-pair)
+//                   consecutive floats.
 // Every mbarrier wait is bounded; on a timeout the CTA records an error,
-// drains what it issued and frees its TMEM.
+// drains what it issued, waits for its MMAs to retire and frees its TMEM.
 #include "ykb_internal.hpp"
 
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <algorithm>
 #include <mutex>
 
 namespace ykb {
@@ -118,40 +125,57 @@ __device__ __forceinline__ void segment_parts(int seg, int& a, int& t)
     t = (0x012010 >> (4 * seg)) & 0xF;
 }
 
+constexpr int kEpiWarps = 4;
+constexpr int kFilterThreads = 64 + 32 * kEpiWarps;  // producer, MMA issuer, 4 epilogue warps
+constexpr int kStagePitch = 17;                       // floats per staged row (odd: no bank conflicts)
+
+__device__ __forceinline__ void bar_arrive(uint64_t* b)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
+}
+
+// Persistent CTA (one per SM): tiles t = blockIdx.x + i * gridDim.x of 128
+// output rows x TN columns, row tile t / col_tiles, column tile t % col_tiles
+// (the column tiles of a row tile run back to back, so its A rows are read
+// from L2 while hot).  Two TMEM accumulators: the MMA warp fills one while
+// the epilogue warps drain the other.
 template <int TN, bool PAIR, int NSEG>
-__global__ void __launch_bounds__(128, 1) ramp_tc_kernel(
+__global__ void __launch_bounds__(kFilterThreads, 1) ramp_tc_kernel(
     const __grid_constant__ CUtensorMap map_a0, const __grid_constant__ CUtensorMap map_a1,
     const __grid_constant__ CUtensorMap map_a2, const __grid_constant__ CUtensorMap map_t0,
     const __grid_constant__ CUtensorMap map_t1, const __grid_constant__ CUtensorMap map_t2,
-    long rows, int nu, int nv, int kchunks, const FdkPreweightView* __restrict__ pwv,
-    float* __restrict__ C, int ldc, int* __restrict__ err)
+    long rows, int nu, int nv, int kchunks, int col_tiles, long tiles,
+    const FdkPreweightView* __restrict__ pwv, float* __restrict__ C, int ldc, int* __restrict__ err)
 {
     constexpr uint32_t kBStageBytes = TN * TK * 2;
-    constexpr uint32_t kTmemCols = TN <= 32 ? 32 : TN <= 64 ? 64 : TN <= 128 ? 128 : 256;
+    constexpr uint32_t kAccCols = TN <= 32 ? 32 : TN <= 64 ? 64 : TN <= 128 ? 128 : 256;
+    constexpr uint32_t kTmemCols = 2 * kAccCols;
     extern __shared__ unsigned char smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
     unsigned char* a_ring = smem;
     unsigned char* b_ring = smem + STAGES * kAStageBytes;
-    uint64_t* full = reinterpret_cast<uint64_t*>(b_ring + STAGES * kBStageBytes);
+    float* staging = reinterpret_cast<float*>(b_ring + STAGES * kBStageBytes);
+    uint64_t* full = reinterpret_cast<uint64_t*>(staging + kEpiWarps * 32 * kStagePitch);
     uint64_t* empty = full + STAGES;
-    uint64_t* done = empty + STAGES;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+    uint64_t* acc_full = empty + STAGES;
+    uint64_t* acc_empty = acc_full + 2;
+    uint64_t* mma_done = acc_empty + 2;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mma_done + 1);
     int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const long m0 = static_cast<long>(blockIdx.y) * TM;
-    const int n0 = blockIdx.x * TN;
-    const int total = NSEG * kchunks;
+    const int total = NSEG * kchunks;  // k-steps per tile
 
-    if (warp == 0) {
+    if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
                      ::"r"(smem_u32(tmem_slot)), "r"(kTmemCols) : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
-    if (threadIdx.x == 32) {
+    if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; ++s) { bar_init(&full[s], 1); bar_init(&empty[s], 1); }
-        bar_init(done, 1);
+        for (int b = 0; b < 2; ++b) { bar_init(&acc_full[b], 1); bar_init(&acc_empty[b], kEpiWarps); }
+        bar_init(mma_done, 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -160,102 +184,158 @@ __global__ void __launch_bounds__(128, 1) ramp_tc_kernel(
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tmem_slot;
 
-    if (warp == 0 && lane == 0) {
-        // ------------------------------------------------------- producer ---
-        int issued = 0;
-        for (int i = 0; i < total; ++i) {
-            const int s = i % STAGES;
-            if (i >= STAGES && !bar_wait(&empty[s], ((i / STAGES) - 1) & 1)) {
-                atomicOr(err, kErrTimeout);
-                *(volatile int*)abort_flag = 1;
-                break;
-            }
-            if (*(volatile int*)abort_flag) break;
-            const int seg = i / kchunks, kc = i - seg * kchunks;
-            int pa, pt;
-            segment_parts(seg, pa, pt);
-            const CUtensorMap* ma = pa == 0 ? &map_a0 : pa == 1 ? &map_a1 : &map_a2;
-            const CUtensorMap* mt = pt == 0 ? &map_t0 : pt == 1 ? &map_t1 : &map_t2;
-            bar_expect_tx(&full[s], kAStageBytes + kBStageBytes);
-            tma_2d(a_ring + s * kAStageBytes, ma, &full[s], kc * TK, static_cast<int>(m0));
-            tma_2d(b_ring + s * kBStageBytes, mt, &full[s], kc * TK, n0);
-            issued = i + 1;
-        }
-        // every issued copy must land before the CTA can exit
-        for (int i = (issued > STAGES ? issued - STAGES : 0); i < issued; ++i)
-            bar_wait(&full[i % STAGES], (i / STAGES) & 1);
-    } else if (warp == 1 && lane == 0) {
-        // ----------------------------------------------------- MMA issuer ---
-        const uint32_t idesc = instr_desc<TN>();
-        int issued = 0;
-        for (int i = 0; i < total; ++i) {
-            const int s = i % STAGES;
-            if (!bar_wait(&full[s], (i / STAGES) & 1)) {
-                atomicOr(err, kErrTimeout);
-                *(volatile int*)abort_flag = 1;
-                break;
-            }
-            if (*(volatile int*)abort_flag) break;
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint64_t da = kmajor_sw128_desc(smem_u32(a_ring + s * kAStageBytes));
-            const uint64_t db = kmajor_sw128_desc(smem_u32(b_ring + s * kBStageBytes));
-#pragma unroll
-            for (int kk = 0; kk < TK / 16; ++kk)
-                mma_bf16(tmem, da + 2 * kk, db + 2 * kk, idesc, (i > 0 || kk > 0) ? 1u : 0u);
-            mma_commit(&empty[s]);
-            issued = i + 1;
-        }
-        // `done` completes when every issued MMA has retired
-        mma_commit(done);
-        (void)issued;
-    }
-    __syncwarp();
-
-    // --------------------------------------------------------- epilogue ---
-    const bool ok = bar_wait(done, 0);
-    if (!ok) atomicOr(err, kErrTimeout);
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const long m = m0 + warp * 32 + lane;
-    const bool row_ok = ok && !*(volatile int*)abort_flag && m < rows;
-    int out_lo = 0, out_hi = 0;
-    if (row_ok) {
-        const FdkPreweightView& p = pwv[m / nv];
-        out_lo = p.out_lo;
-        out_hi = p.out_hi;
-    }
-#pragma unroll 1
-    for (int c = 0; c < TN; c += 16) {
-        uint32_t r[16];
-        const uint32_t taddr = tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c);
-        asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-                     : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
-                       "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
-                       "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-                     : "r"(taddr));
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        if (row_ok) {
-            float* dst = C + m * (PAIR ? 2 : 1) * ldc + (PAIR ? 2 * kPairLead : 0);
-#pragma unroll
-            for (int i = 0; i < 16; ++i) {
-                const int j = n0 + c + i;
-                if (j >= nu) continue;
-                const float v = (j >= out_lo && j < out_hi) ? __uint_as_float(r[i]) : 0.f;
-                if constexpr (!PAIR) {
-                    dst[j] = v;
-                } else {
-                    // tap pairs: left of pair j, right of pair j-1; the pairs
-                    // around the row are zero where they reach outside it
-                    dst[2 * j] = v;
-                    dst[2 * j - 1] = v;
-                    if (j == 0) dst[-2] = dst[-3] = dst[-4] = 0.f;
-                    if (j == nu - 1) dst[2 * j + 1] = 0.f;
+    if (warp == 0) {
+        if (lane == 0) {
+            // --------------------------------------------------- producer ---
+            long it = 0, issued = 0;
+            bool stop = false;
+            for (long t = blockIdx.x; t < tiles && !stop; t += gridDim.x) {
+                const int m0 = static_cast<int>((t / col_tiles) * TM);
+                const int n0 = static_cast<int>((t % col_tiles) * TN);
+                for (int i = 0; i < total; ++i, ++it) {
+                    const int s = static_cast<int>(it % STAGES);
+                    if (it >= STAGES && !bar_wait(&empty[s], static_cast<uint32_t>((it / STAGES) - 1) & 1)) {
+                        atomicOr(err, kErrTimeout);
+                        *(volatile int*)abort_flag = 1;
+                    }
+                    if (*(volatile int*)abort_flag) { stop = true; break; }
+                    const int seg = i / kchunks, kc = i - seg * kchunks;
+                    int pa, pt;
+                    segment_parts(seg, pa, pt);
+                    const CUtensorMap* ma = pa == 0 ? &map_a0 : pa == 1 ? &map_a1 : &map_a2;
+                    const CUtensorMap* mt = pt == 0 ? &map_t0 : pt == 1 ? &map_t1 : &map_t2;
+                    bar_expect_tx(&full[s], kAStageBytes + kBStageBytes);
+                    tma_2d(a_ring + s * kAStageBytes, ma, &full[s], kc * TK, m0);
+                    tma_2d(b_ring + s * kBStageBytes, mt, &full[s], kc * TK, n0);
+                    issued = it + 1;
                 }
             }
+            // every issued copy must land before the CTA can exit
+            for (long j = (issued > STAGES ? issued - STAGES : 0); j < issued; ++j)
+                bar_wait(&full[j % STAGES], static_cast<uint32_t>(j / STAGES) & 1);
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // ------------------------------------------------- MMA issuer ---
+            const uint32_t idesc = instr_desc<TN>();
+            long it = 0;
+            int tl = 0;
+            bool stop = false;
+            for (long t = blockIdx.x; t < tiles && !stop; t += gridDim.x, ++tl) {
+                const int buf = tl & 1;
+                // the epilogue has drained this accumulator's previous tile
+                if (tl >= 2 && !bar_wait(&acc_empty[buf], static_cast<uint32_t>((tl >> 1) - 1) & 1)) {
+                    atomicOr(err, kErrTimeout);
+                    *(volatile int*)abort_flag = 1;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t d = tmem + static_cast<uint32_t>(buf) * kAccCols;
+                for (int i = 0; i < total; ++i, ++it) {
+                    const int s = static_cast<int>(it % STAGES);
+                    if (!bar_wait(&full[s], static_cast<uint32_t>(it / STAGES) & 1)) {
+                        atomicOr(err, kErrTimeout);
+                        *(volatile int*)abort_flag = 1;
+                    }
+                    if (*(volatile int*)abort_flag) { stop = true; break; }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint64_t da = kmajor_sw128_desc(smem_u32(a_ring + s * kAStageBytes));
+                    const uint64_t db = kmajor_sw128_desc(smem_u32(b_ring + s * kBStageBytes));
+#pragma unroll
+                    for (int kk = 0; kk < TK / 16; ++kk)
+                        mma_bf16(d, da + 2 * kk, db + 2 * kk, idesc, (i > 0 || kk > 0) ? 1u : 0u);
+                    mma_commit(&empty[s]);
+                }
+                if (!stop) mma_commit(&acc_full[buf]);
+            }
+            // completes when every MMA issued above has retired
+            mma_commit(mma_done);
+        }
+        __syncwarp();
+    } else {
+        // --------------------------------------------------- epilogue ---
+        // warp w reads TMEM lanes 32 (w % 4) ..: rows m0 + 32 (w % 4) + lane
+        const int q = warp & 3;
+        float* stg = staging + (warp - 2) * 32 * kStagePitch;
+        int tl = 0;
+        for (long t = blockIdx.x; t < tiles; t += gridDim.x, ++tl) {
+            const int buf = tl & 1;
+            // the warp leaves together when a wait runs out
+            if (!__all_sync(0xffffffffu, bar_wait(&acc_full[buf], static_cast<uint32_t>(tl >> 1) & 1))) {
+                if (lane == 0) {
+                    atomicOr(err, kErrTimeout);
+                    *(volatile int*)abort_flag = 1;
+                }
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const long m0 = (t / col_tiles) * TM;
+            const int n0 = static_cast<int>((t % col_tiles) * TN);
+            const long m = m0 + q * 32 + lane;
+            int out_lo = 0, out_hi = 0;
+            if (m < rows) {
+                const FdkPreweightView& p = pwv[m / nv];
+                out_lo = p.out_lo;
+                out_hi = p.out_hi;
+            }
+#pragma unroll 1
+            for (int c = 0; c < TN; c += 16) {
+                uint32_t r[16];
+                const uint32_t taddr = tmem + (static_cast<uint32_t>(q * 32) << 16) +
+                    static_cast<uint32_t>(buf) * kAccCols + static_cast<uint32_t>(c);
+                asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                             : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+                               "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
+                               "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                             : "r"(taddr));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                const int c0 = n0 + c;
+                // this lane's row, masked to the samples placed in the padded row
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                    const int j = c0 + i;
+                    stg[lane * kStagePitch + i] = (j < nu && j >= out_lo && j < out_hi)
+                        ? __uint_as_float(r[i]) : 0.f;
+                }
+                __syncwarp();
+                // transposed: each store instruction writes one row's chunk
+                if constexpr (PAIR) {
+                    // tap pairs: floats 2j - 1 (right of pair j - 1) and 2j
+                    // (left of pair j) both hold f[j]; lane l writes float
+                    // 2 c0 - 1 + l, which is f[c0 + l / 2]; the right of the
+                    // last pair (float 2 nu - 1) is zero, as are the floats
+                    // of the pairs before the row (-4 .. -2)
+                    const int j = c0 + (lane >> 1);
+                    for (int rr = 0; rr < 32; ++rr) {
+                        const long mr = m0 + q * 32 + rr;
+                        if (mr >= rows) break;
+                        float* dst = C + mr * 2 * ldc + 2 * kPairLead;
+                        if (j < nu) dst[2 * c0 - 1 + lane] = stg[rr * kStagePitch + (lane >> 1)];
+                        else if (j == nu && (lane & 1) == 0) dst[2 * c0 - 1 + lane] = 0.f;
+                        if (c0 == 0 && lane < 3) dst[-4 + lane] = 0.f;
+                    }
+                } else {
+                    const int half = lane >> 4, jj = c0 + (lane & 15);
+                    for (int rr = 0; rr < 32; rr += 2) {
+                        const long mr = m0 + q * 32 + rr + half;
+                        if (mr < rows && jj < nu)
+                            C[mr * ldc + jj] = stg[(rr + half) * kStagePitch + (lane & 15)];
+                    }
+                }
+                __syncwarp();
+            }
+            // this accumulator is read out: the MMA warp may refill it
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) bar_arrive(&acc_empty[buf]);
         }
     }
+    // teardown: every MMA retired before the TMEM is freed
+    __syncwarp();
+    if (warp == 1 && lane == 0) bar_wait(mma_done, 0);
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    if (warp == 0)
+    if (warp == 1)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
                      ::"r"(tmem), "r"(kTmemCols) : "memory");
 }
@@ -332,14 +412,21 @@ template <int TN, bool PAIR, int NSEG>
 cudaError_t launch_tn3(const CUtensorMap* a, const CUtensorMap* t, long rows, int nu, int nv,
     int kchunks, const FdkPreweightView* pwv, float* C, int ldc, int* err, cudaStream_t s)
 {
-    const size_t smem = 1024 + STAGES * (kAStageBytes + TN * TK * 2) + (2 * STAGES + 1) * 8 + 16;
+    const size_t smem = 1024 + STAGES * (kAStageBytes + TN * TK * 2) +
+        kEpiWarps * 32 * kStagePitch * sizeof(float) + (2 * STAGES + 5) * 8 + 16;
     auto k = ramp_tc_kernel<TN, PAIR, NSEG>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
         static_cast<int>(smem));
     if (e != cudaSuccess) return e;
-    const dim3 grid((nu + TN - 1) / TN, static_cast<unsigned>((rows + TM - 1) / TM));
-    k<<<grid, 128, smem, s>>>(a[0], a[1], a[2], t[0], t[1], t[2], rows, nu, nv, kchunks, pwv, C,
-        ldc, err);
+    int device = 0, sms = 0;
+    if ((e = cudaGetDevice(&device)) != cudaSuccess ||
+        (e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess)
+        return e;
+    const int col_tiles = (nu + TN - 1) / TN;
+    const long tiles = static_cast<long>(col_tiles) * ((rows + TM - 1) / TM);
+    const unsigned grid = static_cast<unsigned>(std::min<long>(tiles, sms));
+    k<<<grid, kFilterThreads, smem, s>>>(a[0], a[1], a[2], t[0], t[1], t[2], rows, nu, nv,
+        kchunks, col_tiles, tiles, pwv, C, ldc, err);
     return cudaGetLastError();
 }
 
