@@ -786,7 +786,18 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
     return fn;
 }
 
-constexpr int kWidths[] = {36, 52, 68, 100, 132, 196, 256};
+// Staged box widths (elements).  Each is 8 mod 16, so a row of tap pairs is
+// 64 mod 128 bytes: the 16 lanes of a half-warp, whose footprints span a few
+// columns and at most a row or two, then rarely meet on one bank (a pitch of
+// 32 mod 128 bytes put rows n and n + 1 four pairs apart on the same banks:
+// 16 % more shared-memory wavefronts, measured).
+constexpr int kWidths[] = {40, 56, 72, 104, 136, 200, 248};
+// Widths 4 narrower, for the axial tap-pair FDK kernel only: taken when the
+// narrower stage leaves room for one more ring stage (a third stage beats
+// the better bank pattern: 1081 vs 1491 ms on the 1024^3 x 1440 workload,
+// whose 52-wide box needs 3 stages of 34.5 KB).  The other kernels launch
+// such a box at the next width of kWidths.
+constexpr int kNarrowWidths[] = {36, 52, 68, 100, 132, 196};
 
 // z tiling: ZT-slice tiles, except that a remainder of at most kZTail
 // slices becomes one kZTail-slice tile instead of a ZT-slice tile that is
@@ -831,27 +842,50 @@ cudaError_t launch_bw(const CUtensorMap& map, const FdkViewCoef* coef, int n_vie
         stages, smem, vol, accumulate, err, pseudo, pw, s);
 }
 
+template <int BW>
+cudaError_t launch_narrow(const CUtensorMap& map, const FdkViewCoef* coef, int n_views,
+    const VolumeGrid& g, int BH, int stages, size_t smem, float* vol, int accumulate, int* err,
+    PipelineWait pw, cudaStream_t s)
+{
+    return launch_kernel(fdk_bp_tma_kernel<BW, true, true, false>, map, coef, n_views, g, BH,
+        stages, smem, vol, accumulate, err, nullptr, pw, s);
+}
+
 template <bool PAIR>
 cudaError_t launch_layout(const CUtensorMap& map, const FdkViewCoef* coef, int n_views,
     const VolumeGrid& g, int bw, int bh, int stages, size_t smem, bool axial, float* vol,
     int accumulate, int* err, const PseudoViewCoef* pseudo, PipelineWait pw, cudaStream_t s)
 {
     switch (bw) {
-    case 36: return launch_bw<36, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, pw, s);
-    case 52: return launch_bw<52, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, pw, s);
-    case 68: return launch_bw<68, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, pw, s);
-    case 100: return launch_bw<100, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, pw, s);
-    case 132: return launch_bw<132, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, pw, s);
-    case 196: return launch_bw<196, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, pw, s);
-    case 256: return launch_bw<256, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, pw, s);
-    default: return cudaErrorInvalidValue;
+    case 40: return launch_bw<40, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, pw, s);
+    case 56: return launch_bw<56, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, pw, s);
+    case 72: return launch_bw<72, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, pw, s);
+    case 104: return launch_bw<104, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, pw, s);
+    case 136: return launch_bw<136, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, pw, s);
+    case 200: return launch_bw<200, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, pw, s);
+    case 248: return launch_bw<248, PAIR>(map, coef, n_views, g, bh, stages, smem, axial, vol, accumulate, err, pseudo, pw, s);
+    default: break;
     }
+    if constexpr (PAIR) {
+        if (axial && !pseudo) {
+            switch (bw) {
+            case 36: return launch_narrow<36>(map, coef, n_views, g, bh, stages, smem, vol, accumulate, err, pw, s);
+            case 52: return launch_narrow<52>(map, coef, n_views, g, bh, stages, smem, vol, accumulate, err, pw, s);
+            case 68: return launch_narrow<68>(map, coef, n_views, g, bh, stages, smem, vol, accumulate, err, pw, s);
+            case 100: return launch_narrow<100>(map, coef, n_views, g, bh, stages, smem, vol, accumulate, err, pw, s);
+            case 132: return launch_narrow<132>(map, coef, n_views, g, bh, stages, smem, vol, accumulate, err, pw, s);
+            case 196: return launch_narrow<196>(map, coef, n_views, g, bh, stages, smem, vol, accumulate, err, pw, s);
+            default: break;
+            }
+        }
+    }
+    return cudaErrorInvalidValue;
 }
 
 } // namespace
 
 // Largest tile box over all views and tiles; returns the chosen width (one of
-// kWidths, 0 if none fits) and height.
+// kWidths or kNarrowWidths, 0 if none fits) and height.
 cudaError_t fdk_tma_box(const FdkViewCoef* coef, int n_views, const VolumeGrid& g, int* scratch2,
     int* bw, int* bh, cudaStream_t s)
 {
@@ -865,10 +899,17 @@ cudaError_t fdk_tma_box(const FdkViewCoef* coef, int n_views, const VolumeGrid& 
     if ((e = cudaMemcpyAsync(host, scratch2, sizeof host, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
         return e;
     if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
+    *bh = host[1];
+    if (*bh > 256) return cudaSuccess;
     for (int w : kWidths)
         if (w >= host[0]) { *bw = w; break; }
-    *bh = host[1];
-    if (*bh > 256) *bw = 0;
+    // the narrower width when it fits the box and buys a ring stage while the
+    // wider one still runs (2 stages or more) for the other kernels
+    const int wide = fdk_tma_stages(*bw, *bh, kFilteredPairs);
+    for (int w : kNarrowWidths)
+        if (w == *bw - 4 && w >= host[0] && wide >= 2 &&
+            fdk_tma_stages(w, *bh, kFilteredPairs) > wide)
+            *bw = w;
     return cudaSuccess;
 }
 
@@ -894,6 +935,7 @@ cudaError_t launch_fdk_backproject_tma(const float* filtered, int layout, int ld
     auto enc = encode_fn();
     if (!enc) return cudaErrorNotSupported;
     const bool pair = layout == kFilteredPairs;
+    if (bw % 16 == 4 && !(pair && axial && !pseudo)) bw += 4;  // a narrow width: see kNarrowWidths
     const size_t esz = pair ? 8 : 4;  // a tap pair moves as one 8-byte element
     CUtensorMap map;
     const cuuint64_t dims[3] = {static_cast<cuuint64_t>(pair ? nu + kPairLead : nu),

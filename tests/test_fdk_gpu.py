@@ -421,3 +421,27 @@ def test_pipeline_wait_timeout_is_reported_and_the_plan_recovers(oracle, cuda_de
     plan.check()
     assert torch.equal(again, expected)
     plan.close()
+
+
+def test_stage_timing_counts_launch_groups(oracle, cuda_device):
+    # ykb_fdk_stage_timing records one event pair per filter and per
+    # backprojection launch group; the tally restarts after each read
+    import torch
+    from fdk_cuda_impl_b200.projectors import FdkPlan
+    case = K.c1_small()
+    views = case.scan.views()
+    p = torch.from_numpy(K.projections(oracle, case, views)).cuda()
+    plan = FdkPlan(views, case.scan.channels, case.scan.rows, case.scan.scan_range, case.grid,
+                   case.filt)
+    plan.stage_timing(True)
+    for _ in range(3):
+        plan.execute(p)
+    t = plan.stage_times()
+    assert t["filter_groups"] == 3 and t["backproject_groups"] == 3
+    assert t["filter_ms"] > 0 and t["backproject_ms"] > 0
+    assert plan.stage_times()["backproject_groups"] == 0
+    plan.stage_timing(False)
+    plan.execute(p)
+    assert plan.stage_times()["filter_groups"] == 0
+    plan.check()
+    plan.close()
