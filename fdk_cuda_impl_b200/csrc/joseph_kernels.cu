@@ -70,7 +70,13 @@ __device__ __forceinline__ void slice_range(float a, float e, int n, int n0, int
     hi = min(hi, static_cast<int>(ceilf(t1)) + 1);
 }
 
-// One thread per ray; a block covers 32 channels x 4 rows of one view.
+// One thread per ray; a block covers 32 channels x 4 rows of one view, a
+// warp one detector row.  The warp walks the union of its rays' slice ranges
+// together, each lane sampling only inside its own: at every step the 32
+// gathers fall on one slice plane, on a run of about 32 magnified voxels of
+// two rows, instead of on up to a few planes when lanes whose rays enter
+// the volume at different slices would run ahead of one another.  Each
+// lane's samples and their order are unchanged.
 __global__ void __launch_bounds__(128) joseph_fp_kernel(const float* __restrict__ slab,
     const JosephView* __restrict__ views, int view0, int nu, int nv, float* __restrict__ proj,
     int accumulate)
@@ -78,20 +84,28 @@ __global__ void __launch_bounds__(128) joseph_fp_kernel(const float* __restrict_
     const int iu = blockIdx.x * 32 + threadIdx.x;
     const int iv = blockIdx.y * 4 + threadIdx.y;
     const int k = view0 + blockIdx.z;
-    if (iu >= nu || iv >= nv) return;
+    const bool pixel = iu < nu && iv < nv;
     const JosephView& j = views[k];
-    const RayParams r = ray_params(j, iu, iv);
-    // FP64 ray sum: keeps the adjoint identity at the 1e-7 level
-    double acc = 0.0;
-    if (r.ok) {
-        int lo = 0, hi = j.n0 - 1;
+    const RayParams r = ray_params(j, min(iu, nu - 1), min(iv, nv - 1));
+    int lo = 0, hi = j.n0 - 1;
+    if (pixel && r.ok) {
         slice_range(r.a1, r.e1, j.n1, j.n0, lo, hi);
         slice_range(r.a2, r.e2, j.n2, j.n0, lo, hi);
+    } else {
+        lo = 1; hi = 0;
+    }
+    // the warp's slice span (every lane reaches here: no early return above)
+    const int wlo = __reduce_min_sync(0xffffffffu, lo <= hi ? lo : 0x7fffffff);
+    const int whi = __reduce_max_sync(0xffffffffu, lo <= hi ? hi : -1);
+    // FP64 ray sum: keeps the adjoint identity at the 1e-7 level
+    double acc = 0.0;
+    {
         const long plane = static_cast<long>(j.n1) * j.n2;
         const float half = 0.5f * (j.n0 - 1);
         // unrolled: the four gathers of several samples are in flight at once
 #pragma unroll 4
-        for (int s = lo; s <= hi; ++s) {
+        for (int s = wlo; s <= whi; ++s) {
+            if (s < lo || s > hi) continue;
             const float c0 = static_cast<float>(s) - half;
             const float f1 = fmaf(r.a1, c0, r.e1);
             const float f2 = fmaf(r.a2, c0, r.e2);
@@ -113,6 +127,7 @@ __global__ void __launch_bounds__(128) joseph_fp_kernel(const float* __restrict_
         }
         acc *= r.len;
     }
+    if (!pixel) return;
     float* dst = proj + (static_cast<long>(k) * nv + iv) * nu + iu;
     *dst = accumulate ? static_cast<float>(*dst + acc) : static_cast<float>(acc);
 }
@@ -299,7 +314,168 @@ __global__ void __launch_bounds__(256) joseph_bp_kernel(const float* __restrict_
     }
 }
 
+// ---------------------------------------------------------------------------
+// Column backprojector, for scans whose detector columns are axial: every
+// view has main axis x or y (so z is minor axis 2) and all rays of a
+// detector column share their minor-1 parameters (a1, e1) bit for bit (the
+// detector's v axis has no component along the main or minor-1 axis; checked
+// on the device when the plan is built).  It applies the same transpose as
+// joseph_bp_kernel with the roles turned around: a thread owns a stack of ZC
+// voxels of one (x, y) column and, per view, walks the candidate detector
+// columns once (the minor-1 weight is a property of the column) and their
+// rays once each, scattering every ray's two minor-2 weights into the stack:
+// about 2.5 columns x 1.3 rays per voxel, each ray touching only the two
+// voxels it reaches, where the gather evaluates every candidate of the box
+// against every voxel of its stack.  The stack is private to its thread
+// (shared memory laid out [slot][thread], one bank per thread, no atomics),
+// so the sums are deterministic: per view in FP32 in ray order, over views
+// in FP64 registers.
+// ---------------------------------------------------------------------------
+
+// (a1, e1) of every detector column from its first row.
+__global__ void joseph_column_table_kernel(const float4* __restrict__ rays, int n_views, int nu,
+    int nv, float2* __restrict__ cols)
+{
+    const long n = static_cast<long>(n_views) * nu;
+    for (long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long>(gridDim.x) * blockDim.x) {
+        const long k = i / nu, iu = i - k * nu;
+        const float4 r = rays[k * nu * nv + iu];
+        cols[i] = make_float2(r.x, r.y);
+    }
+}
+
+// flag[0] = 1 when some ray's (a1, e1) differs from its column's.
+__global__ void joseph_column_check_kernel(const float4* __restrict__ rays,
+    const float2* __restrict__ cols, int n_views, int nu, int nv, int* __restrict__ flag)
+{
+    const long n = static_cast<long>(n_views) * nu * nv;
+    bool differs = false;
+    for (long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long>(gridDim.x) * blockDim.x) {
+        const long k = i / (static_cast<long>(nu) * nv);
+        const long iu = i % nu;
+        const float4 r = rays[i];
+        const float2 c = cols[k * nu + iu];
+        differs |= __float_as_uint(r.x) != __float_as_uint(c.x) ||
+                   __float_as_uint(r.y) != __float_as_uint(c.y);
+    }
+    if (__any_sync(0xffffffffu, differs) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
+}
+
+// (a2, e2, value x chord length, 0) per ray: one 16-byte load per ray in the
+// column backprojector.
+__global__ void joseph_weight_rays4_kernel(const float* __restrict__ proj,
+    const float4* __restrict__ rays, const float* __restrict__ lens, long n,
+    float4* __restrict__ out)
+{
+    for (long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long>(gridDim.x) * blockDim.x) {
+        const float4 r = rays[i];
+        out[i] = make_float4(r.z, r.w, proj[i] * lens[i], 0.f);
+    }
+}
+
+constexpr int kColThreads = 128;  // 32 x 4 voxel columns a block
+
+template <int ZC>
+__global__ void __launch_bounds__(kColThreads) joseph_bp_column_kernel(
+    const float4* __restrict__ w4, const float2* __restrict__ cols,
+    const ViewProj* __restrict__ vp, const JosephView* __restrict__ views, int n_views, int nu,
+    int nv, int nx, int ny, int nz, float* __restrict__ vol, int accumulate)
+{
+    // slot q + 1 holds voxel z0 + q; slots 0 and ZC + 1 catch the half of a
+    // ray's pair that falls just outside the stack
+    __shared__ float part[(ZC + 2) * kColThreads];
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    float* my = part + tid;
+#pragma unroll
+    for (int q = 0; q < ZC + 2; ++q) my[q * kColThreads] = 0.f;
+    const int x = blockIdx.x * 32 + threadIdx.x;
+    const int y = blockIdx.y * 4 + threadIdx.y;
+    const int z0 = blockIdx.z * ZC;
+    if (x >= nx || y >= ny) return;
+    const float zlo = static_cast<float>(z0 - 1), zhi = static_cast<float>(z0 + ZC - 1);
+    double acc[ZC];
+#pragma unroll
+    for (int q = 0; q < ZC; ++q) acc[q] = 0.0;
+    for (int k = 0; k < n_views; ++k) {
+        const JosephView& j = views[k];
+        const int s = j.axis == 0 ? x : y, j1 = j.axis == 0 ? y : x;
+        const float c0 = static_cast<float>(s) - 0.5f * (j.n0 - 1);
+        int u0, u1, v0, v1;
+        footprint_box(vp[k], j, c0, j1, z0, z0 + ZC - 1, nu, nv, u0, u1, v0, v1);
+        const float j1f = static_cast<float>(j1);
+        const float2* ck = cols + static_cast<long>(k) * nu;
+        for (int iu = u0; iu <= u1; ++iu) {
+            // the forward projector's minor-1 weights: 1 - w to floor(f1),
+            // w to floor(f1) + 1
+            const float2 ce = __ldg(ck + iu);
+            const float f1 = fmaf(ce.x, c0, ce.y);
+            const float fl1 = floorf(f1);
+            const float w1 = f1 - fl1;
+            const float h1 = fl1 == j1f ? 1.f - w1 : (fl1 + 1.f == j1f ? w1 : 0.f);
+            if (h1 == 0.f) continue;
+            const float4* r = w4 + (static_cast<long>(k) * nv + v0) * nu + iu;
+#pragma unroll 2
+            for (int iv = v0; iv <= v1; ++iv, r += nu) {
+                const float4 q = __ldg(r);
+                const float f2 = fmaf(q.x, c0, q.y);
+                const float fl2 = floorf(f2);
+                if (!(fl2 >= zlo && fl2 <= zhi)) continue;
+                const float w2 = f2 - fl2;
+                const float t = q.z * h1;
+                float* p = my + (static_cast<int>(fl2) - z0 + 1) * kColThreads;
+                p[0] = fmaf(t, 1.f - w2, p[0]);
+                p[kColThreads] = fmaf(t, w2, p[kColThreads]);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < ZC; ++q) {
+            float* p = my + (q + 1) * kColThreads;
+            acc[q] += static_cast<double>(*p);
+            *p = 0.f;
+        }
+        my[0] = 0.f;
+        my[(ZC + 1) * kColThreads] = 0.f;
+    }
+    const long plane = static_cast<long>(nx) * ny;
+#pragma unroll
+    for (int q = 0; q < ZC; ++q) {
+        if (z0 + q >= nz) break;
+        float* dst = vol + (z0 + q) * plane + static_cast<long>(y) * nx + x;
+        *dst = accumulate ? static_cast<float>(*dst + acc[q]) : static_cast<float>(acc[q]);
+    }
+}
+
 } // namespace
+
+cudaError_t launch_joseph_column_table(const float4* rays, int n_views, int nu, int nv,
+    float2* cols, int* flag, cudaStream_t s)
+{
+    cudaError_t e = cudaMemsetAsync(flag, 0, sizeof(int), s);
+    if (e != cudaSuccess) return e;
+    joseph_column_table_kernel<<<148 * 4, 256, 0, s>>>(rays, n_views, nu, nv, cols);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    joseph_column_check_kernel<<<148 * 8, 256, 0, s>>>(rays, cols, n_views, nu, nv, flag);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_joseph_bp_columns(const float* proj, const float4* rays, const float* lens,
+    const float2* cols, const float* view_proj, const JosephView* views, int n_views, int nu,
+    int nv, const ykb_volume& vol, float4* weighted4, float* out, int accumulate, cudaStream_t s)
+{
+    const long n = static_cast<long>(n_views) * nu * nv;
+    joseph_weight_rays4_kernel<<<148 * 8, 256, 0, s>>>(proj, rays, lens, n, weighted4);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    constexpr int ZC = 16;
+    const dim3 grid((vol.nx + 31) / 32, (vol.ny + 3) / 4, (vol.nz + ZC - 1) / ZC);
+    joseph_bp_column_kernel<ZC><<<grid, dim3(32, 4), 0, s>>>(weighted4, cols,
+        reinterpret_cast<const ViewProj*>(view_proj), views, n_views, nu, nv, vol.nx, vol.ny,
+        vol.nz, out, accumulate);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_joseph_transpose(const float* vol, int nx, int ny, int nz, float* vol_yzx,
     float* vol_xzy, cudaStream_t s)

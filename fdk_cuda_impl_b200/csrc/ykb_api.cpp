@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 
@@ -734,7 +735,6 @@ YKB_API ykb_status ykb_joseph_plan_create(const ykb_cone_view* views, int n_view
         (e = p->view_proj.alloc(sizeof(float) * vp.size())) != cudaSuccess ||
         (e = p->rays.alloc(sizeof(float4) * rays)) != cudaSuccess ||
         (e = p->lens.alloc(sizeof(float) * rays)) != cudaSuccess ||
-        (e = p->weighted.alloc(sizeof(float) * rays)) != cudaSuccess ||
         (need_y && (e = p->slab_y.alloc(vol_bytes)) != cudaSuccess) ||
         (need_x && (e = p->slab_x.alloc(vol_bytes)) != cudaSuccess)) {
         delete p;
@@ -756,6 +756,26 @@ YKB_API ykb_status ykb_joseph_plan_create(const ykb_cone_view* views, int n_view
     e = launch_joseph_ray_table(p->views.as<JosephView>(), n_views, nu, nv, p->rays.as<float4>(),
         p->lens.as<float>(), s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    // the column backprojector when every view's main axis is x or y and its
+    // detector columns are axial (YKB_JOSEPH_BP=gather keeps the gather)
+    bool columns = std::none_of(p->axes.begin(), p->axes.end(), [](int a) { return a == 2; });
+    if (const char* env = std::getenv("YKB_JOSEPH_BP"))
+        if (std::strcmp(env, "gather") == 0) columns = false;
+    if (e == cudaSuccess && columns) {
+        DeviceBuffer flag;
+        int differs = 1;
+        if ((e = p->cols.alloc(sizeof(float2) * n_views * nu)) == cudaSuccess &&
+            (e = flag.alloc(sizeof(int))) == cudaSuccess &&
+            (e = launch_joseph_column_table(p->rays.as<float4>(), n_views, nu, nv,
+                 p->cols.as<float2>(), flag.as<int>(), s)) == cudaSuccess &&
+            (e = cudaMemcpyAsync(&differs, flag.ptr, sizeof(int), cudaMemcpyDeviceToHost, s)) ==
+                cudaSuccess)
+            e = cudaStreamSynchronize(s);
+        p->column_bp = e == cudaSuccess && differs == 0;
+        if (!p->column_bp) p->cols.reset();
+    }
+    if (e == cudaSuccess)
+        e = p->weighted.alloc((p->column_bp ? sizeof(float4) : sizeof(float)) * rays);
     cudaStreamDestroy(s);
     if (e != cudaSuccess) {
         delete p;
@@ -778,7 +798,8 @@ YKB_API size_t ykb_joseph_workspace_bytes(const ykb_joseph_plan* p)
 {
     if (!p) return 0;
     return p->views.bytes + p->view_proj.bytes + p->rays.bytes + p->lens.bytes +
-        p->weighted.bytes + p->slab_x.bytes + p->slab_y.bytes + p->world_views.bytes +
+        p->weighted.bytes + p->cols.bytes + p->slab_x.bytes + p->slab_y.bytes +
+        p->world_views.bytes +
         p->fdk_coef.bytes +
         p->pseudo_coef.bytes + p->pairs.bytes + p->err_flag.bytes;
 }
@@ -1022,9 +1043,15 @@ YKB_API ykb_status ykb_joseph_bp(ykb_joseph_plan* p, const float* d_proj, float*
     if (!d_volume || !d_proj) return fail(YKB_ERR_INVALID_BUFFER, "null volume or projection buffer");
     DeviceGuard guard(p->device);
     const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    YKB_TRY_CUDA(launch_joseph_bp(d_proj, p->rays.as<float4>(), p->lens.as<float>(),
-        p->view_proj.as<float>(), p->views.as<JosephView>(), p->n_views, p->nu, p->nv, p->volume,
-        p->weighted.as<float>(), d_volume, accumulate ? 1 : 0, s));
+    if (p->column_bp)
+        YKB_TRY_CUDA(launch_joseph_bp_columns(d_proj, p->rays.as<float4>(), p->lens.as<float>(),
+            p->cols.as<float2>(), p->view_proj.as<float>(), p->views.as<JosephView>(),
+            p->n_views, p->nu, p->nv, p->volume, p->weighted.as<float4>(), d_volume,
+            accumulate ? 1 : 0, s));
+    else
+        YKB_TRY_CUDA(launch_joseph_bp(d_proj, p->rays.as<float4>(), p->lens.as<float>(),
+            p->view_proj.as<float>(), p->views.as<JosephView>(), p->n_views, p->nu, p->nv,
+            p->volume, p->weighted.as<float>(), d_volume, accumulate ? 1 : 0, s));
     return YKB_OK;
 }
 

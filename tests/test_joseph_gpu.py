@@ -246,3 +246,30 @@ def test_siddon_pair_matches_oracle(oracle, cuda_device, case_fn):
     bp2 = plan.backproject_siddon(yd, bp.clone(), accumulate=True)
     assert K.rel_rmse(bp2.cpu().numpy(), 2 * bp.cpu().numpy()) <= 1e-6
     plan.close()
+
+
+@pytest.mark.parametrize("case_fn,columns", [(K.c1_small, True), (K.odd_case, False)])
+def test_column_backprojector_matches_gather(oracle, cuda_device, monkeypatch, case_fn, columns):
+    # axial-column scans take the column backprojector (its per-ray table is
+    # four floats, so the plan's workspace grows); YKB_JOSEPH_BP=gather keeps
+    # the voxel gather.  Both apply the forward projector's weights, summed
+    # in different orders.  A tilted detector's columns are not axial: that
+    # plan keeps the gather by itself.
+    import torch
+    from fdk_cuda_impl_b200.projectors import JosephPlan
+    case = case_fn()
+    views = case.scan.views()
+    y = torch.from_numpy(oracle.normal((len(views), case.scan.rows, case.scan.channels), 12)).cuda()
+    col = JosephPlan(views, case.scan.channels, case.scan.rows, case.grid)
+    monkeypatch.setenv("YKB_JOSEPH_BP", "gather")
+    gat = JosephPlan(views, case.scan.channels, case.scan.rows, case.grid)
+    a, b = col.adjoint(y), gat.adjoint(y)
+    if columns:
+        assert col.workspace_bytes() > gat.workspace_bytes()
+        assert K.rel_rmse(a.cpu().numpy(), b.cpu().numpy()) <= 1e-6
+    else:
+        assert col.workspace_bytes() == gat.workspace_bytes()
+        assert torch.equal(a, b)
+    assert _adjoint_error(col, case.grid, 4) <= ADJ_TOL
+    col.close()
+    gat.close()
