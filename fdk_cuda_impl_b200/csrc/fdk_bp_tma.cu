@@ -406,19 +406,8 @@ __device__ __forceinline__ void bp_tile(const CUtensorMap& map,
         bool ok = true;
         int s = 0, use = 0;  // stage of view k and how often it was used before
         for (int k = 0; k < n_views; ++k, (++s == stages ? (s = 0, ++use) : 0)) {
-            int go = 1;
-            if (lane == 0) {
-                if (use > 0 && !mbar_wait(&empty[s], (use - 1) & 1, pw.limit_ns)) go = 0;
-                if (*(volatile int*)&abort_flag) go = 0;
-            }
-            go = __shfl_sync(0xffffffffu, go, 0);
-            if (!go) { ok = false; break; }
-            if (k == pw.withheld_view) {
-                // test hook: no copy and no arrival for this view, so every
-                // wait for it runs out
-                issued = k + 1;
-                continue;
-            }
+            // the view's box and terms first, while the consumers still read
+            // the stage: only the copy waits for it to be released
             double umin = 1e300, umax = -1e300, vmin = 1e300, vmax = -1e300;
             if (lane < 8) {
                 corner_uv(coef[k], (lane & 1) ? tg.x1 : tg.x0, (lane & 2) ? tg.y1 : tg.y0,
@@ -432,15 +421,31 @@ __device__ __forceinline__ void bp_tile(const CUtensorMap& map,
                 vmin = fmin(vmin, __shfl_xor_sync(0xffffffffu, vmin, o));
                 vmax = fmax(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
             }
+            const Box b = box_from_range(umin, umax, vmin, vmax);
+            TileTerms tt{};
+            if constexpr (COLS)
+                if (lane == 0) tt = tile_terms(coef[k], tg, g.vz, b.c0, b.r0);
+            int go = 1;
+            if (lane == 0) {
+                if (use > 0 && !mbar_wait(&empty[s], (use - 1) & 1, pw.limit_ns)) go = 0;
+                if (*(volatile int*)&abort_flag) go = 0;
+            }
+            go = __shfl_sync(0xffffffffu, go, 0);
+            if (!go) { ok = false; break; }
+            if (k == pw.withheld_view) {
+                // test hook: no copy and no arrival for this view, so every
+                // wait for it runs out
+                issued = k + 1;
+                continue;
+            }
             int aligned = 1;
             if (lane == 0) {
-                const Box b = box_from_range(umin, umax, vmin, vmax);
                 float* dst = ring + static_cast<size_t>(s) * stage_floats;
                 if ((smem_addr(dst) & 127u) != 0 || (b.c0 & 3) != 0) {
                     aligned = 0;  // never issue a copy the hardware would reject
                 } else {
                     boxes[s] = make_int4(b.c0, b.r0, b.c1, b.r1);
-                    if constexpr (COLS) terms[s] = tile_terms(coef[k], tg, g.vz, b.c0, b.r0);
+                    if constexpr (COLS) terms[s] = tt;
                     mbar_arrive_expect_tx(&full[s], box_bytes);
                     tma_load_3d(dst, &map, &full[s], b.c0 + (PAIR ? kPairLead : 0), b.r0, k);
                 }

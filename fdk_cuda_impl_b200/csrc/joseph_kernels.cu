@@ -132,6 +132,116 @@ __global__ void __launch_bounds__(128) joseph_fp_kernel(const float* __restrict_
     *dst = accumulate ? static_cast<float>(*dst + acc) : static_cast<float>(acc);
 }
 
+// Packed FP32 pairs (sm_100 f32x2 arithmetic): both minor axes at once.
+typedef unsigned long long f2;
+__device__ __forceinline__ f2 f2pack(float lo, float hi)
+{
+    f2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void f2unpack(f2 v, float& lo, float& hi)
+{
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f2 f2fma(f2 a, f2 b, f2 c)
+{
+    f2 d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ f2 f2add(f2 a, f2 b)
+{
+    f2 d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f2 f2sub(f2 a, f2 b)
+{
+    f2 d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+
+// 1.5 * 2^23: for |x| < 2^22, x + kMagic holds round(x) in its low mantissa
+// bits; (f - 1/2) + kMagic thus holds floor(f), except at integer f where
+// it may hold f - 1 -- with fraction 1, the same bilinear weights.
+constexpr float kMagic = 12582912.0f;
+constexpr uint32_t kMagicBits = 0x4B400000u;
+
+// The forward projector for main axis x or y, over the zero-bordered slabs
+// (kSlabPad voxels each side of both minor axes).  The same samples and
+// weights as joseph_fp_kernel, without per-tap bounds checks: each minor
+// coordinate is clamped to [-2, n + 1/4] first, which leaves every in-volume
+// sample as it is and sends every other one onto the zero border, so all
+// four taps are always inside the slab.  Floor and fraction come from the
+// rounding constant (both axes in one packed add each), the sample is the
+// bilinear lerp of the four taps, added to the FP64 ray sum.  Lanes walk
+// the warp's slice span together (see joseph_fp_kernel); a slice outside a
+// lane's own range yields zero.
+__global__ void __launch_bounds__(128) joseph_fp_padded_kernel(const float* __restrict__ slab,
+    const JosephView* __restrict__ views, int view0, int nu, int nv, float* __restrict__ proj,
+    int accumulate)
+{
+    const int iu = blockIdx.x * 32 + threadIdx.x;
+    const int iv = blockIdx.y * 4 + threadIdx.y;
+    const int k = view0 + blockIdx.z;
+    const bool pixel = iu < nu && iv < nv;
+    const JosephView& j = views[k];
+    const RayParams r = ray_params(j, min(iu, nu - 1), min(iv, nv - 1));
+    int lo = 0, hi = j.n0 - 1;
+    if (pixel && r.ok) {
+        slice_range(r.a1, r.e1, j.n1, j.n0, lo, hi);
+        slice_range(r.a2, r.e2, j.n2, j.n0, lo, hi);
+    } else {
+        lo = 1; hi = 0;
+    }
+    const int wlo = __reduce_min_sync(0xffffffffu, lo <= hi ? lo : 0x7fffffff);
+    const int whi = __reduce_max_sync(0xffffffffu, lo <= hi ? hi : -1);
+    const int p1 = j.n1 + 2 * kSlabPad;
+    const long plane = static_cast<long>(p1) * (j.n2 + 2 * kSlabPad);
+    // element (i2, i1) of a slice at word (i2 + pad) p1 + i1 + pad, from the
+    // rounding words t1, t2 of floor(f1), floor(f2) (wrapping arithmetic)
+    const uint32_t koff = static_cast<uint32_t>(kSlabPad) * static_cast<uint32_t>(p1 + 1) -
+        kMagicBits * static_cast<uint32_t>(p1 + 1);
+    // upper clamp just past the last voxel: floor n, taps n and n + 1, both
+    // on the border (pad 2)
+    const float hi1 = static_cast<float>(j.n1) + 0.25f, hi2 = static_cast<float>(j.n2) + 0.25f;
+    const f2 A = f2pack(r.a1, r.a2), E = f2pack(r.e1, r.e2);
+    const f2 H = f2pack(0.5f, 0.5f), M = f2pack(kMagic, kMagic);
+    const float half = 0.5f * (j.n0 - 1);
+    // FP64 ray sum: keeps the adjoint identity at the 1e-7 level even where
+    // <Ax, y> cancels to 1e-4 of its terms
+    double acc = 0.0;
+    // unrolled: the four gathers of several samples are in flight at once
+#pragma unroll 4
+    for (int sq = wlo; sq <= whi; ++sq) {
+        const bool in = sq >= lo && sq <= hi;
+        const float c0 = static_cast<float>(sq) - half;
+        float f1, f2v;
+        f2unpack(f2fma(A, f2pack(c0, c0), E), f1, f2v);
+        f1 = in ? fminf(fmaxf(f1, -2.f), hi1) : -2.f;
+        f2v = in ? fminf(fmaxf(f2v, -2.f), hi2) : -2.f;
+        const f2 f = f2pack(f1, f2v);
+        const f2 t = f2add(f2sub(f, H), M);
+        float t1, t2, w1, w2;
+        f2unpack(t, t1, t2);
+        f2unpack(f2sub(f, f2sub(t, M)), w1, w2);
+        const uint32_t off = __float_as_uint(t2) * static_cast<uint32_t>(p1) +
+            __float_as_uint(t1) + koff;
+        const float* p = slab + sq * plane + off;
+        const float p00 = __ldg(p), p10 = __ldg(p + 1);
+        const float p01 = __ldg(p + p1), p11 = __ldg(p + p1 + 1);
+        const float a = fmaf(w1, p10 - p00, p00);
+        const float b = fmaf(w1, p11 - p01, p01);
+        acc += static_cast<double>(fmaf(w2, b - a, a));
+    }
+    acc *= r.len;
+    if (!pixel) return;
+    float* dst = proj + (static_cast<long>(k) * nv + iv) * nu + iu;
+    *dst = accumulate ? static_cast<float>(*dst + acc) : static_cast<float>(acc);
+}
+
 __global__ void __launch_bounds__(128) joseph_ray_table_kernel(const JosephView* __restrict__ views,
     int nu, int nv, float4* __restrict__ rays, float* __restrict__ lens)
 {
@@ -145,14 +255,17 @@ __global__ void __launch_bounds__(128) joseph_ray_table_kernel(const JosephView*
     lens[idx] = r.ok ? r.len : 0.f;
 }
 
-// vol[z][y][x] -> slab[y][z][x] (main axis Y) and slab[x][z][y] (main axis X)
+// vol[z][y][x] -> slab[y][z][x] (main axis Y) and slab[x][z][y] (main axis X),
+// each slice bordered by kSlabPad zero voxels on both minor axes (the
+// borders are zeroed once, when the plan is built, and never written here)
 __global__ void transpose_yzx_kernel(const float* __restrict__ in, int nx, int ny, int nz,
     float* __restrict__ out)
 {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y, z = blockIdx.z;
     if (x >= nx) return;
-    out[(static_cast<long>(y) * nz + z) * nx + x] = in[(static_cast<long>(z) * ny + y) * nx + x];
+    const long row = static_cast<long>(y) * (nz + 2 * kSlabPad) + z + kSlabPad;
+    out[row * (nx + 2 * kSlabPad) + x + kSlabPad] = in[(static_cast<long>(z) * ny + y) * nx + x];
 }
 
 __global__ void transpose_xzy_kernel(const float* __restrict__ in, int nx, int ny, int nz,
@@ -168,7 +281,8 @@ __global__ void transpose_xzy_kernel(const float* __restrict__ in, int nx, int n
     __syncthreads();
     for (int r = threadIdx.y; r < 32; r += blockDim.y) {
         const int x = x0 + r, y = y0 + threadIdx.x;
-        if (x < nx && y < ny) out[(static_cast<long>(x) * nz + z) * ny + y] = tile[threadIdx.x][r];
+        const long row = static_cast<long>(x) * (nz + 2 * kSlabPad) + z + kSlabPad;
+        if (x < nx && y < ny) out[row * (ny + 2 * kSlabPad) + y + kSlabPad] = tile[threadIdx.x][r];
     }
 }
 
@@ -379,26 +493,31 @@ __global__ void joseph_weight_rays4_kernel(const float* __restrict__ proj,
 constexpr int kColThreads = 128;  // 32 x 4 voxel columns a block
 
 template <int ZC>
-__global__ void __launch_bounds__(kColThreads) joseph_bp_column_kernel(
+__global__ void __launch_bounds__(kColThreads, 7) joseph_bp_column_kernel(
     const float4* __restrict__ w4, const float2* __restrict__ cols,
     const ViewProj* __restrict__ vp, const JosephView* __restrict__ views, int n_views, int nu,
     int nv, int nx, int ny, int nz, float* __restrict__ vol, int accumulate)
 {
-    // slot q + 1 holds voxel z0 + q; slots 0 and ZC + 1 catch the half of a
-    // ray's pair that falls just outside the stack
+    // per view, FP32: slot q + 1 holds voxel z0 + q; slots 0 and ZC + 1
+    // catch the half of a ray's pair that falls just outside the stack.
+    // Over views, FP64, also in shared memory (registers stay few, so that
+    // enough warps are resident to cover the ray loads).
     __shared__ float part[(ZC + 2) * kColThreads];
+    __shared__ double total[ZC * kColThreads];
     const int tid = threadIdx.y * 32 + threadIdx.x;
     float* my = part + tid;
+    double* mine = total + tid;
 #pragma unroll
     for (int q = 0; q < ZC + 2; ++q) my[q * kColThreads] = 0.f;
+#pragma unroll
+    for (int q = 0; q < ZC; ++q) mine[q * kColThreads] = 0.0;
     const int x = blockIdx.x * 32 + threadIdx.x;
     const int y = blockIdx.y * 4 + threadIdx.y;
     const int z0 = blockIdx.z * ZC;
     if (x >= nx || y >= ny) return;
-    const float zlo = static_cast<float>(z0 - 1), zhi = static_cast<float>(z0 + ZC - 1);
-    double acc[ZC];
-#pragma unroll
-    for (int q = 0; q < ZC; ++q) acc[q] = 0.0;
+    // slot of floor(f2) + 1 from the rounding word of f2 - 1/2 (wrapping)
+    const uint32_t slot0 = kMagicBits + static_cast<uint32_t>(z0 - 1);
+    const f2 H = f2pack(0.5f, 0.5f), M = f2pack(kMagic, kMagic);
     for (int k = 0; k < n_views; ++k) {
         const JosephView& j = views[k];
         const int s = j.axis == 0 ? x : y, j1 = j.axis == 0 ? y : x;
@@ -417,23 +536,47 @@ __global__ void __launch_bounds__(kColThreads) joseph_bp_column_kernel(
             const float h1 = fl1 == j1f ? 1.f - w1 : (fl1 + 1.f == j1f ? w1 : 0.f);
             if (h1 == 0.f) continue;
             const float4* r = w4 + (static_cast<long>(k) * nv + v0) * nu + iu;
-#pragma unroll 2
-            for (int iv = v0; iv <= v1; ++iv, r += nu) {
-                const float4 q = __ldg(r);
-                const float f2 = fmaf(q.x, c0, q.y);
-                const float fl2 = floorf(f2);
-                if (!(fl2 >= zlo && fl2 <= zhi)) continue;
-                const float w2 = f2 - fl2;
-                const float t = q.z * h1;
-                float* p = my + (static_cast<int>(fl2) - z0 + 1) * kColThreads;
-                p[0] = fmaf(t, 1.f - w2, p[0]);
-                p[kColThreads] = fmaf(t, w2, p[kColThreads]);
+            int iv = v0;
+            // two rays per step, their floor and fraction in packed pairs
+            for (; iv + 1 <= v1; iv += 2, r += 2 * nu) {
+                const float4 qa = __ldg(r), qb = __ldg(r + nu);
+                const f2 f = f2pack(fmaf(qa.x, c0, qa.y), fmaf(qb.x, c0, qb.y));
+                const f2 t = f2add(f2sub(f, H), M);
+                float ta, tb, wa, wb;
+                f2unpack(t, ta, tb);
+                f2unpack(f2sub(f, f2sub(t, M)), wa, wb);
+                const uint32_t sa = __float_as_uint(ta) - slot0, sb = __float_as_uint(tb) - slot0;
+                if (sa <= static_cast<uint32_t>(ZC)) {
+                    const float tt = qa.z * h1;
+                    float* p = my + sa * kColThreads;
+                    p[0] = fmaf(tt, 1.f - wa, p[0]);
+                    p[kColThreads] = fmaf(tt, wa, p[kColThreads]);
+                }
+                if (sb <= static_cast<uint32_t>(ZC)) {
+                    const float tt = qb.z * h1;
+                    float* p = my + sb * kColThreads;
+                    p[0] = fmaf(tt, 1.f - wb, p[0]);
+                    p[kColThreads] = fmaf(tt, wb, p[kColThreads]);
+                }
+            }
+            if (iv <= v1) {
+                const float4 qa = __ldg(r);
+                const float fa = fmaf(qa.x, c0, qa.y);
+                const float ta = (fa - 0.5f) + kMagic;
+                const float wa = fa - (ta - kMagic);
+                const uint32_t sa = __float_as_uint(ta) - slot0;
+                if (sa <= static_cast<uint32_t>(ZC)) {
+                    const float tt = qa.z * h1;
+                    float* p = my + sa * kColThreads;
+                    p[0] = fmaf(tt, 1.f - wa, p[0]);
+                    p[kColThreads] = fmaf(tt, wa, p[kColThreads]);
+                }
             }
         }
 #pragma unroll
         for (int q = 0; q < ZC; ++q) {
             float* p = my + (q + 1) * kColThreads;
-            acc[q] += static_cast<double>(*p);
+            mine[q * kColThreads] += static_cast<double>(*p);
             *p = 0.f;
         }
         my[0] = 0.f;
@@ -444,7 +587,8 @@ __global__ void __launch_bounds__(kColThreads) joseph_bp_column_kernel(
     for (int q = 0; q < ZC; ++q) {
         if (z0 + q >= nz) break;
         float* dst = vol + (z0 + q) * plane + static_cast<long>(y) * nx + x;
-        *dst = accumulate ? static_cast<float>(*dst + acc[q]) : static_cast<float>(acc[q]);
+        const double a = mine[q * kColThreads];
+        *dst = accumulate ? static_cast<float>(*dst + a) : static_cast<float>(a);
     }
 }
 
@@ -508,8 +652,12 @@ cudaError_t launch_joseph_fp(const float* slabs[3], const JosephView* views,
         while (done < end) {
             const int count = min(end - done, 65535);
             const dim3 grid((nu + 31) / 32, (nv + 3) / 4, count);
-            joseph_fp_kernel<<<grid, dim3(32, 4), 0, s>>>(slabs[axis], views, done, nu, nv, proj,
-                accumulate);
+            if (axis == 2)
+                joseph_fp_kernel<<<grid, dim3(32, 4), 0, s>>>(slabs[axis], views, done, nu, nv,
+                    proj, accumulate);
+            else
+                joseph_fp_padded_kernel<<<grid, dim3(32, 4), 0, s>>>(slabs[axis], views, done, nu,
+                    nv, proj, accumulate);
             const cudaError_t e = cudaGetLastError();
             if (e != cudaSuccess) return e;
             done += count;

@@ -729,14 +729,13 @@ YKB_API ykb_status ykb_joseph_plan_create(const ykb_cone_view* views, int n_view
         }
     }
     const size_t rays = static_cast<size_t>(n_views) * nu * nv;
-    const size_t vol_bytes = volume_elems(*volume) * sizeof(float);
     cudaError_t e;
     if ((e = p->views.alloc(sizeof(JosephView) * n_views)) != cudaSuccess ||
         (e = p->view_proj.alloc(sizeof(float) * vp.size())) != cudaSuccess ||
         (e = p->rays.alloc(sizeof(float4) * rays)) != cudaSuccess ||
         (e = p->lens.alloc(sizeof(float) * rays)) != cudaSuccess ||
-        (need_y && (e = p->slab_y.alloc(vol_bytes)) != cudaSuccess) ||
-        (need_x && (e = p->slab_x.alloc(vol_bytes)) != cudaSuccess)) {
+        (need_y && (e = p->slab_y.alloc(sizeof(float) * joseph_slab_elems(*volume, 1))) != cudaSuccess) ||
+        (need_x && (e = p->slab_x.alloc(sizeof(float) * joseph_slab_elems(*volume, 0))) != cudaSuccess)) {
         delete p;
         return cuda_status(e, "cudaMalloc (Joseph plan)");
     }
@@ -753,8 +752,12 @@ YKB_API ykb_status ykb_joseph_plan_create(const ykb_cone_view* views, int n_view
         delete p;
         return cuda_status(e, "cudaStreamCreate");
     }
-    e = launch_joseph_ray_table(p->views.as<JosephView>(), n_views, nu, nv, p->rays.as<float4>(),
-        p->lens.as<float>(), s);
+    // the slabs' zero borders, written once (the transposes fill the interior)
+    if (p->slab_y.ptr) e = cudaMemsetAsync(p->slab_y.ptr, 0, p->slab_y.bytes, s);
+    if (e == cudaSuccess && p->slab_x.ptr) e = cudaMemsetAsync(p->slab_x.ptr, 0, p->slab_x.bytes, s);
+    if (e == cudaSuccess)
+        e = launch_joseph_ray_table(p->views.as<JosephView>(), n_views, nu, nv,
+            p->rays.as<float4>(), p->lens.as<float>(), s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     // the column backprojector when every view's main axis is x or y and its
     // detector columns are axial (YKB_JOSEPH_BP=gather keeps the gather)

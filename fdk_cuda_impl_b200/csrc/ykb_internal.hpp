@@ -240,6 +240,15 @@ cudaError_t launch_fdk_pairify(const float* in, int ld_in, long rows, int nu, fl
     int ldp, cudaStream_t s);
 
 // Joseph
+// zero voxels bordering each slice of the transposed slabs on both minor axes
+constexpr int kSlabPad = 2;
+// slab of main axis x ([x][z][y]) or y ([y][z][x]) with its zero border
+inline size_t joseph_slab_elems(const ykb_volume& v, int axis)
+{
+    const size_t n0 = static_cast<size_t>(axis == 0 ? v.nx : v.ny);
+    const size_t n1 = static_cast<size_t>(axis == 0 ? v.ny : v.nx) + 2 * kSlabPad;
+    return n0 * (static_cast<size_t>(v.nz) + 2 * kSlabPad) * n1;
+}
 cudaError_t launch_joseph_transpose(const float* vol, int nx, int ny, int nz,
     float* vol_yzx, float* vol_xzy, cudaStream_t s);
 cudaError_t launch_joseph_fp(const float* slabs[3], const JosephView* views,
