@@ -3,11 +3,15 @@
 // Same arithmetic as fdk_bp_kernel in fdk_kernels.cu (the math of
 // .../FDK/kernels/YkFDKBpKernels.cu:112-209 with exact software bilinear
 // weights), organised for Blackwell:
-//   * a CTA owns a 16x16x48 voxel tile; each of its 256 consumer threads walks
-//     a 48-voxel z-column and keeps the 48 sums in registers over all views
-//     (the longer the column, the more voxels share the per-view column
-//     terms; 48 sums still fit two CTAs per SM); a remainder of at most 32
-//     slices runs as 32-voxel columns, the same launch's last z layer;
+//   * a CTA owns a 16x32x64 voxel tile, one CTA per SM; each of its 512
+//     consumer threads walks a 64-voxel z-column and keeps the 64 sums in
+//     registers over all views (the longer the column, the more voxels share
+//     the per-view column terms); a remainder of at most 32 slices runs as
+//     32-voxel columns, the same launch's last z layer.  Against two CTAs of
+//     16x16x48 per SM: the same warps per SM, a third more voxels per
+//     column, and one ring of ~200 KB whose stages each feed twice the
+//     columns, so the copies run further ahead of the consumers (62.2 ->
+//     60.4 ms on the 512^3 x 720 x 768^2 workload);
 //   * one producer warp computes, per view, the detector box covering the
 //     tile's footprint (+1 bilinear tap, +1 pixel margin) and loads it with
 //     cp.async.bulk.tensor (3D tile mode, this GPU's memory only, no
@@ -37,7 +41,7 @@
 namespace ykb {
 namespace {
 
-constexpr int TX = 16, TY = 16, ZT = 48;
+constexpr int TX = 16, TY = 32, ZT = 64;
 constexpr int kZTail = 32;  // column length of a short last z tile
 constexpr int NCONS = TX * TY;          // consumer threads
 constexpr int NCWARPS = NCONS / 32;
@@ -251,7 +255,7 @@ __device__ __forceinline__ Box box_from_range(double umin, double umax, double v
 
 struct TileGeom {
     double x0, x1, y0, y1, z0, z1;
-    double xc, yc;  // centre of the nominal 16x16 tile (reference point of its column terms)
+    double xc, yc;  // centre of the nominal TX x TY tile (reference point of its column terms)
 };
 
 __device__ __forceinline__ TileGeom tile_geom(const VolumeGrid& g, int bx, int by, int za, int zc)
@@ -353,8 +357,8 @@ __device__ __forceinline__ float rcp_approx(float x)
     return r;
 }
 
-// Shared-memory ring budget of one CTA; two CTAs share an SM.
-constexpr size_t kRingBudget = 108 * 1024;
+// Shared-memory ring budget of the one CTA of an SM.
+constexpr size_t kRingBudget = 200 * 1024;
 
 // PSEUDO: the weight of the pseudo-matched backprojection instead of the FDK
 // depth weight (tap pairs only)
@@ -516,7 +520,7 @@ __device__ __forceinline__ void bp_tile(const CUtensorMap& map,
             const float2 t3 = *reinterpret_cast<const float2*>(&T.gp1);
             const float den = fmaf(t2.x, dy, fmaf(t1.w, dx, t1.z));
             float rd = rcp_approx(den);
-            rd = fmaf(rd, fmaf(-den, rd, 1.f), rd);  // one Newton step: vs walks 48 slices
+            rd = fmaf(rd, fmaf(-den, rd, 1.f), rd);  // one Newton step: vs walks 64 slices
             float u = fmaf(fmaf(t0.z, dy, t0.y * dx), rd, t0.x);
             float vbq = fmaf(fmaf(t1.y, dy, t1.x * dx), rd, t0.w);
             float vs = t2.y * rd;
@@ -762,8 +766,11 @@ __device__ __forceinline__ void bp_tile(const CUtensorMap& map,
 // blockIdx.z < main_tiles: ZT-slice tiles from slice 0; above: kZTail-slice
 // tiles after them (a short last part of the volume).  The short tiles are
 // the grid's last blocks, so they fill the final wave of the long ones.
+// One CTA of 17 warps per SM.  Registers are granted for whole groups of
+// four warps (20 here), which caps a thread at 96: enough for the 64 sums of
+// the axial tap-pair path (a few bytes of spill); the other paths spill more.
 template <int BW, bool AXIAL, bool PAIR, bool PSEUDO>
-__global__ void __launch_bounds__(NTHREADS, 2) fdk_bp_tma_kernel(const __grid_constant__ CUtensorMap map,
+__global__ void __launch_bounds__(NTHREADS, 1) fdk_bp_tma_kernel(const __grid_constant__ CUtensorMap map,
     const FdkViewCoef* __restrict__ coef, int n_views, VolumeGrid g, int BH, int stages,
     float* __restrict__ vol, int accumulate, int* __restrict__ err,
     const PseudoViewCoef* __restrict__ pseudo, int main_tiles, PipelineWait pw)
