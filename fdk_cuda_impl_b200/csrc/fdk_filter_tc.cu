@@ -341,11 +341,19 @@ __global__ void __launch_bounds__(kFilterThreads, 1) ramp_tc_kernel(
 }
 
 // preweighted rows split into BF16 parts (two, or three when part2 is
-// given), rows padded to lda
-__global__ void __launch_bounds__(128) preweight_split_kernel(const void* __restrict__ in, int in_bf16,
-    const FdkPreweightView* __restrict__ pw, const float* __restrict__ parker, int nu, int nv,
-    int lda, __nv_bfloat16* __restrict__ part0, __nv_bfloat16* __restrict__ part1,
-    __nv_bfloat16* __restrict__ part2)
+// given), rows padded to lda.  One block per row.  The cosine weight is
+// D w / |q(iu)| with q(iu) = q0 + iu detU, so |q|^2 = A + iu (B + iu C) with
+// the row's A, B, C in FP64 (two FMAs per pixel instead of the vector), then
+// an FP32 reciprocal square root refined once in FP64.  A thread takes four
+// consecutive pixels: one 16-byte (FP32) or 8-byte (BF16) load when `vec`
+// (the input base and row pitch nu keep them aligned), and one 8-byte store
+// per part.
+struct alignas(8) Bf16x4 { __nv_bfloat16 v[4]; };
+
+__global__ void __launch_bounds__(64) preweight_split_kernel(const void* __restrict__ in,
+    int in_bf16, const FdkPreweightView* __restrict__ pw, const float* __restrict__ parker,
+    int nu, int nv, int lda, int vec, __nv_bfloat16* __restrict__ part0,
+    __nv_bfloat16* __restrict__ part1, __nv_bfloat16* __restrict__ part2)
 {
     const long row = blockIdx.x;
     const int view = static_cast<int>(row / nv);
@@ -354,29 +362,55 @@ __global__ void __launch_bounds__(128) preweight_split_kernel(const void* __rest
     const double qx0 = p.detS[0] + iv * p.detV[0] - p.src[0];
     const double qy0 = p.detS[1] + iv * p.detV[1] - p.src[1];
     const double qz0 = p.detS[2] + iv * p.detV[2] - p.src[2];
+    const double A = qx0 * qx0 + qy0 * qy0 + qz0 * qz0;
+    const double B = 2.0 * (qx0 * p.detU[0] + qy0 * p.detU[1] + qz0 * p.detU[2]);
+    const double Cq = p.detU[0] * p.detU[0] + p.detU[1] * p.detU[1] + p.detU[2] * p.detU[2];
     const double scale = p.dsd * p.wgeom;
-    for (int iu = threadIdx.x; iu < lda; iu += blockDim.x) {
-        float x = 0.f;
-        if (iu < nu && iu >= p.in_lo && iu < p.in_hi) {
-            const double qx = fma(static_cast<double>(iu), p.detU[0], qx0);
-            const double qy = fma(static_cast<double>(iu), p.detU[1], qy0);
-            const double qz = fma(static_cast<double>(iu), p.detU[2], qz0);
-            const double r2 = fmax(qx * qx + qy * qy + qz * qz, 1e-20);
-            double r = rsqrtf(static_cast<float>(r2));
-            r = r * (1.5 - 0.5 * r2 * r * r);
-            const float v = in_bf16
-                ? __bfloat162float(static_cast<const __nv_bfloat16*>(in)[row * nu + iu])
-                : static_cast<const float*>(in)[row * nu + iu];
-            float wt = static_cast<float>(scale * r);
-            if (parker) wt *= parker[static_cast<long>(view) * nu + iu];
-            x = v * wt;
+    const float* prow = parker ? parker + static_cast<long>(view) * nu : nullptr;
+    for (int iu0 = 4 * threadIdx.x; iu0 < lda; iu0 += 4 * blockDim.x) {
+        float v[4] = {0.f, 0.f, 0.f, 0.f};
+        if (vec && iu0 < nu) {
+            if (in_bf16) {
+                const uint2 raw = *reinterpret_cast<const uint2*>(
+                    static_cast<const __nv_bfloat16*>(in) + row * nu + iu0);
+                v[0] = __uint_as_float(raw.x << 16); v[1] = __uint_as_float(raw.x & 0xFFFF0000u);
+                v[2] = __uint_as_float(raw.y << 16); v[3] = __uint_as_float(raw.y & 0xFFFF0000u);
+            } else {
+                const float4 raw = *reinterpret_cast<const float4*>(
+                    static_cast<const float*>(in) + row * nu + iu0);
+                v[0] = raw.x; v[1] = raw.y; v[2] = raw.z; v[3] = raw.w;
+            }
+        } else {
+            for (int e = 0; e < 4; ++e)
+                if (iu0 + e < nu)
+                    v[e] = in_bf16
+                        ? __bfloat162float(static_cast<const __nv_bfloat16*>(in)[row * nu + iu0 + e])
+                        : static_cast<const float*>(in)[row * nu + iu0 + e];
         }
-        const __nv_bfloat16 h = __float2bfloat16_rn(x);
-        const float r1 = x - __bfloat162float(h);  // exact
-        const __nv_bfloat16 m = __float2bfloat16_rn(r1);
-        part0[row * lda + iu] = h;
-        part1[row * lda + iu] = m;
-        if (part2) part2[row * lda + iu] = __float2bfloat16_rn(r1 - __bfloat162float(m));
+        Bf16x4 h0, h1, h2;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const int iu = iu0 + e;
+            float x = 0.f;
+            if (iu < nu && iu >= p.in_lo && iu < p.in_hi) {
+                const double u = static_cast<double>(iu);
+                const double r2 = fmax(fma(fma(Cq, u, B), u, A), 1e-20);
+                double r = rsqrtf(static_cast<float>(r2));
+                r = r * (1.5 - 0.5 * r2 * r * r);
+                float wt = static_cast<float>(scale * r);
+                if (prow) wt *= prow[iu];
+                x = v[e] * wt;
+            }
+            const __nv_bfloat16 h = __float2bfloat16_rn(x);
+            const float r1 = x - __bfloat162float(h);  // exact
+            const __nv_bfloat16 m = __float2bfloat16_rn(r1);
+            h0.v[e] = h;
+            h1.v[e] = m;
+            h2.v[e] = __float2bfloat16_rn(r1 - __bfloat162float(m));
+        }
+        *reinterpret_cast<Bf16x4*>(part0 + row * lda + iu0) = h0;
+        *reinterpret_cast<Bf16x4*>(part1 + row * lda + iu0) = h1;
+        if (part2) *reinterpret_cast<Bf16x4*>(part2 + row * lda + iu0) = h2;
     }
 }
 
@@ -462,8 +496,11 @@ cudaError_t launch_fdk_preweight_split_bf16(const void* proj, int proj_dtype,
 {
     const long rows = static_cast<long>(n_views) * nv;
     if (rows <= 0) return cudaSuccess;
-    preweight_split_kernel<<<static_cast<unsigned>(rows), 128, 0, s>>>(proj,
-        proj_dtype == YKB_DTYPE_BF16 ? 1 : 0, pw, parker, nu, nv, ld, parts[0], parts[1], parts[2]);
+    if (ld % 4 != 0) return cudaErrorInvalidValue;  // rows are padded to whole K chunks
+    const bool bf16 = proj_dtype == YKB_DTYPE_BF16;
+    const int vec = nu % 4 == 0 && reinterpret_cast<uintptr_t>(proj) % (bf16 ? 8 : 16) == 0;
+    preweight_split_kernel<<<static_cast<unsigned>(rows), 64, 0, s>>>(proj, bf16 ? 1 : 0, pw,
+        parker, nu, nv, ld, vec, parts[0], parts[1], parts[2]);
     return cudaGetLastError();
 }
 

@@ -321,16 +321,19 @@ __device__ __forceinline__ float hat_weight(float f, float jf)
     return fmaxf(0.f, 1.f - fabsf(f - jf));
 }
 
-// Detector box of the slice rectangle [j1 - 1, j1 + 1] x [j2lo - 1, j2hi + 1]
-// (voxel-index coordinates on the minor axes of slice c0), from its four
-// projected corners, clipped to the detector; empty when u0 > u1 or v0 > v1.
-__device__ __forceinline__ void footprint_box(const ViewProj& m, const JosephView& j, float c0,
-    int j1, int j2lo, int j2hi, int nu, int nv, int& u0, int& u1, int& v0, int& v1)
+// Detector box of the slice rectangle [j1lo - 1, j1hi + 1] x [j2lo - 1,
+// j2hi + 1] (voxel-index coordinates on the minor axes of slice c0), from its
+// four projected corners, clipped to the detector; empty when u0 > u1 or
+// v0 > v1.  The box of a sub-rectangle lies inside (the map is projective,
+// the rectangle convex, and the 0.05-pixel margin covers the rounding).
+__device__ __forceinline__ void footprint_box_range(const ViewProj& m, const JosephView& j,
+    float c0, int j1lo, int j1hi, int j2lo, int j2hi, int nu, int nv, int& u0, int& u1, int& v0,
+    int& v1)
 {
     float umin = 1e30f, umax = -1e30f, vmin = 1e30f, vmax = -1e30f;
 #pragma unroll
     for (int corner = 0; corner < 4; ++corner) {
-        const float q1 = static_cast<float>(j1 + ((corner & 1) ? 1 : -1)) - 0.5f * (j.n1 - 1);
+        const float q1 = static_cast<float>((corner & 1) ? j1hi + 1 : j1lo - 1) - 0.5f * (j.n1 - 1);
         const float q2 = static_cast<float>((corner & 2) ? j2hi + 1 : j2lo - 1) - 0.5f * (j.n2 - 1);
         float px, py, pz;
         if (j.axis == 0) { px = c0; py = q1; pz = q2; }
@@ -349,6 +352,13 @@ __device__ __forceinline__ void footprint_box(const ViewProj& m, const JosephVie
     u1 = min(nu - 1, static_cast<int>(floorf(umax + margin)));
     v0 = max(0, static_cast<int>(ceilf(vmin - margin)));
     v1 = min(nv - 1, static_cast<int>(floorf(vmax + margin)));
+}
+
+// the box of [j1 - 1, j1 + 1] x [j2lo - 1, j2hi + 1]
+__device__ __forceinline__ void footprint_box(const ViewProj& m, const JosephView& j, float c0,
+    int j1, int j2lo, int j2hi, int nu, int nv, int& u0, int& u1, int& v0, int& v1)
+{
+    footprint_box_range(m, j, c0, j1, j1, j2lo, j2hi, nu, nv, u0, u1, v0, v1);
 }
 
 // One thread gathers ZV voxels stacked along z.  When z is a minor axis of
@@ -429,21 +439,11 @@ __global__ void __launch_bounds__(256) joseph_bp_kernel(const float* __restrict_
 }
 
 // ---------------------------------------------------------------------------
-// Column backprojector, for scans whose detector columns are axial: every
-// view has main axis x or y (so z is minor axis 2) and all rays of a
-// detector column share their minor-1 parameters (a1, e1) bit for bit (the
-// detector's v axis has no component along the main or minor-1 axis; checked
-// on the device when the plan is built).  It applies the same transpose as
-// joseph_bp_kernel with the roles turned around: a thread owns a stack of ZC
-// voxels of one (x, y) column and, per view, walks the candidate detector
-// columns once (the minor-1 weight is a property of the column) and their
-// rays once each, scattering every ray's two minor-2 weights into the stack:
-// about 2.5 columns x 1.3 rays per voxel, each ray touching only the two
-// voxels it reaches, where the gather evaluates every candidate of the box
-// against every voxel of its stack.  The stack is private to its thread
-// (shared memory laid out [slot][thread], one bank per thread, no atomics),
-// so the sums are deterministic: per view in FP32 in ray order, over views
-// in FP64 registers.
+// Axial-column scans: every view has main axis x or y (so z is minor axis 2)
+// and all rays of a detector column share their minor-1 parameters (a1, e1)
+// bit for bit (the detector's v axis has no component along the main or
+// minor-1 axis; checked on the device when the plan is built).  Their
+// matched backprojection is joseph_bp_lines_kernel below.
 // ---------------------------------------------------------------------------
 
 // (a1, e1) of every detector column from its first row.
@@ -478,7 +478,7 @@ __global__ void joseph_column_check_kernel(const float4* __restrict__ rays,
 }
 
 // (a2, e2, value x chord length, 0) per ray: one 16-byte load per ray in the
-// column backprojector.
+// line backprojector.
 __global__ void joseph_weight_rays4_kernel(const float* __restrict__ proj,
     const float4* __restrict__ rays, const float* __restrict__ lens, long n,
     float4* __restrict__ out)
@@ -490,104 +490,180 @@ __global__ void joseph_weight_rays4_kernel(const float* __restrict__ proj,
     }
 }
 
-constexpr int kColThreads = 128;  // 32 x 4 voxel columns a block
+// ---------------------------------------------------------------------------
+// Line backprojector (axial-column scans).  The transpose factors per
+// detector column: voxel (s, j1, j2) of a view gets
+//   sum over columns iu of h1(iu, s, j1) * L(iu, s, j2),
+//   L(iu, s, j2) = sum over rows iv of t(iu, iv) h2(f2(iu, iv, s) - j2),
+// where L, the column's rays splatted onto the z line of slice s, does not
+// depend on j1.  A CTA owns 16 x 16 voxel columns of ZC slices.  Per view it
+// builds, for each of its 16 slices, the lines of the detector columns that
+// reach its 16 minor-1 indices (a warp per slice, a lane per line, each lane
+// walking its column's rays in order: every ray once per slice instead of
+// once per voxel column it touches, about 2.5), then each thread adds the
+// lines of its own column's candidate detector columns, weighted by h1, to
+// its ZC sums.  Weights are the forward projector's; per view the sums are
+// FP32 (lines in ray order, then over detector columns), over views FP64 in
+// shared memory.  Lines live in shared memory as [slice][slot][line], one
+// bank per lane, slices an odd number of words apart (the threads of a warp
+// read up to 16 slices at one line offset); a slice with more than kLineMax
+// lines takes several passes.
+// ---------------------------------------------------------------------------
+constexpr int kLineBlock = 16;    // 16 x 16 voxel columns a CTA
+constexpr int kLineThreads = 256;
+constexpr int kLineMax = 32;      // lines of a slice per pass
+
+// words from one slice's lines to the next
+template <int ZC>
+__host__ __device__ constexpr int line_slice_words() { return (ZC + 2) * kLineMax + 1; }
 
 template <int ZC>
-__global__ void __launch_bounds__(kColThreads, 7) joseph_bp_column_kernel(
+constexpr size_t line_smem_bytes()
+{
+    return sizeof(double) * ZC * kLineThreads + sizeof(float) * kLineBlock * line_slice_words<ZC>() +
+        sizeof(int4) * kLineBlock + 16;
+}
+
+template <int ZC>
+__global__ void __launch_bounds__(kLineThreads, 3) joseph_bp_lines_kernel(
     const float4* __restrict__ w4, const float2* __restrict__ cols,
     const ViewProj* __restrict__ vp, const JosephView* __restrict__ views, int n_views, int nu,
     int nv, int nx, int ny, int nz, float* __restrict__ vol, int accumulate)
 {
-    // per view, FP32: slot q + 1 holds voxel z0 + q; slots 0 and ZC + 1
-    // catch the half of a ray's pair that falls just outside the stack.
-    // Over views, FP64, also in shared memory (registers stay few, so that
-    // enough warps are resident to cover the ray loads).
-    __shared__ float part[(ZC + 2) * kColThreads];
-    __shared__ double total[ZC * kColThreads];
-    const int tid = threadIdx.y * 32 + threadIdx.x;
-    float* my = part + tid;
-    double* mine = total + tid;
+    constexpr int B = kLineBlock, SL = ZC + 2, LM = kLineMax, PS = line_slice_words<ZC>();
+    extern __shared__ __align__(16) unsigned char line_smem[];
+    double* total = reinterpret_cast<double*>(line_smem);                 // [q][thread]
+    float* lines = reinterpret_cast<float*>(total + ZC * kLineThreads);  // [slice][slot][line]
+    int4* pbox = reinterpret_cast<int4*>(                                 // per slice: u0, u1, v0, v1
+        (reinterpret_cast<uintptr_t>(lines + B * PS) + 15) & ~static_cast<uintptr_t>(15));
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tx = tid % B, ty = tid / B;
+    const int X0 = blockIdx.x * B, Y0 = blockIdx.y * B, z0 = blockIdx.z * ZC;
+    const int x = X0 + tx, y = Y0 + ty;
+    const bool mine = x < nx && y < ny;
 #pragma unroll
-    for (int q = 0; q < ZC + 2; ++q) my[q * kColThreads] = 0.f;
-#pragma unroll
-    for (int q = 0; q < ZC; ++q) mine[q * kColThreads] = 0.0;
-    const int x = blockIdx.x * 32 + threadIdx.x;
-    const int y = blockIdx.y * 4 + threadIdx.y;
-    const int z0 = blockIdx.z * ZC;
-    if (x >= nx || y >= ny) return;
+    for (int q = 0; q < ZC; ++q) total[q * kLineThreads + tid] = 0.0;
     // slot of floor(f2) + 1 from the rounding word of f2 - 1/2 (wrapping)
     const uint32_t slot0 = kMagicBits + static_cast<uint32_t>(z0 - 1);
     const f2 H = f2pack(0.5f, 0.5f), M = f2pack(kMagic, kMagic);
     for (int k = 0; k < n_views; ++k) {
         const JosephView& j = views[k];
-        const int s = j.axis == 0 ? x : y, j1 = j.axis == 0 ? y : x;
-        const float c0 = static_cast<float>(s) - 0.5f * (j.n0 - 1);
-        int u0, u1, v0, v1;
-        footprint_box(vp[k], j, c0, j1, z0, z0 + ZC - 1, nu, nv, u0, u1, v0, v1);
+        const bool ax0 = j.axis == 0;
+        const int S0 = ax0 ? X0 : Y0, J0 = ax0 ? Y0 : X0;  // first slice, first minor-1 index
+        const int nS = min(B, j.n0 - S0), nJ = min(B, j.n1 - J0);
+        const float half = 0.5f * (j.n0 - 1);
+        if (tid < B) {
+            int u0 = 0, u1 = -1, v0 = 0, v1 = -1;
+            if (tid < nS)
+                footprint_box_range(vp[k], j, static_cast<float>(S0 + tid) - half, J0,
+                    J0 + nJ - 1, z0, z0 + ZC - 1, nu, nv, u0, u1, v0, v1);
+            pbox[tid] = make_int4(u0, u1, v0, v1);
+        }
+        __syncthreads();
+        int passes = 0;
+#pragma unroll
+        for (int p = 0; p < B; ++p) passes = max(passes, (pbox[p].y - pbox[p].x + LM) / LM);
+        // this thread's voxel column: its slice, minor-1 index, candidates
+        const int pl = ax0 ? tx : ty, j1 = ax0 ? y : x;
+        const float c0 = static_cast<float>(S0 + pl) - half;
+        int cu0 = 0, cu1 = -1, cv0, cv1;
+        if (mine) footprint_box(vp[k], j, c0, j1, z0, z0 + ZC - 1, nu, nv, cu0, cu1, cv0, cv1);
         const float j1f = static_cast<float>(j1);
         const float2* ck = cols + static_cast<long>(k) * nu;
-        for (int iu = u0; iu <= u1; ++iu) {
-            // the forward projector's minor-1 weights: 1 - w to floor(f1),
-            // w to floor(f1) + 1
-            const float2 ce = __ldg(ck + iu);
-            const float f1 = fmaf(ce.x, c0, ce.y);
-            const float fl1 = floorf(f1);
-            const float w1 = f1 - fl1;
-            const float h1 = fl1 == j1f ? 1.f - w1 : (fl1 + 1.f == j1f ? w1 : 0.f);
-            if (h1 == 0.f) continue;
-            const float4* r = w4 + (static_cast<long>(k) * nv + v0) * nu + iu;
-            int iv = v0;
-            // two rays per step, their floor and fraction in packed pairs
-            for (; iv + 1 <= v1; iv += 2, r += 2 * nu) {
-                const float4 qa = __ldg(r), qb = __ldg(r + nu);
-                const f2 f = f2pack(fmaf(qa.x, c0, qa.y), fmaf(qb.x, c0, qb.y));
-                const f2 t = f2add(f2sub(f, H), M);
-                float ta, tb, wa, wb;
-                f2unpack(t, ta, tb);
-                f2unpack(f2sub(f, f2sub(t, M)), wa, wb);
-                const uint32_t sa = __float_as_uint(ta) - slot0, sb = __float_as_uint(tb) - slot0;
-                if (sa <= static_cast<uint32_t>(ZC)) {
-                    const float tt = qa.z * h1;
-                    float* p = my + sa * kColThreads;
-                    p[0] = fmaf(tt, 1.f - wa, p[0]);
-                    p[kColThreads] = fmaf(tt, wa, p[kColThreads]);
+        float acc[ZC];
+#pragma unroll
+        for (int q = 0; q < ZC; ++q) acc[q] = 0.f;
+        for (int pass = 0; pass < passes; ++pass) {
+            // ---- lines: warp w builds slices w and w + 8, lane = line
+            for (int sp = warp; sp < B; sp += kLineThreads / 32) {
+                const int4 b = pbox[sp];
+                float* L = lines + sp * PS + lane;
+#pragma unroll
+                for (int q = 0; q < SL; ++q) L[q * LM] = 0.f;
+                const int iu = b.x + pass * LM + lane;
+                if (iu > b.y) continue;
+                const float cs = static_cast<float>(S0 + sp) - half;
+                const float4* r = w4 + (static_cast<long>(k) * nv + b.z) * nu + iu;
+                int iv = b.z;
+                auto splat = [&](const float4& qa, const float4& qb) {
+                    const f2 f = f2pack(fmaf(qa.x, cs, qa.y), fmaf(qb.x, cs, qb.y));
+                    const f2 t = f2add(f2sub(f, H), M);
+                    float ta, tb, wa, wb;
+                    f2unpack(t, ta, tb);
+                    f2unpack(f2sub(f, f2sub(t, M)), wa, wb);
+                    const uint32_t sa = __float_as_uint(ta) - slot0, sb = __float_as_uint(tb) - slot0;
+                    if (sa <= static_cast<uint32_t>(ZC)) {
+                        float* o = L + sa * LM;
+                        o[0] = fmaf(qa.z, 1.f - wa, o[0]);
+                        o[LM] = fmaf(qa.z, wa, o[LM]);
+                    }
+                    if (sb <= static_cast<uint32_t>(ZC)) {
+                        float* o = L + sb * LM;
+                        o[0] = fmaf(qb.z, 1.f - wb, o[0]);
+                        o[LM] = fmaf(qb.z, wb, o[LM]);
+                    }
+                };
+                // eight rays per step: their loads are in flight together
+                for (; iv + 7 <= b.w; iv += 8, r += 8 * nu) {
+                    const float4 qa = __ldg(r), qb = __ldg(r + nu);
+                    const float4 qc = __ldg(r + 2 * nu), qd = __ldg(r + 3 * nu);
+                    const float4 qe = __ldg(r + 4 * nu), qf = __ldg(r + 5 * nu);
+                    const float4 qg = __ldg(r + 6 * nu), qh = __ldg(r + 7 * nu);
+                    splat(qa, qb);
+                    splat(qc, qd);
+                    splat(qe, qf);
+                    splat(qg, qh);
                 }
-                if (sb <= static_cast<uint32_t>(ZC)) {
-                    const float tt = qb.z * h1;
-                    float* p = my + sb * kColThreads;
-                    p[0] = fmaf(tt, 1.f - wb, p[0]);
-                    p[kColThreads] = fmaf(tt, wb, p[kColThreads]);
+                for (; iv + 3 <= b.w; iv += 4, r += 4 * nu) {
+                    const float4 qa = __ldg(r), qb = __ldg(r + nu);
+                    const float4 qc = __ldg(r + 2 * nu), qd = __ldg(r + 3 * nu);
+                    splat(qa, qb);
+                    splat(qc, qd);
+                }
+                for (; iv + 1 <= b.w; iv += 2, r += 2 * nu) splat(__ldg(r), __ldg(r + nu));
+                if (iv <= b.w) {
+                    const float4 qa = __ldg(r);
+                    const float fa = fmaf(qa.x, cs, qa.y);
+                    const float ta = (fa - 0.5f) + kMagic;
+                    const float wa = fa - (ta - kMagic);
+                    const uint32_t sa = __float_as_uint(ta) - slot0;
+                    if (sa <= static_cast<uint32_t>(ZC)) {
+                        float* o = L + sa * LM;
+                        o[0] = fmaf(qa.z, 1.f - wa, o[0]);
+                        o[LM] = fmaf(qa.z, wa, o[LM]);
+                    }
                 }
             }
-            if (iv <= v1) {
-                const float4 qa = __ldg(r);
-                const float fa = fmaf(qa.x, c0, qa.y);
-                const float ta = (fa - 0.5f) + kMagic;
-                const float wa = fa - (ta - kMagic);
-                const uint32_t sa = __float_as_uint(ta) - slot0;
-                if (sa <= static_cast<uint32_t>(ZC)) {
-                    const float tt = qa.z * h1;
-                    float* p = my + sa * kColThreads;
-                    p[0] = fmaf(tt, 1.f - wa, p[0]);
-                    p[kColThreads] = fmaf(tt, wa, p[kColThreads]);
+            __syncthreads();
+            // ---- this column: its candidates among this pass's lines
+            if (mine) {
+                const int base = pbox[pl].x + pass * LM;
+                const int lo = max(cu0, base), hi = min(min(cu1, pbox[pl].y), base + LM - 1);
+                const float* Lp = lines + pl * PS - base;
+                for (int iu = lo; iu <= hi; ++iu) {
+                    // the forward projector's minor-1 weights
+                    const float2 ce = __ldg(ck + iu);
+                    const float f1 = fmaf(ce.x, c0, ce.y);
+                    const float fl1 = floorf(f1);
+                    const float w1 = f1 - fl1;
+                    const float h1 = fl1 == j1f ? 1.f - w1 : (fl1 + 1.f == j1f ? w1 : 0.f);
+                    if (h1 == 0.f) continue;
+#pragma unroll
+                    for (int q = 0; q < ZC; ++q) acc[q] = fmaf(h1, Lp[(q + 1) * LM + iu], acc[q]);
                 }
             }
+            __syncthreads();
         }
 #pragma unroll
-        for (int q = 0; q < ZC; ++q) {
-            float* p = my + (q + 1) * kColThreads;
-            mine[q * kColThreads] += static_cast<double>(*p);
-            *p = 0.f;
-        }
-        my[0] = 0.f;
-        my[(ZC + 1) * kColThreads] = 0.f;
+        for (int q = 0; q < ZC; ++q) total[q * kLineThreads + tid] += static_cast<double>(acc[q]);
     }
+    if (!mine) return;
     const long plane = static_cast<long>(nx) * ny;
 #pragma unroll
     for (int q = 0; q < ZC; ++q) {
         if (z0 + q >= nz) break;
         float* dst = vol + (z0 + q) * plane + static_cast<long>(y) * nx + x;
-        const double a = mine[q * kColThreads];
+        const double a = total[q * kLineThreads + tid];
         *dst = accumulate ? static_cast<float>(*dst + a) : static_cast<float>(a);
     }
 }
@@ -605,7 +681,7 @@ cudaError_t launch_joseph_column_table(const float4* rays, int n_views, int nu, 
     return cudaGetLastError();
 }
 
-cudaError_t launch_joseph_bp_columns(const float* proj, const float4* rays, const float* lens,
+cudaError_t launch_joseph_bp_lines(const float* proj, const float4* rays, const float* lens,
     const float2* cols, const float* view_proj, const JosephView* views, int n_views, int nu,
     int nv, const ykb_volume& vol, float4* weighted4, float* out, int accumulate, cudaStream_t s)
 {
@@ -614,10 +690,15 @@ cudaError_t launch_joseph_bp_columns(const float* proj, const float4* rays, cons
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     constexpr int ZC = 16;
-    const dim3 grid((vol.nx + 31) / 32, (vol.ny + 3) / 4, (vol.nz + ZC - 1) / ZC);
-    joseph_bp_column_kernel<ZC><<<grid, dim3(32, 4), 0, s>>>(weighted4, cols,
-        reinterpret_cast<const ViewProj*>(view_proj), views, n_views, nu, nv, vol.nx, vol.ny,
-        vol.nz, out, accumulate);
+    auto k = joseph_bp_lines_kernel<ZC>;
+    constexpr size_t smem = line_smem_bytes<ZC>();
+    if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+             static_cast<int>(smem))) != cudaSuccess)
+        return e;
+    const dim3 grid((vol.nx + kLineBlock - 1) / kLineBlock, (vol.ny + kLineBlock - 1) / kLineBlock,
+        (vol.nz + ZC - 1) / ZC);
+    k<<<grid, kLineThreads, smem, s>>>(weighted4, cols, reinterpret_cast<const ViewProj*>(view_proj),
+        views, n_views, nu, nv, vol.nx, vol.ny, vol.nz, out, accumulate);
     return cudaGetLastError();
 }
 

@@ -759,7 +759,7 @@ YKB_API ykb_status ykb_joseph_plan_create(const ykb_cone_view* views, int n_view
         e = launch_joseph_ray_table(p->views.as<JosephView>(), n_views, nu, nv,
             p->rays.as<float4>(), p->lens.as<float>(), s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    // the column backprojector when every view's main axis is x or y and its
+    // the line backprojector when every view's main axis is x or y and its
     // detector columns are axial (YKB_JOSEPH_BP=gather keeps the gather)
     bool columns = std::none_of(p->axes.begin(), p->axes.end(), [](int a) { return a == 2; });
     if (const char* env = std::getenv("YKB_JOSEPH_BP"))
@@ -1047,7 +1047,7 @@ YKB_API ykb_status ykb_joseph_bp(ykb_joseph_plan* p, const float* d_proj, float*
     DeviceGuard guard(p->device);
     const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     if (p->column_bp)
-        YKB_TRY_CUDA(launch_joseph_bp_columns(d_proj, p->rays.as<float4>(), p->lens.as<float>(),
+        YKB_TRY_CUDA(launch_joseph_bp_lines(d_proj, p->rays.as<float4>(), p->lens.as<float>(),
             p->cols.as<float2>(), p->view_proj.as<float>(), p->views.as<JosephView>(),
             p->n_views, p->nu, p->nv, p->volume, p->weighted.as<float4>(), d_volume,
             accumulate ? 1 : 0, s));

@@ -271,12 +271,13 @@ cudaError_t launch_siddon_fp(const float* vol, const ykb_cone_view* views, int n
 cudaError_t launch_siddon_bp(const float* proj, const ykb_cone_view* views, int n_views, int nu,
     int nv, const VolumeGrid& g, float* vol, int accumulate, cudaStream_t s);
 // (a1, e1) of every detector column from its first row into cols[n][nu];
-// flag[0] = 1 when any ray of a column differs (the column backprojector
+// flag[0] = 1 when any ray of a column differs (the line backprojector
 // then does not apply)
 cudaError_t launch_joseph_column_table(const float4* rays, int n_views, int nu, int nv,
     float2* cols, int* flag, cudaStream_t s);
-// matched backprojection for axial-column scans (see launch_joseph_column_table)
-cudaError_t launch_joseph_bp_columns(const float* proj, const float4* rays, const float* lens,
+// matched backprojection for axial-column scans (see launch_joseph_column_table):
+// weighted4 receives (a2, e2, input x chord length, 0) per ray
+cudaError_t launch_joseph_bp_lines(const float* proj, const float4* rays, const float* lens,
     const float2* cols, const float* view_proj, const JosephView* views, int n_views, int nu,
     int nv, const ykb_volume& vol, float4* weighted4, float* out, int accumulate, cudaStream_t s);
 cudaError_t launch_joseph_bp(const float* proj, const float4* rays, const float* lens,
@@ -351,7 +352,7 @@ struct ykb_joseph_plan {
     // backprojector input x chord length: float[n*nv*nu], or for the column
     // backprojector float4 (a2, e2, input x chord length, 0)
     ykb::DeviceBuffer weighted;
-    bool column_bp = false;      // every view's detector columns are axial
+    bool column_bp = false;      // every view's detector columns are axial (line backprojector)
     ykb::DeviceBuffer cols;      // float2[n*nu]: (a1, e1) per detector column
     ykb::DeviceBuffer slab_y, slab_x;  // transposed volume copies
     ykb::DeviceBuffer world_views;     // ykb_cone_view[n] (Siddon), uploaded on first use

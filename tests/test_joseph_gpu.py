@@ -249,8 +249,8 @@ def test_siddon_pair_matches_oracle(oracle, cuda_device, case_fn):
 
 
 @pytest.mark.parametrize("case_fn,columns", [(K.c1_small, True), (K.odd_case, False)])
-def test_column_backprojector_matches_gather(oracle, cuda_device, monkeypatch, case_fn, columns):
-    # axial-column scans take the column backprojector (its per-ray table is
+def test_line_backprojector_matches_gather(oracle, cuda_device, monkeypatch, case_fn, columns):
+    # axial-column scans take the line backprojector (its per-ray table is
     # four floats, so the plan's workspace grows); YKB_JOSEPH_BP=gather keeps
     # the voxel gather.  Both apply the forward projector's weights, summed
     # in different orders.  A tilted detector's columns are not axial: that
@@ -272,4 +272,27 @@ def test_column_backprojector_matches_gather(oracle, cuda_device, monkeypatch, c
         assert torch.equal(a, b)
     assert _adjoint_error(col, case.grid, 4) <= ADJ_TOL
     col.close()
+    gat.close()
+
+
+def test_line_backprojector_many_lines_per_slice(oracle, cuda_device, monkeypatch):
+    # pixels an eighth of a voxel at the isocentre: a CTA slice spans about
+    # 140 detector columns, so the line backprojector takes several passes of
+    # 32 lines; odd volume sizes leave partial CTAs in x, y and z
+    import torch
+    from fdk_cuda_impl_b200.projectors import JosephPlan
+    scan = CircularScan(12, 12, 300.0, 600.0, 160, 120, 0.25, 0.25)
+    grid = VolumeGrid(37, 29, 21, (1.0, 1.0, 1.0))
+    views = scan.views()
+    y = torch.from_numpy(oracle.normal((len(views), 120, 160), 21)).cuda()
+    lines = JosephPlan(views, 160, 120, grid)
+    monkeypatch.setenv("YKB_JOSEPH_BP", "gather")
+    gat = JosephPlan(views, 160, 120, grid)
+    assert lines.workspace_bytes() > gat.workspace_bytes()
+    a, b = lines.adjoint(y), gat.adjoint(y)
+    assert K.rel_rmse(a.cpu().numpy(), b.cpu().numpy()) <= 1e-6
+    ref = oracle.joseph_bp(views, 160, 120, K.oracle_volume(oracle, grid), y.cpu().numpy())
+    assert K.rel_rmse(a.cpu().numpy(), ref) <= FP32_TOL
+    assert _adjoint_error(lines, grid, 5) <= ADJ_TOL
+    lines.close()
     gat.close()
