@@ -606,10 +606,12 @@ def main():
     bp_bytes = 4.0 * w.n_views * w.n_det ** 2 + 4.0 * w.n_vox ** 3
     achieved = bp_bytes / (bp_step_ms * 1e-3) / 1e9
     # DRAM traffic of one launch: ncu (dram__bytes_read + write) on the
-    # 256^3 x 360 x 384^2 case gave 830.8 MB against 279.4 MB compulsory
-    # (tap-pair rows are 8 B per sample; L2 misses re-read some rows);
-    # scaled by the compulsory bytes, which grow in proportion
-    traffic = 830.8e6 * bp_bytes / (4.0 * 360 * 384 * 384 + 4.0 * 256 ** 3)
+    # 256^3 x 360 x 384^2 case gave 703.4 + 64.8 MB against 279.4 MB
+    # compulsory (tap-pair rows are 8 B per sample; L2 misses re-read some
+    # rows); scaled by the compulsory bytes of one launch, which grow in
+    # proportion
+    traffic = 768.2e6 * (bp_bytes / stages["groups_per_step"]) / (
+        4.0 * 360 * 384 * 384 + 4.0 * 256 ** 3)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "peak_source": peak_src,
                 "traffic_source": "ncu 256^3x360x384^2 capture scaled by compulsory bytes",

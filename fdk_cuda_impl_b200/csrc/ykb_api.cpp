@@ -348,15 +348,51 @@ ykb_status filter_chunk_(ykb_fdk_plan* p, const void* proj, int proj_dtype, int 
     if (p->tc_filter) {
         const size_t part = static_cast<size_t>(p->batch_capacity) * p->nv * p->lda;
         __nv_bfloat16* a0 = p->work_a.as<__nv_bfloat16>();
-        __nv_bfloat16* const a[3] = {a0, a0 + part, p->tc_parts == 3 ? a0 + 2 * part : nullptr};
-        YKB_TRY_CUDA(launch_fdk_preweight_split_bf16(proj, proj_dtype, pwv, parker, count, p->nu, p->nv,
-            p->lda, a, s));
-        const __nv_bfloat16* const ac[3] = {a[0], a[1], a[2]};
         const __nv_bfloat16* const t[3] = {p->toeplitz_hi.as<__nv_bfloat16>(),
             p->toeplitz_lo.as<__nv_bfloat16>(),
             p->tc_parts == 3 ? p->toeplitz_lo2.as<__nv_bfloat16>() : nullptr};
-        YKB_TRY_CUDA(launch_fdk_ramp_tcgen05(ac, t, count * p->nv, p->nu, p->lda, pwv, p->nv,
-            dst, layout, ldc, p->err_flag.as<int>(), s));
+        // sub-batches of views: the preweight (memory bound) of sub-batch
+        // b + 1 runs on the auxiliary stream under the ramp filter (tensor
+        // bound) of sub-batch b
+        constexpr int kSub = ykb_fdk_plan::kFilterSubBatches;
+        const int nsub = count >= 16 * kSub ? kSub : 1;
+        if (nsub > 1 && !p->aux_stream) {
+            YKB_TRY_CUDA(cudaStreamCreateWithFlags(&p->aux_stream, cudaStreamNonBlocking));
+            YKB_TRY_CUDA(cudaEventCreateWithFlags(&p->aux_in, cudaEventDisableTiming));
+            for (cudaEvent_t& e : p->aux_done)
+                YKB_TRY_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        }
+        const cudaStream_t pw_stream = nsub > 1 ? p->aux_stream : s;
+        if (nsub > 1) {
+            // the input is ready and the previous filter call has read the parts
+            YKB_TRY_CUDA(cudaEventRecord(p->aux_in, s));
+            YKB_TRY_CUDA(cudaStreamWaitEvent(p->aux_stream, p->aux_in, 0));
+        }
+        const size_t in_esz = proj_dtype == YKB_DTYPE_BF16 ? 2 : 4;
+        for (int b = 0; b < nsub; ++b) {
+            const int v0 = static_cast<int>(static_cast<long>(count) * b / nsub);
+            const int v1 = static_cast<int>(static_cast<long>(count) * (b + 1) / nsub);
+            const size_t row0 = static_cast<size_t>(v0) * p->nv;
+            __nv_bfloat16* const a[3] = {a0 + row0 * p->lda, a0 + part + row0 * p->lda,
+                p->tc_parts == 3 ? a0 + 2 * part + row0 * p->lda : nullptr};
+            YKB_TRY_CUDA(launch_fdk_preweight_split_bf16(
+                static_cast<const char*>(proj) + row0 * p->nu * in_esz, proj_dtype, pwv + v0,
+                parker ? parker + static_cast<size_t>(v0) * p->nu : nullptr, v1 - v0, p->nu, p->nv,
+                p->lda, a, pw_stream));
+            if (nsub > 1) YKB_TRY_CUDA(cudaEventRecord(p->aux_done[b], p->aux_stream));
+        }
+        for (int b = 0; b < nsub; ++b) {
+            const int v0 = static_cast<int>(static_cast<long>(count) * b / nsub);
+            const int v1 = static_cast<int>(static_cast<long>(count) * (b + 1) / nsub);
+            const size_t row0 = static_cast<size_t>(v0) * p->nv;
+            const __nv_bfloat16* const ac[3] = {a0 + row0 * p->lda, a0 + part + row0 * p->lda,
+                p->tc_parts == 3 ? a0 + 2 * part + row0 * p->lda : nullptr};
+            if (nsub > 1) YKB_TRY_CUDA(cudaStreamWaitEvent(s, p->aux_done[b], 0));
+            const size_t out_row = layout == kFilteredPairs ? 2 * static_cast<size_t>(ldc)
+                                                            : static_cast<size_t>(ldc);
+            YKB_TRY_CUDA(launch_fdk_ramp_tcgen05(ac, t, (v1 - v0) * p->nv, p->nu, p->lda, pwv + v0,
+                p->nv, dst + row0 * out_row, layout, ldc, p->err_flag.as<int>(), s));
+        }
         return YKB_OK;
     }
     YKB_TRY_CUDA(launch_fdk_preweight(proj, proj_dtype, pwv, parker, count, p->nu, p->nv,

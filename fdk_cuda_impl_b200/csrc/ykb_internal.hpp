@@ -320,6 +320,13 @@ struct ykb_fdk_plan {
     bool timing = false;
     std::vector<StageEvents> stage_events;
     size_t stage_events_used = 0;
+    // tensor-core filter: the preweight of the next sub-batch of views runs on
+    // this stream while the ramp filter of the current one runs on the
+    // caller's (created on first use)
+    static constexpr int kFilterSubBatches = 4;
+    cudaStream_t aux_stream = nullptr;
+    cudaEvent_t aux_in = nullptr;                       // the caller's stream reached the filter
+    cudaEvent_t aux_done[kFilterSubBatches] = {};       // sub-batch preweighted
     // host-input streaming (ykb_fdk_execute_host), created on first use
     ykb::DeviceBuffer stage_in;  // two batches of input views
     int stage_views = 0;         // views per batch slot
@@ -332,6 +339,9 @@ struct ykb_fdk_plan {
             if (e.start) cudaEventDestroy(e.start);
             if (e.stop) cudaEventDestroy(e.stop);
         }
+        for (cudaEvent_t e : aux_done) if (e) cudaEventDestroy(e);
+        if (aux_in) cudaEventDestroy(aux_in);
+        if (aux_stream) cudaStreamDestroy(aux_stream);
         for (cudaEvent_t e : copied) if (e) cudaEventDestroy(e);
         for (cudaEvent_t e : consumed) if (e) cudaEventDestroy(e);
         if (copy_stream) cudaStreamDestroy(copy_stream);
