@@ -70,6 +70,28 @@ __device__ __forceinline__ void slice_range(float a, float e, int n, int n0, int
     hi = min(hi, static_cast<int>(ceilf(t1)) + 1);
 }
 
+// Slices where f = a (s - (n0 - 1)/2) + e lies in [-3/2, n + 1/2], in FP64
+// from the float a and e the kernels evaluate: they hold every sample with
+// a non-zero weight (-1 < f < n), and the float f of each of them is within
+// an ulp of that interval, so its floor is in [-2, n] and both taps are
+// inside a two-voxel border.
+__device__ __forceinline__ void slice_range_border(float a, float e, int n, int n0, int& lo,
+    int& hi)
+{
+    const double L = -1.5, U = static_cast<double>(n) + 0.5, h = 0.5 * (n0 - 1);
+    const double ad = a, ed = e;
+    if (fabs(ad) < 1e-300) {
+        if (!(ed >= L && ed <= U)) { lo = 1; hi = 0; }
+        return;
+    }
+    double t0 = (L - ed) / ad + h, t1 = (U - ed) / ad + h;
+    if (t0 > t1) { const double t = t0; t0 = t1; t1 = t; }
+    t0 = fmin(fmax(t0, -1e9), 1e9);
+    t1 = fmin(fmax(t1, -1e9), 1e9);
+    lo = max(lo, static_cast<int>(ceil(t0)));
+    hi = min(hi, static_cast<int>(floor(t1)));
+}
+
 // One thread per ray; a block covers 32 channels x 4 rows of one view, a
 // warp one detector row.  The warp walks the union of its rays' slice ranges
 // together, each lane sampling only inside its own: at every step the 32
@@ -171,10 +193,10 @@ constexpr uint32_t kMagicBits = 0x4B400000u;
 
 // The forward projector for main axis x or y, over the zero-bordered slabs
 // (kSlabPad voxels each side of both minor axes).  The same samples and
-// weights as joseph_fp_kernel, without per-tap bounds checks: each minor
-// coordinate is clamped to [-2, n + 1/4] first, which leaves every in-volume
-// sample as it is and sends every other one onto the zero border, so all
-// four taps are always inside the slab.  Floor and fraction come from the
+// weights as joseph_fp_kernel, without per-tap bounds checks: each lane's
+// slices are those where both minor coordinates lie in [-3/2, n + 1/2]
+// (slice_range_border), so its four taps are inside the slab's border.
+// Floor and fraction come from the
 // rounding constant (both axes in one packed add each), the sample is the
 // bilinear lerp of the four taps, added to the FP64 ray sum.  Lanes walk
 // the warp's slice span together (see joseph_fp_kernel); a slice outside a
@@ -191,8 +213,8 @@ __global__ void __launch_bounds__(128) joseph_fp_padded_kernel(const float* __re
     const RayParams r = ray_params(j, min(iu, nu - 1), min(iv, nv - 1));
     int lo = 0, hi = j.n0 - 1;
     if (pixel && r.ok) {
-        slice_range(r.a1, r.e1, j.n1, j.n0, lo, hi);
-        slice_range(r.a2, r.e2, j.n2, j.n0, lo, hi);
+        slice_range_border(r.a1, r.e1, j.n1, j.n0, lo, hi);
+        slice_range_border(r.a2, r.e2, j.n2, j.n0, lo, hi);
     } else {
         lo = 1; hi = 0;
     }
@@ -201,34 +223,29 @@ __global__ void __launch_bounds__(128) joseph_fp_padded_kernel(const float* __re
     const int p1 = j.n1 + 2 * kSlabPad;
     const long plane = static_cast<long>(p1) * (j.n2 + 2 * kSlabPad);
     // element (i2, i1) of a slice at word (i2 + pad) p1 + i1 + pad, from the
-    // rounding words t1, t2 of floor(f1), floor(f2) (wrapping arithmetic)
+    // rounding words t1, t2 of floor(f1), floor(f2) (wrapping arithmetic);
+    // never past the slice's last 2x2 taps
     const uint32_t koff = static_cast<uint32_t>(kSlabPad) * static_cast<uint32_t>(p1 + 1) -
         kMagicBits * static_cast<uint32_t>(p1 + 1);
-    // upper clamp just past the last voxel: floor n, taps n and n + 1, both
-    // on the border (pad 2)
-    const float hi1 = static_cast<float>(j.n1) + 0.25f, hi2 = static_cast<float>(j.n2) + 0.25f;
+    const uint32_t last = static_cast<uint32_t>(plane) - static_cast<uint32_t>(p1) - 2u;
     const f2 A = f2pack(r.a1, r.a2), E = f2pack(r.e1, r.e2);
     const f2 H = f2pack(0.5f, 0.5f), M = f2pack(kMagic, kMagic);
-    const float half = 0.5f * (j.n0 - 1);
+    float c0 = static_cast<float>(wlo) - 0.5f * (j.n0 - 1);  // exact: integers and halves
     // FP64 ray sum: keeps the adjoint identity at the 1e-7 level even where
     // <Ax, y> cancels to 1e-4 of its terms
     double acc = 0.0;
     // unrolled: the four gathers of several samples are in flight at once
 #pragma unroll 4
-    for (int sq = wlo; sq <= whi; ++sq) {
+    for (int sq = wlo; sq <= whi; ++sq, c0 += 1.f) {
+        // a slice outside this lane's range reads the zero border corner
         const bool in = sq >= lo && sq <= hi;
-        const float c0 = static_cast<float>(sq) - half;
-        float f1, f2v;
-        f2unpack(f2fma(A, f2pack(c0, c0), E), f1, f2v);
-        f1 = in ? fminf(fmaxf(f1, -2.f), hi1) : -2.f;
-        f2v = in ? fminf(fmaxf(f2v, -2.f), hi2) : -2.f;
-        const f2 f = f2pack(f1, f2v);
+        const f2 f = f2fma(A, f2pack(c0, c0), E);
         const f2 t = f2add(f2sub(f, H), M);
         float t1, t2, w1, w2;
         f2unpack(t, t1, t2);
         f2unpack(f2sub(f, f2sub(t, M)), w1, w2);
-        const uint32_t off = __float_as_uint(t2) * static_cast<uint32_t>(p1) +
-            __float_as_uint(t1) + koff;
+        const uint32_t off = in ? min(__float_as_uint(t2) * static_cast<uint32_t>(p1) +
+            __float_as_uint(t1) + koff, last) : 0u;
         const float* p = slab + sq * plane + off;
         const float p00 = __ldg(p), p10 = __ldg(p + 1);
         const float p01 = __ldg(p + p1), p11 = __ldg(p + p1 + 1);
@@ -505,17 +522,20 @@ __global__ void joseph_weight_rays4_kernel(const float* __restrict__ proj,
 // its ZC sums.  Weights are the forward projector's; per view the sums are
 // FP32 (lines in ray order, then over detector columns), over views FP64 in
 // shared memory.  Lines live in shared memory as [slice][slot][line], one
-// bank per lane, slices an odd number of words apart (the threads of a warp
-// read up to 16 slices at one line offset); a slice with more than kLineMax
-// lines takes several passes.
+// bank per lane, slices 21 mod 32 words apart; a slice with more than
+// kLineMax lines takes several passes.
 // ---------------------------------------------------------------------------
 constexpr int kLineBlock = 16;    // 16 x 16 voxel columns a CTA
 constexpr int kLineThreads = 256;
 constexpr int kLineMax = 32;      // lines of a slice per pass
 
-// words from one slice's lines to the next
+// words from one slice's lines to the next: 21 mod 32.  A warp reads two
+// slices (16 lanes each, similar detector columns) or sixteen slices (one
+// lane each, similar column offsets); an odd shift near half the banks keeps
+// both patterns apart (two slices: the second starts 21 banks on; sixteen:
+// 21 s mod 32 are distinct)
 template <int ZC>
-__host__ __device__ constexpr int line_slice_words() { return (ZC + 2) * kLineMax + 1; }
+__host__ __device__ constexpr int line_slice_words() { return (ZC + 2) * kLineMax + 21; }
 
 template <int ZC>
 constexpr size_t line_smem_bytes()
