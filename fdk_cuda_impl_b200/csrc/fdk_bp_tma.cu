@@ -360,119 +360,71 @@ __device__ __forceinline__ float rcp_approx(float x)
 // Shared-memory ring budget of the one CTA of an SM.
 constexpr size_t kRingBudget = 200 * 1024;
 
-// PSEUDO: the weight of the pseudo-matched backprojection instead of the FDK
-// depth weight (tap pairs only)
-template <int BW, bool AXIAL, bool PAIR, bool PSEUDO, int ZC>
-__device__ __forceinline__ void bp_tile(const CUtensorMap& map,
-    const FdkViewCoef* __restrict__ coef, int n_views, const VolumeGrid& g, int BH, int stages,
-    float* __restrict__ vol, int accumulate, int* __restrict__ err,
-    const PseudoViewCoef* __restrict__ pseudo, int za, PipelineWait pw)
+// Shared memory of the backprojection CTA: the ring of stages, their
+// full/empty barriers, and per stage the staged box and (FDK axial tap-pair
+// path) the producer's tile terms of its view.
+struct BpSmem {
+    float* ring;
+    uint64_t* full;
+    uint64_t* empty;
+    int4* boxes;
+    TileTerms* terms;
+    int* abort_flag;
+    int stage_floats;
+};
+
+__device__ __forceinline__ BpSmem bp_smem(int BW, int BH, bool pair, int stages)
 {
     extern __shared__ unsigned char smem_raw[];
     // 128-byte aligned base (the launch requests 128 bytes of slack)
     unsigned char* smem = reinterpret_cast<unsigned char*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~static_cast<uintptr_t>(127));
-    const int stage_floats = stage_stride_floats(BW, BH, PAIR);
-    const uint32_t box_bytes = static_cast<uint32_t>(BW * BH * (PAIR ? 8 : 4));
-    const size_t ring_bytes = static_cast<size_t>(stage_floats) * sizeof(float) * stages;
-    float* ring = reinterpret_cast<float*>(smem);
-    uint64_t* full = reinterpret_cast<uint64_t*>(smem + ring_bytes);
-    uint64_t* empty = full + stages;
-    int4* boxes = reinterpret_cast<int4*>(empty + stages);
-    // FDK axial tap-pair path: the producer's tile terms of each stage's view
-    constexpr bool COLS = AXIAL && PAIR && !PSEUDO;
-    TileTerms* terms = reinterpret_cast<TileTerms*>(boxes + stages);
-    int* abort_ptr = reinterpret_cast<int*>(terms + stages);
-    int& abort_flag = *abort_ptr;
+    BpSmem m;
+    m.stage_floats = stage_stride_floats(BW, BH, pair);
+    const size_t ring_bytes = static_cast<size_t>(m.stage_floats) * sizeof(float) * stages;
+    m.ring = reinterpret_cast<float*>(smem);
+    m.full = reinterpret_cast<uint64_t*>(smem + ring_bytes);
+    m.empty = m.full + stages;
+    m.boxes = reinterpret_cast<int4*>(m.empty + stages);
+    m.terms = reinterpret_cast<TileTerms*>(m.boxes + stages);
+    m.abort_flag = reinterpret_cast<int*>(m.terms + stages);
+    return m;
+}
 
+// Tiles in order: layers of TX x TY tiles (x fastest), the ZT-slice layers
+// from slice 0, then at most one layer of kZTail-slice tiles (a short last
+// part of the volume; it lies inside the ZT-slice layer of the box pre-pass,
+// so its footprints fit the same box).
+struct TileId { int bx, by, za; bool main; };
+
+__device__ __forceinline__ TileId tile_id(long t, int tiles_x, int tiles_y, int main_tiles)
+{
+    const long per_layer = static_cast<long>(tiles_x) * tiles_y;
+    const int bz = static_cast<int>(t / per_layer);
+    const int rem = static_cast<int>(t - bz * per_layer);
+    TileId id;
+    id.by = rem / tiles_x;
+    id.bx = rem - id.by * tiles_x;
+    id.main = bz < main_tiles;
+    id.za = id.main ? bz * ZT : main_tiles * ZT + (bz - main_tiles) * kZTail;
+    return id;
+}
+
+// The consumer warps' part of one tile (bx, by, slices from za).  The stage
+// index s and its phase run on across the CTA's tiles.  False when a wait
+// ran out (the CTA stops).
+// PSEUDO: the weight of the pseudo-matched backprojection instead of the FDK
+// depth weight (tap pairs only)
+template <int BW, bool AXIAL, bool PAIR, bool PSEUDO, int ZC, bool ACC>
+__device__ __forceinline__ bool bp_consume(const BpSmem& sm,
+    const FdkViewCoef* __restrict__ coef, int n_views, const VolumeGrid& g, int BH, int stages,
+    float* __restrict__ vol, int* __restrict__ err,
+    const PseudoViewCoef* __restrict__ pseudo, int bx, int by, int za, PipelineWait pw, int& s,
+    uint32_t& phase)
+{
+    constexpr bool COLS = AXIAL && PAIR && !PSEUDO;
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
-    if (tid == 0) {
-        abort_flag = 0;
-        if ((smem_addr(full) & 7u) != 0 || (smem_addr(ring) & 127u) != 0) {
-            atomicOr(err, kErrAlign);
-            abort_flag = 1;
-        }
-        for (int s = 0; s < stages; ++s) {
-            mbar_init(&full[s], 1);
-            mbar_init(&empty[s], NCWARPS);
-        }
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    __syncthreads();
-    if (abort_flag) return;
-    const TileGeom tg = tile_geom(g, blockIdx.x, blockIdx.y, za, ZC);
-
-    if (warp == NCWARPS) {
-        // ------------------------------------------------------ producer ---
-        // lanes 0..7 project one tile corner each; lane 0 owns the barriers
-        int issued = 0;
-        bool ok = true;
-        int s = 0, use = 0;  // stage of view k and how often it was used before
-        for (int k = 0; k < n_views; ++k, (++s == stages ? (s = 0, ++use) : 0)) {
-            // the view's box and terms first, while the consumers still read
-            // the stage: only the copy waits for it to be released
-            double umin = 1e300, umax = -1e300, vmin = 1e300, vmax = -1e300;
-            if (lane < 8) {
-                corner_uv(coef[k], (lane & 1) ? tg.x1 : tg.x0, (lane & 2) ? tg.y1 : tg.y0,
-                    (lane & 4) ? tg.z1 : tg.z0, umin, vmin);
-                umax = umin; vmax = vmin;
-            }
-#pragma unroll
-            for (int o = 4; o > 0; o >>= 1) {
-                umin = fmin(umin, __shfl_xor_sync(0xffffffffu, umin, o));
-                umax = fmax(umax, __shfl_xor_sync(0xffffffffu, umax, o));
-                vmin = fmin(vmin, __shfl_xor_sync(0xffffffffu, vmin, o));
-                vmax = fmax(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
-            }
-            const Box b = box_from_range(umin, umax, vmin, vmax);
-            TileTerms tt{};
-            if constexpr (COLS)
-                if (lane == 0) tt = tile_terms(coef[k], tg, g.vz, b.c0, b.r0);
-            int go = 1;
-            if (lane == 0) {
-                if (use > 0 && !mbar_wait(&empty[s], (use - 1) & 1, pw.limit_ns)) go = 0;
-                if (*(volatile int*)&abort_flag) go = 0;
-            }
-            go = __shfl_sync(0xffffffffu, go, 0);
-            if (!go) { ok = false; break; }
-            if (k == pw.withheld_view) {
-                // test hook: no copy and no arrival for this view, so every
-                // wait for it runs out
-                issued = k + 1;
-                continue;
-            }
-            int aligned = 1;
-            if (lane == 0) {
-                float* dst = ring + static_cast<size_t>(s) * stage_floats;
-                if ((smem_addr(dst) & 127u) != 0 || (b.c0 & 3) != 0) {
-                    aligned = 0;  // never issue a copy the hardware would reject
-                } else {
-                    boxes[s] = make_int4(b.c0, b.r0, b.c1, b.r1);
-                    if constexpr (COLS) terms[s] = tt;
-                    mbar_arrive_expect_tx(&full[s], box_bytes);
-                    tma_load_3d(dst, &map, &full[s], b.c0 + (PAIR ? kPairLead : 0), b.r0, k);
-                }
-            }
-            aligned = __shfl_sync(0xffffffffu, aligned, 0);
-            if (!aligned) {
-                if (lane == 0) atomicOr(err, kErrAlign);
-                ok = false;
-                break;
-            }
-            issued = k + 1;
-        }
-        if (!ok && lane == 0) {
-            atomicOr(err, kErrTimeout);
-            *(volatile int*)&abort_flag = 1;
-            // drain: every issued copy must land before the CTA exits
-            const int first = max(0, issued - stages);
-            for (int k = first; k < issued; ++k)
-                if (k != pw.withheld_view) mbar_wait(&full[k % stages], (k / stages) & 1);
-        }
-        return;
-    }
-
     // --------------------------------------------------------- consumers ---
     // a warp covers an 8x4 block of columns, each half-warp a 4x4 block: the
     // detector footprint of 16 lanes then spans few columns, so the 16-lane
@@ -480,7 +432,7 @@ __device__ __forceinline__ void bp_tile(const CUtensorMap& map,
     // a bank
     const int lx = 8 * (warp & 1) + 4 * (lane >> 4) + (lane & 3);
     const int ly = 4 * (warp >> 1) + ((lane >> 2) & 3);
-    const int x = blockIdx.x * TX + lx, y = blockIdx.y * TY + ly;
+    const int x = bx * TX + lx, y = by * TY + ly;
     const int z0 = za;
     const bool active = x < g.nx && y < g.ny;
     const double X = g.ox + x * g.vx, Y = g.oy + y * g.vy, Z0 = g.oz + z0 * g.vz;
@@ -493,27 +445,25 @@ __device__ __forceinline__ void bp_tile(const CUtensorMap& map,
     // the column's offset from the tile centre (exact: a few voxel pitches)
     float dx = 0.f, dy = 0.f;
     if constexpr (COLS) {
-        const TileGeom tg = tile_geom(g, blockIdx.x, blockIdx.y, za, ZC);
+        const TileGeom tg = tile_geom(g, bx, by, za, ZC);
         dx = static_cast<float>(X - tg.xc);
         dy = static_cast<float>(Y - tg.yc);
     }
 
-    int s = 0;
-    uint32_t phase = 0;
     for (int k = 0; k < n_views; ++k, (++s == stages ? (s = 0, phase ^= 1u) : 0)) {
         // the warp leaves together: a lane whose wait ran out takes its whole
         // warp with it, so no lane is left waiting at the warp barrier below
-        if (!__all_sync(0xffffffffu, mbar_wait(&full[s], phase, pw.limit_ns))) {
+        if (!__all_sync(0xffffffffu, mbar_wait(&sm.full[s], phase, pw.limit_ns))) {
             if (lane == 0) {
                 atomicOr(err, kErrTimeout);
-                *(volatile int*)&abort_flag = 1;
+                *(volatile int*)sm.abort_flag = 1;
             }
-            return;
+            return false;
         }
-        const float* S = ring + static_cast<size_t>(s) * stage_floats;
+        const float* S = sm.ring + static_cast<size_t>(s) * sm.stage_floats;
         if constexpr (COLS) {
             // the column's terms in FP32 from the tile terms of this view
-            const TileTerms& T = terms[s];
+            const TileTerms& T = sm.terms[s];
             const float4 t0 = *reinterpret_cast<const float4*>(&T.uc);
             const float4 t1 = *reinterpret_cast<const float4*>(&T.hv0);
             const float4 t2 = *reinterpret_cast<const float4*>(&T.gd1);
@@ -568,10 +518,10 @@ __device__ __forceinline__ void bp_tile(const CUtensorMap& map,
                 acc[2 * j + 1] = fmaf(w1, r1, fmaf(w0, l1, acc[2 * j + 1]));
             }
             __syncwarp();
-            if (lane == 0) mbar_arrive(&empty[s]);
+            if (lane == 0) mbar_arrive(&sm.empty[s]);
             continue;
         }
-        const int4 b = boxes[s];
+        const int4 b = sm.boxes[s];
         const FdkViewCoef& c = coef[k];
         if (AXIAL) {
             // next view's terms first: independent of this view's stage
@@ -747,41 +697,159 @@ __device__ __forceinline__ void bp_tile(const CUtensorMap& map,
             }
         }
         __syncwarp();
-        if (lane == 0) mbar_arrive(&empty[s]);
+        if (lane == 0) mbar_arrive(&sm.empty[s]);
     }
     if (bad) atomicOr(err, kErrFootprint);
-    if (!active) return;
+    if (!active) return true;
     const long plane = static_cast<long>(g.nx) * g.ny;
     float* dst = vol + static_cast<long>(y) * g.nx + x;
+    if constexpr (ACC) {
+        // a reduction in L2 (each voxel has this one writer, so the sum is the
+        // plain old + acc): no load round trip per value, which one after
+        // another cost about 1 ms per 512^3 launch
 #pragma unroll
-    for (int i = 0; i < ZC; ++i) {
-        const int z = z0 + i;
-        if (z < g.nz) {
-            float* p = dst + z * plane;
-            *p = accumulate ? *p + acc[i] : acc[i];
+        for (int i = 0; i < ZC; ++i) {
+            const int z = z0 + i;
+            if (z < g.nz) atomicAdd(dst + z * plane, acc[i]);
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < ZC; ++i) {
+            const int z = z0 + i;
+            if (z < g.nz) dst[z * plane] = acc[i];
         }
     }
+    return true;
 }
 
-// blockIdx.z < main_tiles: ZT-slice tiles from slice 0; above: kZTail-slice
-// tiles after them (a short last part of the volume).  The short tiles are
-// the grid's last blocks, so they fill the final wave of the long ones.
-// One CTA of 17 warps per SM.  Registers are granted for whole groups of
-// four warps (20 here), which caps a thread at 96: enough for the 64 sums of
-// the axial tap-pair path (a few bytes of spill); the other paths spill more.
-template <int BW, bool AXIAL, bool PAIR, bool PSEUDO>
+// Persistent: one CTA of 17 warps per SM walks tiles blockIdx.x, +gridDim.x,
+// ... (see tile_id).  The producer warp runs on into the next tile's views
+// while the consumers finish a tile and write its sums, so a tile costs no
+// pipeline fill or drain of its own (a CTA per tile cost about 0.8 ms per
+// 512^3 launch in starting and ending 4096 CTAs).  Registers are granted for
+// whole groups of four warps (20 here), which caps a thread at 96: enough
+// for the 64 sums of the axial tap-pair path (a few bytes of spill); the
+// other paths spill more.
+// ACC: add to the volume instead of writing it (a separate kernel, so that
+// the write-only form's registers are not shaped by the reductions)
+template <int BW, bool AXIAL, bool PAIR, bool PSEUDO, bool ACC>
 __global__ void __launch_bounds__(NTHREADS, 1) fdk_bp_tma_kernel(const __grid_constant__ CUtensorMap map,
     const FdkViewCoef* __restrict__ coef, int n_views, VolumeGrid g, int BH, int stages,
-    float* __restrict__ vol, int accumulate, int* __restrict__ err,
-    const PseudoViewCoef* __restrict__ pseudo, int main_tiles, PipelineWait pw)
+    float* __restrict__ vol, int* __restrict__ err,
+    const PseudoViewCoef* __restrict__ pseudo, int main_tiles, int tiles_x, int tiles_y,
+    long n_tiles, PipelineWait pw)
 {
-    const int bz = static_cast<int>(blockIdx.z);
-    if (bz < main_tiles)
-        bp_tile<BW, AXIAL, PAIR, PSEUDO, ZT>(map, coef, n_views, g, BH, stages, vol, accumulate,
-            err, pseudo, bz * ZT, pw);
-    else
-        bp_tile<BW, AXIAL, PAIR, PSEUDO, kZTail>(map, coef, n_views, g, BH, stages, vol,
-            accumulate, err, pseudo, main_tiles * ZT + (bz - main_tiles) * kZTail, pw);
+    constexpr bool COLS = AXIAL && PAIR && !PSEUDO;
+    const BpSmem sm = bp_smem(BW, BH, PAIR, stages);
+    const uint32_t box_bytes = static_cast<uint32_t>(BW * BH * (PAIR ? 8 : 4));
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    if (tid == 0) {
+        *sm.abort_flag = 0;
+        if ((smem_addr(sm.full) & 7u) != 0 || (smem_addr(sm.ring) & 127u) != 0) {
+            atomicOr(err, kErrAlign);
+            *sm.abort_flag = 1;
+        }
+        for (int s = 0; s < stages; ++s) {
+            mbar_init(&sm.full[s], 1);
+            mbar_init(&sm.empty[s], NCWARPS);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (*sm.abort_flag) return;
+
+    if (warp == NCWARPS) {
+        // ------------------------------------------------------ producer ---
+        // lanes 0..7 project one tile corner each; lane 0 owns the barriers.
+        // q counts the CTA's copies over all its tiles: stage q % stages,
+        // used q / stages times before
+        long q = 0, issued = 0;
+        bool ok = true;
+        for (long t = blockIdx.x; t < n_tiles && ok; t += gridDim.x) {
+            const TileId id = tile_id(t, tiles_x, tiles_y, main_tiles);
+            const TileGeom tg = tile_geom(g, id.bx, id.by, id.za, id.main ? ZT : kZTail);
+            for (int k = 0; k < n_views; ++k, ++q) {
+                const int s = static_cast<int>(q % stages);
+                const long use = q / stages;
+                // the view's box and terms first, while the consumers still
+                // read the stage: only the copy waits for it to be released
+                double umin = 1e300, umax = -1e300, vmin = 1e300, vmax = -1e300;
+                if (lane < 8) {
+                    corner_uv(coef[k], (lane & 1) ? tg.x1 : tg.x0, (lane & 2) ? tg.y1 : tg.y0,
+                        (lane & 4) ? tg.z1 : tg.z0, umin, vmin);
+                    umax = umin; vmax = vmin;
+                }
+#pragma unroll
+                for (int o = 4; o > 0; o >>= 1) {
+                    umin = fmin(umin, __shfl_xor_sync(0xffffffffu, umin, o));
+                    umax = fmax(umax, __shfl_xor_sync(0xffffffffu, umax, o));
+                    vmin = fmin(vmin, __shfl_xor_sync(0xffffffffu, vmin, o));
+                    vmax = fmax(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+                }
+                const Box b = box_from_range(umin, umax, vmin, vmax);
+                TileTerms tt{};
+                if constexpr (COLS)
+                    if (lane == 0) tt = tile_terms(coef[k], tg, g.vz, b.c0, b.r0);
+                int go = 1;
+                if (lane == 0) {
+                    if (use > 0 && !mbar_wait(&sm.empty[s], static_cast<uint32_t>(use - 1) & 1u,
+                            pw.limit_ns))
+                        go = 0;
+                    if (*(volatile int*)sm.abort_flag) go = 0;
+                }
+                go = __shfl_sync(0xffffffffu, go, 0);
+                if (!go) { ok = false; break; }
+                if (k == pw.withheld_view) {
+                    // test hook: no copy and no arrival for this view, so every
+                    // wait for it runs out
+                    issued = q + 1;
+                    continue;
+                }
+                int aligned = 1;
+                if (lane == 0) {
+                    float* dst = sm.ring + static_cast<size_t>(s) * sm.stage_floats;
+                    if ((smem_addr(dst) & 127u) != 0 || (b.c0 & 3) != 0) {
+                        aligned = 0;  // never issue a copy the hardware would reject
+                    } else {
+                        sm.boxes[s] = make_int4(b.c0, b.r0, b.c1, b.r1);
+                        if constexpr (COLS) sm.terms[s] = tt;
+                        mbar_arrive_expect_tx(&sm.full[s], box_bytes);
+                        tma_load_3d(dst, &map, &sm.full[s], b.c0 + (PAIR ? kPairLead : 0), b.r0, k);
+                    }
+                }
+                aligned = __shfl_sync(0xffffffffu, aligned, 0);
+                if (!aligned) {
+                    if (lane == 0) atomicOr(err, kErrAlign);
+                    ok = false;
+                    break;
+                }
+                issued = q + 1;
+            }
+        }
+        if (!ok && lane == 0) {
+            atomicOr(err, kErrTimeout);
+            *(volatile int*)sm.abort_flag = 1;
+            // drain: every issued copy must land before the CTA exits
+            for (long j = max(0L, issued - stages); j < issued; ++j)
+                if (static_cast<int>(j % n_views) != pw.withheld_view)
+                    mbar_wait(&sm.full[j % stages], static_cast<uint32_t>(j / stages) & 1u);
+        }
+        return;
+    }
+
+    // --------------------------------------------------------- consumers ---
+    int s = 0;
+    uint32_t phase = 0;
+    for (long t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+        const TileId id = tile_id(t, tiles_x, tiles_y, main_tiles);
+        const bool ok = id.main
+            ? bp_consume<BW, AXIAL, PAIR, PSEUDO, ZT, ACC>(sm, coef, n_views, g, BH, stages, vol,
+                  err, pseudo, id.bx, id.by, id.za, pw, s, phase)
+            : bp_consume<BW, AXIAL, PAIR, PSEUDO, kZTail, ACC>(sm, coef, n_views, g, BH, stages,
+                  vol, err, pseudo, id.bx, id.by, id.za, pw, s, phase);
+        if (!ok) return;
+    }
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
@@ -813,8 +881,7 @@ constexpr int kNarrowWidths[] = {36, 52, 68, 100, 132, 196};
 
 // z tiling: ZT-slice tiles, except that a remainder of at most kZTail
 // slices becomes one kZTail-slice tile instead of a ZT-slice tile that is
-// mostly outside the volume.  The short tile lies inside the ZT-slice tile
-// of the box pre-pass, so its footprints fit the same box.
+// mostly outside the volume (see tile_id).
 template <typename K>
 cudaError_t launch_kernel(K k, const CUtensorMap& map, const FdkViewCoef* coef, int n_views,
     const VolumeGrid& g, int BH, int stages, size_t smem, float* vol, int accumulate, int* err,
@@ -823,12 +890,19 @@ cudaError_t launch_kernel(K k, const CUtensorMap& map, const FdkViewCoef* coef, 
     const int rem = g.nz % ZT;
     const bool tail = rem > 0 && rem <= kZTail;
     const int main_tiles = tail ? g.nz / ZT : (g.nz + ZT - 1) / ZT;
-    const dim3 grid((g.nx + TX - 1) / TX, (g.ny + TY - 1) / TY, main_tiles + (tail ? 1 : 0));
-    const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    const int tiles_x = (g.nx + TX - 1) / TX, tiles_y = (g.ny + TY - 1) / TY;
+    const long n_tiles = static_cast<long>(tiles_x) * tiles_y * (main_tiles + (tail ? 1 : 0));
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
         static_cast<int>(smem));
     if (e != cudaSuccess) return e;
-    k<<<grid, NTHREADS, smem, s>>>(map, coef, n_views, g, BH, stages, vol, accumulate, err, pseudo,
-        main_tiles, pw);
+    int device = 0, sms = 0;
+    if ((e = cudaGetDevice(&device)) != cudaSuccess ||
+        (e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess)
+        return e;
+    // one persistent CTA per SM (the ring takes most of its shared memory)
+    const unsigned grid = static_cast<unsigned>(std::min<long>(n_tiles, sms));
+    k<<<grid, NTHREADS, smem, s>>>(map, coef, n_views, g, BH, stages, vol, err, pseudo,
+        main_tiles, tiles_x, tiles_y, n_tiles, pw);
     return cudaGetLastError();
 }
 
@@ -839,18 +913,18 @@ cudaError_t launch_bw(const CUtensorMap& map, const FdkViewCoef* coef, int n_vie
 {
     if constexpr (PAIR) {
         if (pseudo && axial)
-            return launch_kernel(fdk_bp_tma_kernel<BW, true, true, true>, map, coef, n_views, g,
+            return launch_kernel(accumulate ? fdk_bp_tma_kernel<BW, true, true, true, true> : fdk_bp_tma_kernel<BW, true, true, true, false>, map, coef, n_views, g,
                 BH, stages, smem, vol, accumulate, err, pseudo, pw, s);
         if (pseudo)
-            return launch_kernel(fdk_bp_tma_kernel<BW, false, true, true>, map, coef, n_views, g,
+            return launch_kernel(accumulate ? fdk_bp_tma_kernel<BW, false, true, true, true> : fdk_bp_tma_kernel<BW, false, true, true, false>, map, coef, n_views, g,
                 BH, stages, smem, vol, accumulate, err, pseudo, pw, s);
     } else {
         if (pseudo) return cudaErrorInvalidValue;  // pseudo-matched input is staged as pairs
     }
     if (axial)
-        return launch_kernel(fdk_bp_tma_kernel<BW, true, PAIR, false>, map, coef, n_views, g, BH,
+        return launch_kernel(accumulate ? fdk_bp_tma_kernel<BW, true, PAIR, false, true> : fdk_bp_tma_kernel<BW, true, PAIR, false, false>, map, coef, n_views, g, BH,
             stages, smem, vol, accumulate, err, pseudo, pw, s);
-    return launch_kernel(fdk_bp_tma_kernel<BW, false, PAIR, false>, map, coef, n_views, g, BH,
+    return launch_kernel(accumulate ? fdk_bp_tma_kernel<BW, false, PAIR, false, true> : fdk_bp_tma_kernel<BW, false, PAIR, false, false>, map, coef, n_views, g, BH,
         stages, smem, vol, accumulate, err, pseudo, pw, s);
 }
 
@@ -859,7 +933,7 @@ cudaError_t launch_narrow(const CUtensorMap& map, const FdkViewCoef* coef, int n
     const VolumeGrid& g, int BH, int stages, size_t smem, float* vol, int accumulate, int* err,
     PipelineWait pw, cudaStream_t s)
 {
-    return launch_kernel(fdk_bp_tma_kernel<BW, true, true, false>, map, coef, n_views, g, BH,
+    return launch_kernel(accumulate ? fdk_bp_tma_kernel<BW, true, true, false, true> : fdk_bp_tma_kernel<BW, true, true, false, false>, map, coef, n_views, g, BH,
         stages, smem, vol, accumulate, err, nullptr, pw, s);
 }
 

@@ -454,19 +454,23 @@ ykb_status backproject_chunk(ykb_fdk_plan* p, const void* filtered, int layout, 
 
 // Host projections streamed through the plan, copied on the plan's copy
 // stream into two staging slots double-buffered against the filter and
-// backprojection on `s`.  Batches grow geometrically from 16 views up to a
-// quarter of the views: the kernels wait only for the first, short copy,
-// and each later copy (a view copies in about a third of the time its
-// kernels take) completes while the previous batch is processed; a
-// remainder of between one and two batches runs as two halves.  With
-// h_volume, the last batch is backprojected in z slabs of whole z
-// tiles and each finished slab is copied to h_volume behind the next slab's
-// kernel; `s` then completes with the host volume.
+// backprojection on `s`.  Batches double from 16 views up to half of the
+// views: the kernels wait only for the first, short copy, and each later
+// copy (a view copies in about half the time its kernels take) completes
+// while the previous batch is processed; a remainder of between one and two
+// batches runs as two halves.  Few batches matter: each backprojection
+// launch costs about 0.8 ms beyond its views (512^3 x 720: 64.6 ms in one
+// launch, 75.7 ms in seven).  With h_volume, the last batch is
+// backprojected in z slabs of whole z tiles, about a quarter of the volume
+// each (two 64-slice layers of 512 CTAs at 512^3 fill whole waves of 148
+// SMs, where one layer leaves half a wave idle), and each finished slab is
+// copied to h_volume behind the next slab's kernel; `s` then completes with
+// the host volume.
 ykb_status stream_host(ykb_fdk_plan* p, const void* h_proj, int proj_dtype, int view_offset,
     int n_views, float* d_volume, float* h_volume, int clear_output, cudaStream_t s)
 {
     const size_t view_bytes = static_cast<size_t>(p->nu) * p->nv * dtype_bytes(proj_dtype);
-    const int batch = std::min(p->batch_capacity, std::max(16, (p->n_views + 3) / 4));
+    const int batch = std::min(p->batch_capacity, std::max(16, (p->n_views + 1) / 2));
     if (p->stage_views < batch || p->stage_in.bytes < 2 * batch * static_cast<size_t>(p->nu) * p->nv * 4) {
         if (p->copy_stream) YKB_TRY_CUDA(cudaStreamSynchronize(p->copy_stream));
         YKB_TRY_CUDA(cudaStreamSynchronize(s));
@@ -487,10 +491,10 @@ ykb_status stream_host(ykb_fdk_plan* p, const void* h_proj, int proj_dtype, int 
     const size_t slot_bytes = static_cast<size_t>(p->stage_views) * view_bytes;
     int next_batch = std::min(batch, 16);
     const int nz = p->volume.nz;
-    // eighths of the volume in whole z tiles: the download of the last slab
+    // quarters of the volume in whole z tiles: the download of the last slab
     // is what stays exposed
     const int zt = fdk_tma_z_tile();
-    const int slab = std::max(zt, (nz / 8 + zt - 1) / zt * zt);
+    const int slab = std::max(zt, (nz / 4 + zt - 1) / zt * zt);
     const size_t plane = static_cast<size_t>(p->volume.nx) * p->volume.ny;
     for (int c = 0, b = 0; c < n_views; ++b) {
         // between one and two batches left: two halves, so that the last
