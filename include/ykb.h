@@ -263,8 +263,8 @@ YKB_API ykb_status ykb_fdk_test_pipeline_wait(ykb_fdk_plan* plan,
  * inside the library, present on every GPU that loads it until exit;
  * limits: nu <= 8192, n_views <= 16384, nu*nv*4 <= 30,867,456 bytes
  * (29.4 MiB) per view, else YKB_ERR_INVALID_CONFIG.  The first call on a
- * device looks up that device's scratch address (make it before any stream
- * capture).  All calls share the one array: calls that overlap on the GPU
+ * device looks up that device's scratch address (cudaGetSymbolAddress).
+ * All calls share the one array: calls that overlap on the GPU
  * (different streams, without ordering between them) race and corrupt each
  * other. */
 YKB_API ykb_status ykb_fdk_filter_static(const ykb_cone_view* views,
