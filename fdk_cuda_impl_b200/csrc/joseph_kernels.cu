@@ -519,8 +519,8 @@ __global__ void joseph_weight_rays4_kernel(const float* __restrict__ proj,
 // walking its column's rays in order: every ray once per slice instead of
 // once per voxel column it touches, about 2.5), then each thread adds the
 // lines of its own column's candidate detector columns, weighted by h1, to
-// its ZC sums.  Weights are the forward projector's; per view the sums are
-// FP32 (lines in ray order, then over detector columns), over views FP64 in
+// its ZC sums.  Weights are the forward projector's; over two views the sums
+// are FP32 (lines in ray order, then over detector columns), then FP64 in
 // shared memory.  Lines live in shared memory as [slice][slot][line], one
 // bank per lane, slices 21 mod 32 words apart; a slice with more than
 // kLineMax lines takes several passes.
@@ -566,6 +566,9 @@ __global__ void __launch_bounds__(kLineThreads, 3) joseph_bp_lines_kernel(
     // slot of floor(f2) + 1 from the rounding word of f2 - 1/2 (wrapping)
     const uint32_t slot0 = kMagicBits + static_cast<uint32_t>(z0 - 1);
     const f2 H = f2pack(0.5f, 0.5f), M = f2pack(kMagic, kMagic);
+    float acc[ZC];  // FP32 over two views, then into the FP64 sums
+#pragma unroll
+    for (int q = 0; q < ZC; ++q) acc[q] = 0.f;
     for (int k = 0; k < n_views; ++k) {
         const JosephView& j = views[k];
         const bool ax0 = j.axis == 0;
@@ -590,9 +593,6 @@ __global__ void __launch_bounds__(kLineThreads, 3) joseph_bp_lines_kernel(
         if (mine) footprint_box(vp[k], j, c0, j1, z0, z0 + ZC - 1, nu, nv, cu0, cu1, cv0, cv1);
         const float j1f = static_cast<float>(j1);
         const float2* ck = cols + static_cast<long>(k) * nu;
-        float acc[ZC];
-#pragma unroll
-        for (int q = 0; q < ZC; ++q) acc[q] = 0.f;
         for (int pass = 0; pass < passes; ++pass) {
             // ---- lines: warp w builds slices w and w + 8, lane = line
             for (int sp = warp; sp < B; sp += kLineThreads / 32) {
@@ -674,8 +674,13 @@ __global__ void __launch_bounds__(kLineThreads, 3) joseph_bp_lines_kernel(
             }
             __syncthreads();
         }
+        if ((k & 1) || k + 1 == n_views) {
 #pragma unroll
-        for (int q = 0; q < ZC; ++q) total[q * kLineThreads + tid] += static_cast<double>(acc[q]);
+            for (int q = 0; q < ZC; ++q) {
+                total[q * kLineThreads + tid] += static_cast<double>(acc[q]);
+                acc[q] = 0.f;
+            }
+        }
     }
     if (!mine) return;
     const long plane = static_cast<long>(nx) * ny;
