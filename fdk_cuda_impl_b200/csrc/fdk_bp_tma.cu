@@ -511,9 +511,15 @@ __device__ __forceinline__ bool bp_consume(const BpSmem& sm,
                 const uint32_t a1 = __float_as_uint(t1f) * (8u * BW) + base;
                 const f2 A0 = lds2<0>(a0), B0 = lds2<8 * BW>(a0);
                 const f2 A1 = lds2<0>(a1), B1 = lds2<8 * BW>(a1);
-                float l0, r0, l1, r1;
-                f2unpack(f2fma(f2pack(f0, f0), f2sub(B0, A0), A0), l0, r0);
-                f2unpack(f2fma(f2pack(f1, f1), f2sub(B1, A1), A1), l1, r1);
+                // vertical lerps as scalar FMAs on the halves of the pairs
+                // (a packed FMA would need each fraction in both halves)
+                float al0, ar0, dl0, dr0, al1, ar1, dl1, dr1;
+                f2unpack(A0, al0, ar0);
+                f2unpack(f2sub(B0, A0), dl0, dr0);
+                f2unpack(A1, al1, ar1);
+                f2unpack(f2sub(B1, A1), dl1, dr1);
+                const float l0 = fmaf(f0, dl0, al0), r0 = fmaf(f0, dr0, ar0);
+                const float l1 = fmaf(f1, dl1, al1), r1 = fmaf(f1, dr1, ar1);
                 acc[2 * j] = fmaf(w1, r0, fmaf(w0, l0, acc[2 * j]));
                 acc[2 * j + 1] = fmaf(w1, r1, fmaf(w0, l1, acc[2 * j + 1]));
             }
