@@ -11,6 +11,11 @@
 //   NSEG 3 (BF16 plans): A0 T0 + A0 T1 + A1 T0, about 16 significant bits;
 //   NSEG 6 (FP32 plans): A0 T0 + A0 T1 + A1 T0 + A0 T2 + A1 T1 + A2 T0, the
 //     24 bits of FP32 (the dropped products are below 2^-24 of the result).
+//     The last three, each at most 2^-18 of |A| |T|, run only over the K
+//     chunks near the output tile's columns (`near` chunks each side): the
+//     ramp taps fall off as 1/d^2, and the host picks `near` so that the taps
+//     beyond carry at most 2^-8 of sum |h|, which leaves what is skipped
+//     below the FP32 rounding of the result.
 //
 // Persistent CTAs, one per SM, walk the output tiles (128 rows x TN
 // columns) with six warps:
@@ -33,6 +38,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <cmath>
 #include <mutex>
 
 namespace ykb {
@@ -125,9 +131,37 @@ __device__ __forceinline__ void segment_parts(int seg, int& a, int& t)
     t = (0x012010 >> (4 * seg)) & 0xF;
 }
 
+// K steps of the output tile starting at column n0: segments 0-2 over all
+// kchunks chunks, then (NSEG 6) segments 3-5 over chunks [lo, lo + n)
+struct NearChunks { int lo, n; };
+template <int TN>
+__device__ __forceinline__ NearChunks near_chunks(int n0, int kchunks, int near)
+{
+    const int c0 = n0 / TK;  // TN is a multiple of TK
+    const int lo = max(0, c0 - near), hi = min(kchunks, c0 + TN / TK + near);
+    return {lo, max(hi - lo, 0)};
+}
+template <int NSEG>
+__device__ __forceinline__ int tile_steps(int kchunks, NearChunks nc)
+{
+    return NSEG == 6 ? 3 * kchunks + 3 * nc.n : NSEG * kchunks;
+}
+__device__ __forceinline__ void step_of(int i, int kchunks, NearChunks nc, int& seg, int& kc)
+{
+    if (i < 3 * kchunks) {
+        seg = i / kchunks;
+        kc = i - seg * kchunks;
+    } else {
+        const int j = i - 3 * kchunks, q = j / nc.n;
+        seg = 3 + q;
+        kc = nc.lo + j - q * nc.n;
+    }
+}
+
+static_assert((2 * kPairLead) % 4 == 0, "tap-pair rows start 16-byte aligned after the lead");
 constexpr int kEpiWarps = 4;
 constexpr int kFilterThreads = 64 + 32 * kEpiWarps;  // producer, MMA issuer, 4 epilogue warps
-constexpr int kStagePitch = 17;                       // floats per staged row (odd: no bank conflicts)
+constexpr int kStagePitch = 19;                       // floats per staged row: 2 carried + 16 (odd: no bank conflicts)
 
 __device__ __forceinline__ void bar_arrive(uint64_t* b)
 {
@@ -144,8 +178,9 @@ __global__ void __launch_bounds__(kFilterThreads, 1) ramp_tc_kernel(
     const __grid_constant__ CUtensorMap map_a0, const __grid_constant__ CUtensorMap map_a1,
     const __grid_constant__ CUtensorMap map_a2, const __grid_constant__ CUtensorMap map_t0,
     const __grid_constant__ CUtensorMap map_t1, const __grid_constant__ CUtensorMap map_t2,
-    long rows, int nu, int nv, int kchunks, int col_tiles, long tiles,
-    const FdkPreweightView* __restrict__ pwv, float* __restrict__ C, int ldc, int* __restrict__ err)
+    long rows, int nu, int nv, int kchunks, int near, int col_tiles, long tiles,
+    const FdkPreweightView* __restrict__ pwv, float* __restrict__ C, int ldc, int vec,
+    int* __restrict__ err)
 {
     constexpr uint32_t kBStageBytes = TN * TK * 2;
     constexpr uint32_t kAccCols = TN <= 32 ? 32 : TN <= 64 ? 64 : TN <= 128 ? 128 : 256;
@@ -165,7 +200,6 @@ __global__ void __launch_bounds__(kFilterThreads, 1) ramp_tc_kernel(
     int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int total = NSEG * kchunks;  // k-steps per tile
 
     if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
@@ -192,6 +226,8 @@ __global__ void __launch_bounds__(kFilterThreads, 1) ramp_tc_kernel(
             for (long t = blockIdx.x; t < tiles && !stop; t += gridDim.x) {
                 const int m0 = static_cast<int>((t / col_tiles) * TM);
                 const int n0 = static_cast<int>((t % col_tiles) * TN);
+                const NearChunks nc = near_chunks<TN>(n0, kchunks, near);
+                const int total = tile_steps<NSEG>(kchunks, nc);
                 for (int i = 0; i < total; ++i, ++it) {
                     const int s = static_cast<int>(it % STAGES);
                     if (it >= STAGES && !bar_wait(&empty[s], static_cast<uint32_t>((it / STAGES) - 1) & 1)) {
@@ -199,8 +235,8 @@ __global__ void __launch_bounds__(kFilterThreads, 1) ramp_tc_kernel(
                         *(volatile int*)abort_flag = 1;
                     }
                     if (*(volatile int*)abort_flag) { stop = true; break; }
-                    const int seg = i / kchunks, kc = i - seg * kchunks;
-                    int pa, pt;
+                    int seg, kc, pa, pt;
+                    step_of(i, kchunks, nc, seg, kc);
                     segment_parts(seg, pa, pt);
                     const CUtensorMap* ma = pa == 0 ? &map_a0 : pa == 1 ? &map_a1 : &map_a2;
                     const CUtensorMap* mt = pt == 0 ? &map_t0 : pt == 1 ? &map_t1 : &map_t2;
@@ -231,6 +267,8 @@ __global__ void __launch_bounds__(kFilterThreads, 1) ramp_tc_kernel(
                 }
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 const uint32_t d = tmem + static_cast<uint32_t>(buf) * kAccCols;
+                const int total = tile_steps<NSEG>(kchunks,
+                    near_chunks<TN>(static_cast<int>((t % col_tiles) * TN), kchunks, near));
                 for (int i = 0; i < total; ++i, ++it) {
                     const int s = static_cast<int>(it % STAGES);
                     if (!bar_wait(&full[s], static_cast<uint32_t>(it / STAGES) & 1)) {
@@ -271,13 +309,24 @@ __global__ void __launch_bounds__(kFilterThreads, 1) ramp_tc_kernel(
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const long m0 = (t / col_tiles) * TM;
             const int n0 = static_cast<int>((t % col_tiles) * TN);
-            const long m = m0 + q * 32 + lane;
-            int out_lo = 0, out_hi = 0;
+            const long wrow0 = m0 + q * 32;  // the warp's first row
+            const long m = wrow0 + lane;
+            // this lane's row keeps columns [lo, hi) (the samples placed in
+            // the padded FFT row)
+            int lo = 0, hi = 0;
             if (m < rows) {
                 const FdkPreweightView& p = pwv[m / nv];
-                out_lo = p.out_lo;
-                out_hi = p.out_hi;
+                lo = max(p.out_lo, 0);
+                hi = max(min(p.out_hi, nu), lo);
             }
+            // tap pairs: this tile writes the floats [X0, X1) of each row
+            // (float x holds f[(x + 1) >> 1]): from 2 n0 - 1, or -4 for the
+            // first tile (the pairs before the row are zero), up to the
+            // next tile's first float, or 2 nu (the right half of the last
+            // pair is zero)
+            const int X0 = n0 == 0 ? -4 : 2 * n0 - 1;
+            const int X1 = n0 + TN >= nu ? 2 * nu : 2 * (n0 + TN) - 1;
+            float carry0 = 0.f, carry1 = 0.f;  // columns c0 - 2 and c0 - 1 of the lane's row
 #pragma unroll 1
             for (int c = 0; c < TN; c += 16) {
                 uint32_t r[16];
@@ -290,39 +339,104 @@ __global__ void __launch_bounds__(kFilterThreads, 1) ramp_tc_kernel(
                              : "r"(taddr));
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
                 const int c0 = n0 + c;
-                // this lane's row, masked to the samples placed in the padded row
+                float x[16];
 #pragma unroll
-                for (int i = 0; i < 16; ++i) {
-                    const int j = c0 + i;
-                    stg[lane * kStagePitch + i] = (j < nu && j >= out_lo && j < out_hi)
-                        ? __uint_as_float(r[i]) : 0.f;
+                for (int i = 0; i < 16; ++i) x[i] = __uint_as_float(r[i]);
+                if (c0 < lo || c0 + 16 > hi) {
+#pragma unroll
+                    for (int i = 0; i < 16; ++i)
+                        if (static_cast<unsigned>(c0 + i - lo) >= static_cast<unsigned>(hi - lo)) x[i] = 0.f;
                 }
+                // staged row: columns c0 - 2 .. c0 + 15
+                float* srow = stg + lane * kStagePitch;
+                srow[0] = carry0;
+                srow[1] = carry1;
+#pragma unroll
+                for (int i = 0; i < 16; ++i) srow[2 + i] = x[i];
+                carry0 = x[14];
+                carry1 = x[15];
                 __syncwarp();
-                // transposed: each store instruction writes one row's chunk
+                // transposed: each store instruction writes whole row segments
                 if constexpr (PAIR) {
-                    // tap pairs: floats 2j - 1 (right of pair j - 1) and 2j
-                    // (left of pair j) both hold f[j]; lane l writes float
-                    // 2 c0 - 1 + l, which is f[c0 + l / 2]; the right of the
-                    // last pair (float 2 nu - 1) is zero, as are the floats
-                    // of the pairs before the row (-4 .. -2)
-                    const int j = c0 + (lane >> 1);
-                    for (int rr = 0; rr < 32; ++rr) {
-                        const long mr = m0 + q * 32 + rr;
-                        if (mr >= rows) break;
-                        float* dst = C + mr * 2 * ldc + 2 * kPairLead;
-                        if (j < nu) dst[2 * c0 - 1 + lane] = stg[rr * kStagePitch + (lane >> 1)];
-                        else if (j == nu && (lane & 1) == 0) dst[2 * c0 - 1 + lane] = 0.f;
-                        if (c0 == 0 && lane < 3) dst[-4 + lane] = 0.f;
+                    if (vec) {
+                        // 16-byte blocks [xb, xb + 4), xb = 2 c0 - 4 + 4 t:
+                        // (f[m], f[m+1], f[m+1], f[m+2]), m = c0 - 2 + 2 t;
+                        // eight lanes a row, four rows a store
+                        const int t = lane & 7, g = lane >> 3;
+                        const int xb = 2 * c0 - 4 + 4 * t;
+                        const bool whole = xb >= X0 && xb + 4 <= X1;
+                        const bool some = xb + 4 > X0 && xb < X1;
+#pragma unroll
+                        for (int qq = 0; qq < 8; ++qq) {
+                            const int rr = 4 * qq + g;
+                            const long mr = wrow0 + rr;
+                            if (mr >= rows || !some) continue;
+                            const float* sp = stg + rr * kStagePitch + 2 * t;
+                            const float a = sp[0], b = sp[1], e = sp[2];
+                            float* dst = C + mr * 2 * ldc + 2 * kPairLead + xb;
+                            if (whole) {
+                                *reinterpret_cast<float4*>(dst) = make_float4(a, b, b, e);
+                            } else {
+                                if (xb >= X0 && xb < X1) dst[0] = a;
+                                if (xb + 1 >= X0 && xb + 1 < X1) dst[1] = b;
+                                if (xb + 2 >= X0 && xb + 2 < X1) dst[2] = b;
+                                if (xb + 3 >= X0 && xb + 3 < X1) dst[3] = e;
+                            }
+                        }
+                    } else {
+                        // lane l writes float 2 c0 - 1 + l, which is f[c0 + l / 2]
+                        const int xl = 2 * c0 - 1 + lane;
+                        for (int rr = 0; rr < 32; ++rr) {
+                            const long mr = wrow0 + rr;
+                            if (mr >= rows) break;
+                            float* dst = C + mr * 2 * ldc + 2 * kPairLead;
+                            if (xl >= X0 && xl < X1) dst[xl] = stg[rr * kStagePitch + 2 + (lane >> 1)];
+                            if (c0 == 0 && lane < 3) dst[-4 + lane] = 0.f;
+                        }
                     }
                 } else {
-                    const int half = lane >> 4, jj = c0 + (lane & 15);
-                    for (int rr = 0; rr < 32; rr += 2) {
-                        const long mr = m0 + q * 32 + rr + half;
-                        if (mr < rows && jj < nu)
-                            C[mr * ldc + jj] = stg[(rr + half) * kStagePitch + (lane & 15)];
+                    const int xe = min(n0 + TN, nu);  // this tile's columns [n0, xe)
+                    if (vec) {
+                        // 16-byte blocks: four lanes a row, eight rows a store
+                        const int t = lane & 3, g = lane >> 2;
+                        const int xb = c0 + 4 * t;
+#pragma unroll
+                        for (int qq = 0; qq < 4; ++qq) {
+                            const int rr = 8 * qq + g;
+                            const long mr = wrow0 + rr;
+                            if (mr >= rows || xb >= xe) continue;
+                            const float* sp = stg + rr * kStagePitch + 2 + 4 * t;
+                            float* dst = C + mr * ldc + xb;
+                            if (xb + 4 <= xe) {
+                                *reinterpret_cast<float4*>(dst) = make_float4(sp[0], sp[1], sp[2], sp[3]);
+                            } else {
+                                for (int e = 0; e < 4; ++e)
+                                    if (xb + e < xe) dst[e] = sp[e];
+                            }
+                        }
+                    } else {
+                        const int half = lane >> 4, jj = c0 + (lane & 15);
+                        for (int rr = 0; rr < 32; rr += 2) {
+                            const long mr = wrow0 + rr + half;
+                            if (mr < rows && jj < xe)
+                                C[mr * ldc + jj] = stg[(rr + half) * kStagePitch + 2 + (lane & 15)];
+                        }
                     }
                 }
                 __syncwarp();
+            }
+            if constexpr (PAIR) {
+                // the tile's last block, floats 2 (n0 + TN) - 4 .. - 1 =
+                // f[n0 + TN - 2], f[n0 + TN - 1] twice, f[n0 + TN]; the last
+                // is the next tile's, or zero when the tile ends at nu
+                if (vec && m < rows) {
+                    const int xb = 2 * (n0 + TN) - 4;
+                    float* dst = C + m * 2 * ldc + 2 * kPairLead + xb;
+                    if (xb >= X0 && xb < X1) dst[0] = carry0;
+                    if (xb + 1 >= X0 && xb + 1 < X1) dst[1] = carry1;
+                    if (xb + 2 >= X0 && xb + 2 < X1) dst[2] = carry1;
+                    if (xb + 3 >= X0 && xb + 3 < X1) dst[3] = 0.f;
+                }
             }
             // this accumulator is read out: the MMA warp may refill it
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -444,8 +558,11 @@ bool make_map(CUtensorMap* map, const void* base, long inner, long outer, long l
 
 template <int TN, bool PAIR, int NSEG>
 cudaError_t launch_tn3(const CUtensorMap* a, const CUtensorMap* t, long rows, int nu, int nv,
-    int kchunks, const FdkPreweightView* pwv, float* C, int ldc, int* err, cudaStream_t s)
+    int kchunks, int near, const FdkPreweightView* pwv, float* C, int ldc, int* err, cudaStream_t s)
 {
+    // 16-byte stores need the rows 16-byte aligned: tap-pair rows are
+    // 2 ldc floats with kPairLead pairs before element 0
+    const int vec = reinterpret_cast<uintptr_t>(C) % 16 == 0 && ldc % (PAIR ? 2 : 4) == 0;
     const size_t smem = 1024 + STAGES * (kAStageBytes + TN * TK * 2) +
         kEpiWarps * 32 * kStagePitch * sizeof(float) + (2 * STAGES + 5) * 8 + 16;
     auto k = ramp_tc_kernel<TN, PAIR, NSEG>;
@@ -460,16 +577,17 @@ cudaError_t launch_tn3(const CUtensorMap* a, const CUtensorMap* t, long rows, in
     const long tiles = static_cast<long>(col_tiles) * ((rows + TM - 1) / TM);
     const unsigned grid = static_cast<unsigned>(std::min<long>(tiles, sms));
     k<<<grid, kFilterThreads, smem, s>>>(a[0], a[1], a[2], t[0], t[1], t[2], rows, nu, nv,
-        kchunks, col_tiles, tiles, pwv, C, ldc, err);
+        kchunks, near, col_tiles, tiles, pwv, C, ldc, vec, err);
     return cudaGetLastError();
 }
 
 template <int TN, bool PAIR>
 cudaError_t launch_tn(const CUtensorMap* a, const CUtensorMap* t, int nseg, long rows, int nu,
-    int nv, int kchunks, const FdkPreweightView* pwv, float* C, int ldc, int* err, cudaStream_t s)
+    int nv, int kchunks, int near, const FdkPreweightView* pwv, float* C, int ldc, int* err,
+    cudaStream_t s)
 {
-    return nseg == 6 ? launch_tn3<TN, PAIR, 6>(a, t, rows, nu, nv, kchunks, pwv, C, ldc, err, s)
-                     : launch_tn3<TN, PAIR, 3>(a, t, rows, nu, nv, kchunks, pwv, C, ldc, err, s);
+    return nseg == 6 ? launch_tn3<TN, PAIR, 6>(a, t, rows, nu, nv, kchunks, near, pwv, C, ldc, err, s)
+                     : launch_tn3<TN, PAIR, 3>(a, t, rows, nu, nv, kchunks, near, pwv, C, ldc, err, s);
 }
 
 } // namespace
@@ -490,6 +608,23 @@ bool tcgen05_filter_supported(int nu) { return tma_encode() != nullptr && nu >= 
 
 int tc_filter_lda(int nu) { return (nu + TK - 1) / TK * TK; }
 
+int tc_filter_near_chunks(const std::vector<double>& h, int nu)
+{
+    // h[nu - 1 + d] = h(d), d in (-nu, nu); a tile skips, in its 2^-16
+    // products, only lags |d| > near * TK
+    const int kchunks = (nu + TK - 1) / TK;
+    double total = 0.0;
+    for (double v : h) total += std::fabs(v);
+    for (int near = 1; near < kchunks; ++near) {
+        double tail = 0.0;
+        for (int d = near * TK + 1; d < nu; ++d)
+            tail += std::fabs(h[static_cast<size_t>(nu - 1 + d)]) +
+                std::fabs(h[static_cast<size_t>(nu - 1 - d)]);
+        if (tail <= total / 256.0) return near;
+    }
+    return kchunks;
+}
+
 cudaError_t launch_fdk_preweight_split_bf16(const void* proj, int proj_dtype,
     const FdkPreweightView* pw, const float* parker, int n_views, int nu, int nv, int ld,
     __nv_bfloat16* const parts[3], cudaStream_t s)
@@ -506,7 +641,7 @@ cudaError_t launch_fdk_preweight_split_bf16(const void* proj, int proj_dtype,
 
 cudaError_t launch_fdk_ramp_tcgen05(const __nv_bfloat16* const a_parts[3],
     const __nv_bfloat16* const t_parts[3], int rows, int nu, int ld, const FdkPreweightView* pwv,
-    int nv, float* out, int layout, int ldc, int* err, cudaStream_t s)
+    int nv, float* out, int layout, int ldc, int near_chunks, int* err, cudaStream_t s)
 {
     if (rows <= 0) return cudaSuccess;
     const int tn = tc_filter_tile_n(nu);
@@ -521,16 +656,17 @@ cudaError_t launch_fdk_ramp_tcgen05(const __nv_bfloat16* const a_parts[3],
     }
     const int nseg = nparts == 3 ? 6 : 3;
     const int kchunks = (nu + TK - 1) / TK;
+    const int near = std::min(std::max(near_chunks, 1), kchunks);
     const bool pair = layout == kFilteredPairs;
     switch (tn) {
-    case 256: return pair ? launch_tn<256, true>(a, t, nseg, rows, nu, nv, kchunks, pwv, out, ldc, err, s)
-                          : launch_tn<256, false>(a, t, nseg, rows, nu, nv, kchunks, pwv, out, ldc, err, s);
-    case 192: return pair ? launch_tn<192, true>(a, t, nseg, rows, nu, nv, kchunks, pwv, out, ldc, err, s)
-                          : launch_tn<192, false>(a, t, nseg, rows, nu, nv, kchunks, pwv, out, ldc, err, s);
-    case 128: return pair ? launch_tn<128, true>(a, t, nseg, rows, nu, nv, kchunks, pwv, out, ldc, err, s)
-                          : launch_tn<128, false>(a, t, nseg, rows, nu, nv, kchunks, pwv, out, ldc, err, s);
-    default: return pair ? launch_tn<64, true>(a, t, nseg, rows, nu, nv, kchunks, pwv, out, ldc, err, s)
-                         : launch_tn<64, false>(a, t, nseg, rows, nu, nv, kchunks, pwv, out, ldc, err, s);
+    case 256: return pair ? launch_tn<256, true>(a, t, nseg, rows, nu, nv, kchunks, near, pwv, out, ldc, err, s)
+                          : launch_tn<256, false>(a, t, nseg, rows, nu, nv, kchunks, near, pwv, out, ldc, err, s);
+    case 192: return pair ? launch_tn<192, true>(a, t, nseg, rows, nu, nv, kchunks, near, pwv, out, ldc, err, s)
+                          : launch_tn<192, false>(a, t, nseg, rows, nu, nv, kchunks, near, pwv, out, ldc, err, s);
+    case 128: return pair ? launch_tn<128, true>(a, t, nseg, rows, nu, nv, kchunks, near, pwv, out, ldc, err, s)
+                          : launch_tn<128, false>(a, t, nseg, rows, nu, nv, kchunks, near, pwv, out, ldc, err, s);
+    default: return pair ? launch_tn<64, true>(a, t, nseg, rows, nu, nv, kchunks, near, pwv, out, ldc, err, s)
+                         : launch_tn<64, false>(a, t, nseg, rows, nu, nv, kchunks, near, pwv, out, ldc, err, s);
     }
 }
 

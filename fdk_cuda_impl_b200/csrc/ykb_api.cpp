@@ -229,6 +229,9 @@ YKB_API ykb_status ykb_fdk_plan_create_ex(const ykb_cone_view* views, int n_view
                 if (p->tc_parts == 3)
                     t2[at] = __float2bfloat16_rn(static_cast<float>(v - static_cast<double>(__bfloat162float(b1))));
             }
+        p->tc_near = tc_filter_near_chunks(h, nu);
+        if (const char* v = std::getenv("YKB_FDK_FILTER_NEAR"))
+            if (std::atoi(v) > 0) p->tc_near = std::atoi(v);
         if ((e = p->toeplitz_hi.alloc(tn * 2)) != cudaSuccess ||
             (e = p->toeplitz_lo.alloc(tn * 2)) != cudaSuccess ||
             (p->tc_parts == 3 && (e = p->toeplitz_lo2.alloc(tn * 2)) != cudaSuccess) ||
@@ -391,7 +394,7 @@ ykb_status filter_chunk_(ykb_fdk_plan* p, const void* proj, int proj_dtype, int 
             const size_t out_row = layout == kFilteredPairs ? 2 * static_cast<size_t>(ldc)
                                                             : static_cast<size_t>(ldc);
             YKB_TRY_CUDA(launch_fdk_ramp_tcgen05(ac, t, (v1 - v0) * p->nv, p->nu, p->lda, pwv + v0,
-                p->nv, dst + row0 * out_row, layout, ldc, p->err_flag.as<int>(), s));
+                p->nv, dst + row0 * out_row, layout, ldc, p->tc_near, p->err_flag.as<int>(), s));
         }
         return YKB_OK;
     }

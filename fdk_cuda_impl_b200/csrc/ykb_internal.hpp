@@ -199,11 +199,16 @@ cudaError_t launch_fdk_preweight_split_bf16(const void* proj, int proj_dtype,
     __nv_bfloat16* const parts[3], cudaStream_t s);
 // tcgen05 Toeplitz filter over split operands: two parts each (3 products,
 // BF16 plans) or three (6 products, FP32 accuracy) when a_parts[2] and
-// t_parts[2] are given
+// t_parts[2] are given.  With three parts the three products at the 2^-16
+// level run only over the K chunks (64 columns each) within `near_chunks`
+// chunks of each output tile; tc_filter_near_chunks(h, nu) picks the
+// fewest chunks for which the filter taps left out carry at most 2^-8 of
+// the taps' absolute sum.
 cudaError_t launch_fdk_ramp_tcgen05(const __nv_bfloat16* const a_parts[3],
     const __nv_bfloat16* const t_parts[3], int rows, int nu, int ld,
-    const FdkPreweightView* pwv, int nv, float* out, int layout, int ldc, int* err_flag,
-    cudaStream_t s);
+    const FdkPreweightView* pwv, int nv, float* out, int layout, int ldc, int near_chunks,
+    int* err_flag, cudaStream_t s);
+int tc_filter_near_chunks(const std::vector<double>& h, int nu);
 bool tcgen05_filter_supported(int nu);
 int tc_filter_lda(int nu);
 cudaError_t launch_fdk_backproject(const void* filtered, int dtype,
@@ -297,6 +302,7 @@ struct ykb_fdk_plan {
     bool axial = false;
     bool tc_filter = false;
     int tc_parts = 0;            // BF16 parts per operand of the tensor-core filter (2 or 3)
+    int tc_near = 0;             // K chunks each side of a tile that its 2^-16 products cover
     int batch_capacity = 0;      // views the workspace holds
     int ld = 0;                  // row pitch (elements) of the filtered workspace
     int layout = 0;              // FilteredLayout of the filtered workspace

@@ -234,6 +234,41 @@ def test_fdk_filter_stage_wide(oracle, cuda_device, monkeypatch, nu, path):
     assert K.rel_rmse(got, ref) <= 5e-6 * max(1.0, nu / 768)
 
 
+@pytest.mark.parametrize("kind,cutoff", [("ramlak", 0.5), ("hamming", 0.5), ("ramlak", 0.3),
+                                         ("tukey", 0.45)])
+def test_tc_filter_near_band_matches_full_band(oracle, cuda_device, monkeypatch, kind, cutoff):
+    # FP32 plans run their three 2^-16 products only over the K chunks near
+    # each output tile when the taps beyond are small (1/d^2 tails); a slow
+    # tail (a sharp cut-off below Nyquist) keeps more chunks.  Smooth rows:
+    # the ramp output cancels most of the lag sum
+    import torch
+    from fdk_cuda_impl_b200.geometry import CircularScan
+    from fdk_cuda_impl_b200.projectors import FdkPlan
+    nu, nv = 1536, 6
+    scan = CircularScan(3, 3, 500.0, 1000.0, nu, nv, 0.4, 0.4)
+    v = scan.views()
+    case = K.c1_small()
+    filt = K.RampFilter.named(kind, cutoff=cutoff)
+    u = (np.arange(nu) - nu / 2 + 0.3) / (0.35 * nu)
+    disc = 100.0 * np.sqrt(np.clip(1.0 - u * u, 0.0, None))
+    p = (disc[None, None, :] + oracle.uniform((3, nv, nu), -0.5, 0.5, 61)).astype(np.float32)
+    out = {}
+    for near in ("auto", "1000"):
+        if near == "auto":
+            monkeypatch.delenv("YKB_FDK_FILTER_NEAR", raising=False)
+        else:
+            monkeypatch.setenv("YKB_FDK_FILTER_NEAR", near)
+        plan = FdkPlan(v, nu, nv, scan.scan_range, case.grid, filt)
+        out[near] = plan.filter(torch.from_numpy(p).cuda()).cpu().numpy()
+        plan.check()
+        plan.close()
+    ref = oracle.fdk_filter(v, nu, nv, scan.scan_range, K.oracle_filter(oracle, filt), p)
+    full, near = K.rel_rmse(out["1000"], ref), K.rel_rmse(out["auto"], ref)
+    # FP32 sums over 1536 lags (the full band measured 1.0e-5 for Hamming)
+    assert full <= 2e-5
+    assert near <= 1.1 * full
+
+
 @pytest.mark.parametrize("nu,nv,views", [(96, 64, 12), (53, 41, 7), (192, 24, 5), (384, 8, 3),
                                          (768, 8, 2), (1536, 6, 2)])
 def test_tc_filter_stage(oracle, cuda_device, nu, nv, views):
