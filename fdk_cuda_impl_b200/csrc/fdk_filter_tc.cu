@@ -160,8 +160,29 @@ __device__ __forceinline__ void step_of(int i, int kchunks, NearChunks nc, int& 
 
 static_assert((2 * kPairLead) % 4 == 0, "tap-pair rows start 16-byte aligned after the lead");
 constexpr int kEpiWarps = 4;
-constexpr int kFilterThreads = 64 + 32 * kEpiWarps;  // producer, MMA issuer, 4 epilogue warps
+constexpr int kEpiSplit = kEpiWarps / 4;             // epilogue warps per quarter of the TMEM lanes
+constexpr int kFilterThreads = 64 + 32 * kEpiWarps;  // producer, MMA issuer, epilogue warps
 constexpr int kStagePitch = 19;                       // floats per staged row: 2 carried + 16 (odd: no bank conflicts)
+
+// 16 consecutive TMEM columns of this warp's 32 lanes, one per register;
+// the registers are valid after tmem_wait_ld, which takes them as operands
+// so that no use of them is placed before the wait
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16])
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+                   "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
+                   "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                 : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld(uint32_t (&r)[16])
+{
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]),
+                   "+r"(r[6]), "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]),
+                   "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15])
+                 :: "memory");
+}
 
 __device__ __forceinline__ void bar_arrive(uint64_t* b)
 {
@@ -292,8 +313,14 @@ __global__ void __launch_bounds__(kFilterThreads, 1) ramp_tc_kernel(
         __syncwarp();
     } else {
         // --------------------------------------------------- epilogue ---
-        // warp w reads TMEM lanes 32 (w % 4) ..: rows m0 + 32 (w % 4) + lane
-        const int q = warp & 3;
+        // warp w reads TMEM lanes 32 (w % 4) ..: rows m0 + 32 (w % 4) + lane,
+        // columns [h TW, (h + 1) TW) of the tile, h = (w - 2) / 4.  Eight
+        // epilogue warps, or the next chunk's TMEM load issued before this
+        // one's stores, measured no faster: both take registers from the
+        // preweight that runs beside this kernel
+        constexpr int TW = TN / kEpiSplit;
+        static_assert(TW % 16 == 0, "whole 16-column chunks per epilogue warp");
+        const int q = warp & 3, h = (warp - 2) >> 2;
         float* stg = staging + (warp - 2) * 32 * kStagePitch;
         int tl = 0;
         for (long t = blockIdx.x; t < tiles; t += gridDim.x, ++tl) {
@@ -308,7 +335,7 @@ __global__ void __launch_bounds__(kFilterThreads, 1) ramp_tc_kernel(
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const long m0 = (t / col_tiles) * TM;
-            const int n0 = static_cast<int>((t % col_tiles) * TN);
+            const int n0 = static_cast<int>((t % col_tiles) * TN) + h * TW;  // this warp's columns
             const long wrow0 = m0 + q * 32;  // the warp's first row
             const long m = wrow0 + lane;
             // this lane's row keeps columns [lo, hi) (the samples placed in
@@ -319,29 +346,27 @@ __global__ void __launch_bounds__(kFilterThreads, 1) ramp_tc_kernel(
                 lo = max(p.out_lo, 0);
                 hi = max(min(p.out_hi, nu), lo);
             }
-            // tap pairs: this tile writes the floats [X0, X1) of each row
-            // (float x holds f[(x + 1) >> 1]): from 2 n0 - 1, or -4 for the
-            // first tile (the pairs before the row are zero), up to the
-            // next tile's first float, or 2 nu (the right half of the last
-            // pair is zero)
+            // tap pairs: this warp writes the floats [X0, X1) of each row
+            // (float x holds f[(x + 1) >> 1]): from 2 n0 - 1, or -4 at
+            // column 0 (the pairs before the row are zero), up to the next
+            // warp's (or tile's) first float, or 2 nu (the right half of the
+            // last pair is zero)
             const int X0 = n0 == 0 ? -4 : 2 * n0 - 1;
-            const int X1 = n0 + TN >= nu ? 2 * nu : 2 * (n0 + TN) - 1;
+            const int X1 = n0 + TW >= nu ? 2 * nu : 2 * (n0 + TW) - 1;
             float carry0 = 0.f, carry1 = 0.f;  // columns c0 - 2 and c0 - 1 of the lane's row
+            const uint32_t tcol = tmem + (static_cast<uint32_t>(q * 32) << 16) +
+                static_cast<uint32_t>(buf) * kAccCols + static_cast<uint32_t>(h * TW);
 #pragma unroll 1
-            for (int c = 0; c < TN; c += 16) {
+            for (int c = 0; c < TW; c += 16) {
                 uint32_t r[16];
-                const uint32_t taddr = tmem + (static_cast<uint32_t>(q * 32) << 16) +
-                    static_cast<uint32_t>(buf) * kAccCols + static_cast<uint32_t>(c);
-                asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-                             : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
-                               "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
-                               "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-                             : "r"(taddr));
-                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                tmem_ld16(tcol + static_cast<uint32_t>(c), r);
+                tmem_wait_ld(r);
                 const int c0 = n0 + c;
                 float x[16];
 #pragma unroll
                 for (int i = 0; i < 16; ++i) x[i] = __uint_as_float(r[i]);
+                // the next chunk's load runs while this one is stored
+
                 if (c0 < lo || c0 + 16 > hi) {
 #pragma unroll
                     for (int i = 0; i < 16; ++i)
@@ -395,7 +420,7 @@ __global__ void __launch_bounds__(kFilterThreads, 1) ramp_tc_kernel(
                         }
                     }
                 } else {
-                    const int xe = min(n0 + TN, nu);  // this tile's columns [n0, xe)
+                    const int xe = min(n0 + TW, nu);  // this warp's columns [n0, xe)
                     if (vec) {
                         // 16-byte blocks: four lanes a row, eight rows a store
                         const int t = lane & 3, g = lane >> 2;
@@ -426,11 +451,11 @@ __global__ void __launch_bounds__(kFilterThreads, 1) ramp_tc_kernel(
                 __syncwarp();
             }
             if constexpr (PAIR) {
-                // the tile's last block, floats 2 (n0 + TN) - 4 .. - 1 =
-                // f[n0 + TN - 2], f[n0 + TN - 1] twice, f[n0 + TN]; the last
-                // is the next tile's, or zero when the tile ends at nu
+                // the warp's last block, floats 2 (n0 + TW) - 4 .. - 1 =
+                // f[n0 + TW - 2], f[n0 + TW - 1] twice, f[n0 + TW]; the last
+                // is the next warp's, or zero when the columns end at nu
                 if (vec && m < rows) {
-                    const int xb = 2 * (n0 + TN) - 4;
+                    const int xb = 2 * (n0 + TW) - 4;
                     float* dst = C + m * 2 * ldc + 2 * kPairLead + xb;
                     if (xb >= X0 && xb < X1) dst[0] = carry0;
                     if (xb + 1 >= X0 && xb + 1 < X1) dst[1] = carry1;

@@ -494,19 +494,6 @@ __global__ void joseph_column_check_kernel(const float4* __restrict__ rays,
     if (__any_sync(0xffffffffu, differs) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
 }
 
-// (a2, e2, value x chord length, 0) per ray: one 16-byte load per ray in the
-// line backprojector.
-__global__ void joseph_weight_rays4_kernel(const float* __restrict__ proj,
-    const float4* __restrict__ rays, const float* __restrict__ lens, long n,
-    float4* __restrict__ out)
-{
-    for (long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; i < n;
-         i += static_cast<long>(gridDim.x) * blockDim.x) {
-        const float4 r = rays[i];
-        out[i] = make_float4(r.z, r.w, proj[i] * lens[i], 0.f);
-    }
-}
-
 // ---------------------------------------------------------------------------
 // Line backprojector (axial-column scans).  The transpose factors per
 // detector column: voxel (s, j1, j2) of a view gets
@@ -515,9 +502,10 @@ __global__ void joseph_weight_rays4_kernel(const float* __restrict__ proj,
 // where L, the column's rays splatted onto the z line of slice s, does not
 // depend on j1.  A CTA owns 16 x 16 voxel columns of ZC slices.  Per view it
 // builds, for each of its 16 slices, the lines of the detector columns that
-// reach its 16 minor-1 indices (a warp per slice, a lane per line, each lane
-// walking its column's rays in order: every ray once per slice instead of
-// once per voxel column it touches, about 2.5), then each thread adds the
+// reach its 16 minor-1 indices (a warp per two adjacent slices, a lane per
+// line, each lane walking its column's rays in order and splatting each
+// onto both slices: every ray loaded once per two slices instead of once per
+// voxel column it touches, about 2.5), then each thread adds the
 // lines of its own column's candidate detector columns, weighted by h1, to
 // its ZC sums.  Weights are the forward projector's; over two views the sums
 // are FP32 (lines in ray order, then over detector columns), then FP64 in
@@ -546,7 +534,7 @@ constexpr size_t line_smem_bytes()
 
 template <int ZC>
 __global__ void __launch_bounds__(kLineThreads, 3) joseph_bp_lines_kernel(
-    const float4* __restrict__ w4, const float2* __restrict__ cols,
+    const float4* __restrict__ rays, const float* __restrict__ wv, const float2* __restrict__ cols,
     const ViewProj* __restrict__ vp, const JosephView* __restrict__ views, int n_views, int nu,
     int nv, int nx, int ny, int nz, float* __restrict__ vol, int accumulate)
 {
@@ -580,6 +568,20 @@ __global__ void __launch_bounds__(kLineThreads, 3) joseph_bp_lines_kernel(
             if (tid < nS)
                 footprint_box_range(vp[k], j, static_cast<float>(S0 + tid) - half, J0,
                     J0 + nJ - 1, z0, z0 + ZC - 1, nu, nv, u0, u1, v0, v1);
+            // slices 2i and 2i + 1 share the union of their boxes: a ray
+            // outside a slice's own box adds nothing to the lines its voxel
+            // columns read
+            const bool some = u0 <= u1 && v0 <= v1;
+            const int pu0 = __shfl_xor_sync(0xFFFFu, u0, 1), pu1 = __shfl_xor_sync(0xFFFFu, u1, 1);
+            const int pv0 = __shfl_xor_sync(0xFFFFu, v0, 1), pv1 = __shfl_xor_sync(0xFFFFu, v1, 1);
+            if (pu0 <= pu1 && pv0 <= pv1) {
+                if (some) {
+                    u0 = min(u0, pu0); u1 = max(u1, pu1);
+                    v0 = min(v0, pv0); v1 = max(v1, pv1);
+                } else {
+                    u0 = pu0; u1 = pu1; v0 = pv0; v1 = pv1;
+                }
+            }
             pbox[tid] = make_int4(u0, u1, v0, v1);
         }
         __syncthreads();
@@ -594,64 +596,59 @@ __global__ void __launch_bounds__(kLineThreads, 3) joseph_bp_lines_kernel(
         const float j1f = static_cast<float>(j1);
         const float2* ck = cols + static_cast<long>(k) * nu;
         for (int pass = 0; pass < passes; ++pass) {
-            // ---- lines: warp w builds slices w and w + 8, lane = line
-            for (int sp = warp; sp < B; sp += kLineThreads / 32) {
-                const int4 b = pbox[sp];
-                float* L = lines + sp * PS + lane;
+            // ---- lines: warp w builds slices 2w and 2w + 1, lane = line
+            {
+                static_assert(B == 2 * (kLineThreads / 32), "a warp per two slices");
+                const int sp = 2 * warp;
+                const int4 b = pbox[sp];  // the pair's box
+                float* La = lines + sp * PS + lane;
+                float* Lb = La + PS;
 #pragma unroll
-                for (int q = 0; q < SL; ++q) L[q * LM] = 0.f;
+                for (int q = 0; q < SL; ++q) {
+                    La[q * LM] = 0.f;
+                    Lb[q * LM] = 0.f;
+                }
                 const int iu = b.x + pass * LM + lane;
-                if (iu > b.y) continue;
-                const float cs = static_cast<float>(S0 + sp) - half;
-                const float4* r = w4 + (static_cast<long>(k) * nv + b.z) * nu + iu;
-                int iv = b.z;
-                auto splat = [&](const float4& qa, const float4& qb) {
-                    const f2 f = f2pack(fmaf(qa.x, cs, qa.y), fmaf(qb.x, cs, qb.y));
-                    const f2 t = f2add(f2sub(f, H), M);
-                    float ta, tb, wa, wb;
-                    f2unpack(t, ta, tb);
-                    f2unpack(f2sub(f, f2sub(t, M)), wa, wb);
-                    const uint32_t sa = __float_as_uint(ta) - slot0, sb = __float_as_uint(tb) - slot0;
-                    if (sa <= static_cast<uint32_t>(ZC)) {
-                        float* o = L + sa * LM;
-                        o[0] = fmaf(qa.z, 1.f - wa, o[0]);
-                        o[LM] = fmaf(qa.z, wa, o[LM]);
+                if (iu <= b.y) {
+                    const float csa = static_cast<float>(S0 + sp) - half;
+                    const float csb = static_cast<float>(S0 + sp + 1) - half;
+                    const long r0 = (static_cast<long>(k) * nv + b.z) * nu + iu;
+                    // (a2, e2) are the last two floats of each ray's record
+                    const float2* ae = reinterpret_cast<const float2*>(rays) + 2 * r0 + 1;
+                    const float* tv = wv + r0;
+                    const long st = 2l * nu;  // float2 records from one row to the next
+                    int iv = b.z;
+                    auto splat = [&](const float2 a, const float v) {
+                        const f2 f = f2pack(fmaf(a.x, csa, a.y), fmaf(a.x, csb, a.y));
+                        const f2 t = f2add(f2sub(f, H), M);
+                        float ta, tb, wa, wb;
+                        f2unpack(t, ta, tb);
+                        f2unpack(f2sub(f, f2sub(t, M)), wa, wb);
+                        const uint32_t sa = __float_as_uint(ta) - slot0, sb = __float_as_uint(tb) - slot0;
+                        if (sa <= static_cast<uint32_t>(ZC)) {
+                            float* o = La + sa * LM;
+                            o[0] = fmaf(v, 1.f - wa, o[0]);
+                            o[LM] = fmaf(v, wa, o[LM]);
+                        }
+                        if (sb <= static_cast<uint32_t>(ZC)) {
+                            float* o = Lb + sb * LM;
+                            o[0] = fmaf(v, 1.f - wb, o[0]);
+                            o[LM] = fmaf(v, wb, o[LM]);
+                        }
+                    };
+                    // eight rays per step: their loads are in flight together
+                    for (; iv + 7 <= b.w; iv += 8, ae += 8 * st, tv += 8 * nu) {
+                        float2 a[8];
+                        float v[8];
+#pragma unroll
+                        for (int i = 0; i < 8; ++i) {
+                            a[i] = __ldg(ae + i * st);
+                            v[i] = __ldg(tv + i * nu);
+                        }
+#pragma unroll
+                        for (int i = 0; i < 8; ++i) splat(a[i], v[i]);
                     }
-                    if (sb <= static_cast<uint32_t>(ZC)) {
-                        float* o = L + sb * LM;
-                        o[0] = fmaf(qb.z, 1.f - wb, o[0]);
-                        o[LM] = fmaf(qb.z, wb, o[LM]);
-                    }
-                };
-                // eight rays per step: their loads are in flight together
-                for (; iv + 7 <= b.w; iv += 8, r += 8 * nu) {
-                    const float4 qa = __ldg(r), qb = __ldg(r + nu);
-                    const float4 qc = __ldg(r + 2 * nu), qd = __ldg(r + 3 * nu);
-                    const float4 qe = __ldg(r + 4 * nu), qf = __ldg(r + 5 * nu);
-                    const float4 qg = __ldg(r + 6 * nu), qh = __ldg(r + 7 * nu);
-                    splat(qa, qb);
-                    splat(qc, qd);
-                    splat(qe, qf);
-                    splat(qg, qh);
-                }
-                for (; iv + 3 <= b.w; iv += 4, r += 4 * nu) {
-                    const float4 qa = __ldg(r), qb = __ldg(r + nu);
-                    const float4 qc = __ldg(r + 2 * nu), qd = __ldg(r + 3 * nu);
-                    splat(qa, qb);
-                    splat(qc, qd);
-                }
-                for (; iv + 1 <= b.w; iv += 2, r += 2 * nu) splat(__ldg(r), __ldg(r + nu));
-                if (iv <= b.w) {
-                    const float4 qa = __ldg(r);
-                    const float fa = fmaf(qa.x, cs, qa.y);
-                    const float ta = (fa - 0.5f) + kMagic;
-                    const float wa = fa - (ta - kMagic);
-                    const uint32_t sa = __float_as_uint(ta) - slot0;
-                    if (sa <= static_cast<uint32_t>(ZC)) {
-                        float* o = L + sa * LM;
-                        o[0] = fmaf(qa.z, 1.f - wa, o[0]);
-                        o[LM] = fmaf(qa.z, wa, o[LM]);
-                    }
+                    for (; iv <= b.w; ++iv, ae += st, tv += nu) splat(__ldg(ae), __ldg(tv));
                 }
             }
             __syncthreads();
@@ -708,10 +705,10 @@ cudaError_t launch_joseph_column_table(const float4* rays, int n_views, int nu, 
 
 cudaError_t launch_joseph_bp_lines(const float* proj, const float4* rays, const float* lens,
     const float2* cols, const float* view_proj, const JosephView* views, int n_views, int nu,
-    int nv, const ykb_volume& vol, float4* weighted4, float* out, int accumulate, cudaStream_t s)
+    int nv, const ykb_volume& vol, float* weighted, float* out, int accumulate, cudaStream_t s)
 {
     const long n = static_cast<long>(n_views) * nu * nv;
-    joseph_weight_rays4_kernel<<<148 * 8, 256, 0, s>>>(proj, rays, lens, n, weighted4);
+    joseph_weight_rays_kernel<<<148 * 8, 256, 0, s>>>(proj, lens, n, weighted);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     constexpr int ZC = 16;
@@ -722,7 +719,7 @@ cudaError_t launch_joseph_bp_lines(const float* proj, const float4* rays, const 
         return e;
     const dim3 grid((vol.nx + kLineBlock - 1) / kLineBlock, (vol.ny + kLineBlock - 1) / kLineBlock,
         (vol.nz + ZC - 1) / ZC);
-    k<<<grid, kLineThreads, smem, s>>>(weighted4, cols, reinterpret_cast<const ViewProj*>(view_proj),
+    k<<<grid, kLineThreads, smem, s>>>(rays, weighted, cols, reinterpret_cast<const ViewProj*>(view_proj),
         views, n_views, nu, nv, vol.nx, vol.ny, vol.nz, out, accumulate);
     return cudaGetLastError();
 }

@@ -821,7 +821,7 @@ YKB_API ykb_status ykb_joseph_plan_create(const ykb_cone_view* views, int n_view
         if (!p->column_bp) p->cols.reset();
     }
     if (e == cudaSuccess)
-        e = p->weighted.alloc((p->column_bp ? sizeof(float4) : sizeof(float)) * rays);
+        e = p->weighted.alloc(sizeof(float) * rays);
     cudaStreamDestroy(s);
     if (e != cudaSuccess) {
         delete p;
@@ -1092,7 +1092,7 @@ YKB_API ykb_status ykb_joseph_bp(ykb_joseph_plan* p, const float* d_proj, float*
     if (p->column_bp)
         YKB_TRY_CUDA(launch_joseph_bp_lines(d_proj, p->rays.as<float4>(), p->lens.as<float>(),
             p->cols.as<float2>(), p->view_proj.as<float>(), p->views.as<JosephView>(),
-            p->n_views, p->nu, p->nv, p->volume, p->weighted.as<float4>(), d_volume,
+            p->n_views, p->nu, p->nv, p->volume, p->weighted.as<float>(), d_volume,
             accumulate ? 1 : 0, s));
     else
         YKB_TRY_CUDA(launch_joseph_bp(d_proj, p->rays.as<float4>(), p->lens.as<float>(),

@@ -281,10 +281,10 @@ cudaError_t launch_siddon_bp(const float* proj, const ykb_cone_view* views, int 
 cudaError_t launch_joseph_column_table(const float4* rays, int n_views, int nu, int nv,
     float2* cols, int* flag, cudaStream_t s);
 // matched backprojection for axial-column scans (see launch_joseph_column_table):
-// weighted4 receives (a2, e2, input x chord length, 0) per ray
+// weighted receives input x chord length per ray
 cudaError_t launch_joseph_bp_lines(const float* proj, const float4* rays, const float* lens,
     const float2* cols, const float* view_proj, const JosephView* views, int n_views, int nu,
-    int nv, const ykb_volume& vol, float4* weighted4, float* out, int accumulate, cudaStream_t s);
+    int nv, const ykb_volume& vol, float* weighted, float* out, int accumulate, cudaStream_t s);
 cudaError_t launch_joseph_bp(const float* proj, const float4* rays, const float* lens,
     const float* view_proj, const JosephView* views, int n_views, int nu, int nv,
     const ykb_volume& vol, float* weighted, float* out, int accumulate, cudaStream_t s);
