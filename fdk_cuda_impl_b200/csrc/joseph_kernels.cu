@@ -507,7 +507,7 @@ __global__ void joseph_column_check_kernel(const float4* __restrict__ rays,
 // onto both slices: every ray loaded once per two slices instead of once per
 // voxel column it touches, about 2.5), then each thread adds the
 // lines of its own column's candidate detector columns, weighted by h1, to
-// its ZC sums.  Weights are the forward projector's; over two views the sums
+// its ZC sums.  Weights are the forward projector's; over four views the sums
 // are FP32 (lines in ray order, then over detector columns), then FP64 in
 // shared memory.  Lines live in shared memory as [slice][slot][line], one
 // bank per lane, slices 21 mod 32 words apart; a slice with more than
@@ -529,7 +529,7 @@ template <int ZC>
 constexpr size_t line_smem_bytes()
 {
     return sizeof(double) * ZC * kLineThreads + sizeof(float) * kLineBlock * line_slice_words<ZC>() +
-        sizeof(int4) * kLineBlock + 16;
+        sizeof(int4) * 2 * (kLineBlock + 1) + 16;
 }
 
 template <int ZC>
@@ -542,7 +542,11 @@ __global__ void __launch_bounds__(kLineThreads, 3) joseph_bp_lines_kernel(
     extern __shared__ __align__(16) unsigned char line_smem[];
     double* total = reinterpret_cast<double*>(line_smem);                 // [q][thread]
     float* lines = reinterpret_cast<float*>(total + ZC * kLineThreads);  // [slice][slot][line]
-    int4* pbox = reinterpret_cast<int4*>(                                 // per slice: u0, u1, v0, v1
+    // per view, by view parity: per slice u0, u1, v0, v1, then the passes.
+    // A thread still reading view k's entries keeps them from being
+    // overwritten (at view k + 2) until it reaches view k + 1's barrier, also
+    // when view k needs no pass (and so no barrier of its own)
+    int4* pbox2 = reinterpret_cast<int4*>(
         (reinterpret_cast<uintptr_t>(lines + B * PS) + 15) & ~static_cast<uintptr_t>(15));
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int tx = tid % B, ty = tid / B;
@@ -554,7 +558,7 @@ __global__ void __launch_bounds__(kLineThreads, 3) joseph_bp_lines_kernel(
     // slot of floor(f2) + 1 from the rounding word of f2 - 1/2 (wrapping)
     const uint32_t slot0 = kMagicBits + static_cast<uint32_t>(z0 - 1);
     const f2 H = f2pack(0.5f, 0.5f), M = f2pack(kMagic, kMagic);
-    float acc[ZC];  // FP32 over two views, then into the FP64 sums
+    float acc[ZC];  // FP32 over four views, then into the FP64 sums
 #pragma unroll
     for (int q = 0; q < ZC; ++q) acc[q] = 0.f;
     for (int k = 0; k < n_views; ++k) {
@@ -562,6 +566,8 @@ __global__ void __launch_bounds__(kLineThreads, 3) joseph_bp_lines_kernel(
         const bool ax0 = j.axis == 0;
         const int S0 = ax0 ? X0 : Y0, J0 = ax0 ? Y0 : X0;  // first slice, first minor-1 index
         const int nS = min(B, j.n0 - S0), nJ = min(B, j.n1 - J0);
+        int4* pbox = pbox2 + (k & 1) * (B + 1);
+        int* pass_count = reinterpret_cast<int*>(pbox + B);
         const float half = 0.5f * (j.n0 - 1);
         if (tid < B) {
             int u0 = 0, u1 = -1, v0 = 0, v1 = -1;
@@ -583,11 +589,14 @@ __global__ void __launch_bounds__(kLineThreads, 3) joseph_bp_lines_kernel(
                 }
             }
             pbox[tid] = make_int4(u0, u1, v0, v1);
+            // passes of LM lines that the widest box needs
+            int np = u0 <= u1 ? (u1 - u0 + LM) / LM : 0;
+#pragma unroll
+            for (int o = 8; o > 0; o >>= 1) np = max(np, __shfl_xor_sync(0xFFFFu, np, o));
+            if (tid == 0) *pass_count = np;
         }
         __syncthreads();
-        int passes = 0;
-#pragma unroll
-        for (int p = 0; p < B; ++p) passes = max(passes, (pbox[p].y - pbox[p].x + LM) / LM);
+        const int passes = *pass_count;
         // this thread's voxel column: its slice, minor-1 index, candidates
         const int pl = ax0 ? tx : ty, j1 = ax0 ? y : x;
         const float c0 = static_cast<float>(S0 + pl) - half;
@@ -671,7 +680,7 @@ __global__ void __launch_bounds__(kLineThreads, 3) joseph_bp_lines_kernel(
             }
             __syncthreads();
         }
-        if ((k & 1) || k + 1 == n_views) {
+        if ((k & 3) == 3 || k + 1 == n_views) {
 #pragma unroll
             for (int q = 0; q < ZC; ++q) {
                 total[q * kLineThreads + tid] += static_cast<double>(acc[q]);
