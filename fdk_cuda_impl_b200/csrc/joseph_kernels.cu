@@ -507,7 +507,7 @@ __global__ void joseph_column_check_kernel(const float4* __restrict__ rays,
 // onto both slices: every ray loaded once per two slices instead of once per
 // voxel column it touches, about 2.5), then each thread adds the
 // lines of its own column's candidate detector columns, weighted by h1, to
-// its ZC sums.  Weights are the forward projector's; over eight views the sums
+// its ZC sums.  Weights are the forward projector's; over sixteen views the sums
 // are FP32 (lines in ray order, then over detector columns), then FP64 in
 // shared memory.  Lines live in shared memory as [slice][slot][line], one
 // bank per lane, slices 21 mod 32 words apart; a slice with more than
@@ -558,7 +558,7 @@ __global__ void __launch_bounds__(kLineThreads, 3) joseph_bp_lines_kernel(
     // slot of floor(f2) + 1 from the rounding word of f2 - 1/2 (wrapping)
     const uint32_t slot0 = kMagicBits + static_cast<uint32_t>(z0 - 1);
     const f2 H = f2pack(0.5f, 0.5f), M = f2pack(kMagic, kMagic);
-    float acc[ZC];  // FP32 over eight views, then into the FP64 sums
+    float acc[ZC];  // FP32 over sixteen views, then into the FP64 sums
 #pragma unroll
     for (int q = 0; q < ZC; ++q) acc[q] = 0.f;
     for (int k = 0; k < n_views; ++k) {
@@ -683,7 +683,7 @@ __global__ void __launch_bounds__(kLineThreads, 3) joseph_bp_lines_kernel(
             }
             __syncthreads();
         }
-        if ((k & 7) == 7 || k + 1 == n_views) {
+        if ((k & 15) == 15 || k + 1 == n_views) {
 #pragma unroll
             for (int q = 0; q < ZC; ++q) {
                 total[q * kLineThreads + tid] += static_cast<double>(acc[q]);
